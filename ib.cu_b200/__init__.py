@@ -1,0 +1,350 @@
+"""Python binding of the B200 immersed-boundary coupling library.
+
+The product is ``lib/libibk.so`` (hand-written sm_100a CUDA behind the C ABI
+in ``include/ibk.h``).  This module binds that ABI with ctypes and mirrors the
+reference's operator objects (sonwell/ib.cu ``include/ib/novel.h:193-250``
+and ``include/ib/interpolate.h:88-138``):
+
+    domain = Domain(Dimension(3.2, PERIODIC), Dimension(1.6, SOLID),
+                    Dimension(3.2, PERIODIC))
+    spread = Spread(Mac(64), domain, Bspline(3))
+    interpolate = Interpolate(Mac(64), domain, Bspline(3))
+    fe = spread(n, x, fl)          # list of device vectors, newly allocated
+    spread(n, x, fl, fe)           # overwrites fe
+    ul = interpolate(n, x, ue)
+
+Arrays are torch CUDA float64 tensors (device memory and streams only; no
+torch op is on the compute path).  There is no CPU fallback: every call
+raises if the CUDA library is missing or a CUDA call fails.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "lib", "libibk.so")
+
+# ---------------------------------------------------------------- ABI enums
+IBK_OK = 0
+STATUS_NAMES = {
+    0: "IBK_OK", 1: "IBK_ERR_INVALID_ARGUMENT", 2: "IBK_ERR_UNSUPPORTED",
+    3: "IBK_ERR_OUT_OF_MEMORY", 4: "IBK_ERR_CUDA", 5: "IBK_ERR_CAPACITY",
+    6: "IBK_ERR_DEVICE_CHECK",
+}
+PERIODIC, SOLID = 0, 1
+TAG_MAC, TAG_CENTERED = 0, 1
+BSPLINE, PESKIN, ROMA, COSINE, HAT = 0, 1, 2, 3, 4
+FP64, FP32C = 0, 1
+
+# Every symbol include/ibk.h declares (checked by the CPU test suite).
+ABI_SYMBOLS = (
+    "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
+    "ibk_spread", "ibk_interpolate", "ibk_sort_keys",
+    "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
+    "ibk_plan_launch_count",
+    "ibk_last_error", "ibk_status_string", "ibk_version",
+)
+
+
+class IbkError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class _Domain(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int), ("length", ctypes.c_double * 3),
+                ("boundary", ctypes.c_int * 3)]
+
+
+class _Delta(ctypes.Structure):
+    _fields_ = [("kind", ctypes.c_int), ("order", ctypes.c_int)]
+
+
+class KernelStat(ctypes.Structure):
+    _fields_ = [("name", ctypes.c_char * 48), ("launches", ctypes.c_longlong),
+                ("total_ms", ctypes.c_double)]
+
+
+class GridInfo(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int), ("meshwidths", ctypes.c_int),
+                ("unit", ctypes.c_double), ("resolution", ctypes.c_double),
+                ("points", (ctypes.c_int * 3) * 3), ("cells", (ctypes.c_int * 3) * 3),
+                ("shift", (ctypes.c_double * 3) * 3), ("size", ctypes.c_longlong * 3)]
+
+    def comp_points(self, c):
+        return [self.points[c][d] for d in range(self.dims)]
+
+
+_lib = None
+_vp = ctypes.c_void_p
+
+
+def build(force: bool = False) -> str:
+    """Compile lib/libibk.so for sm_100a with nvcc (in-tree)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-j8", "-C", HERE], check=True)
+    return LIB_PATH
+
+
+def lib() -> ctypes.CDLL:
+    """Load the CUDA library; raises if it is missing (no fallback)."""
+    global _lib
+    if _lib is None:
+        if not os.path.exists(LIB_PATH):
+            raise ImportError(f"CUDA library not built: {LIB_PATH} (run build())")
+        L = ctypes.CDLL(LIB_PATH)
+        L.ibk_plan_create.argtypes = [ctypes.POINTER(_Domain), ctypes.c_int, ctypes.c_int,
+                                      _Delta, ctypes.c_int, ctypes.POINTER(_vp)]
+        L.ibk_plan_destroy.argtypes = [_vp]
+        L.ibk_plan_info.argtypes = [_vp, ctypes.POINTER(GridInfo)]
+        L.ibk_plan_reserve.argtypes = [_vp, ctypes.c_int]
+        L.ibk_spread.argtypes = [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp), _vp]
+        L.ibk_interpolate.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_vp), _vp, _vp]
+        L.ibk_sort_keys.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
+        L.ibk_plan_set_profiling.argtypes = [_vp, ctypes.c_int]
+        L.ibk_plan_kernel_stats.argtypes = [_vp, ctypes.POINTER(KernelStat), ctypes.c_int,
+                                            ctypes.POINTER(ctypes.c_int)]
+        L.ibk_plan_reset_stats.argtypes = [_vp]
+        L.ibk_plan_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.ibk_last_error.restype = ctypes.c_char_p
+        L.ibk_status_string.restype = ctypes.c_char_p
+        L.ibk_status_string.argtypes = [ctypes.c_int]
+        for name in ("ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
+                     "ibk_spread", "ibk_interpolate", "ibk_sort_keys", "ibk_plan_set_profiling",
+                     "ibk_plan_kernel_stats", "ibk_plan_reset_stats", "ibk_plan_launch_count"):
+            getattr(L, name).restype = ctypes.c_int
+        _lib = L
+    return _lib
+
+
+def check(status: int) -> None:
+    if status != IBK_OK:
+        msg = lib().ibk_last_error()
+        raise IbkError(status, msg.decode() if msg else "")
+
+
+def _stream_handle(stream) -> int:
+    if stream is None:
+        import torch
+        return torch.cuda.current_stream().cuda_stream
+    if isinstance(stream, int):
+        return stream
+    return stream.cuda_stream
+
+
+def _ptr(t) -> int:
+    if t is None:
+        return None
+    if isinstance(t, int):
+        return t
+    return t.data_ptr()
+
+
+# ------------------------------------------------ reference-shaped objects
+class Dimension:
+    """fd::dimension{length, boundary} (include/fd/dimension.h:32-80)."""
+
+    def __init__(self, length: float, boundary: int = PERIODIC):
+        self.length = float(length)
+        self.boundary = int(boundary)
+
+
+class Domain:
+    """fd::domain{dims...} (include/fd/domain.h:15-33)."""
+
+    def __init__(self, *dimensions: Dimension):
+        if not 2 <= len(dimensions) <= 3:
+            raise ValueError("domains have 2 or 3 dimensions")
+        self.dimensions = list(dimensions)
+
+    @property
+    def dims(self) -> int:
+        return len(self.dimensions)
+
+    def _abi(self) -> _Domain:
+        d = _Domain()
+        d.dims = self.dims
+        for i, dim in enumerate(self.dimensions):
+            d.length[i] = dim.length
+            d.boundary[i] = dim.boundary
+        return d
+
+
+class Mac:
+    """fd::mac{refinement} (include/fd/cell.h:195)."""
+    tag = TAG_MAC
+
+    def __init__(self, refinement: int):
+        self.refinement = int(refinement)
+
+
+class Centered(Mac):
+    """fd::centered{refinement} (include/fd/cell.h:194)."""
+    tag = TAG_CENTERED
+
+
+class DeltaFn:
+    kind = BSPLINE
+    order = 0
+
+
+class Bspline(DeltaFn):
+    """ib::delta::bspline<n> (include/ib/bspline.h:13-63)."""
+
+    def __init__(self, order: int = 3):
+        self.kind, self.order = BSPLINE, int(order)
+
+
+class Peskin(DeltaFn):
+    kind = PESKIN
+
+
+class Roma(DeltaFn):
+    kind = ROMA
+
+
+class Cosine(DeltaFn):
+    kind = COSINE
+
+
+class Hat(DeltaFn):
+    kind = HAT
+
+
+class Plan:
+    """Owner of one ``ibk_plan`` (grid geometry + device scratch)."""
+
+    def __init__(self, tag: Mac, domain: Domain, delta: DeltaFn, precision: int = FP64):
+        d = _Delta()
+        d.kind, d.order = delta.kind, delta.order
+        h = _vp()
+        check(lib().ibk_plan_create(ctypes.byref(domain._abi()), tag.tag, tag.refinement,
+                                    d, int(precision), ctypes.byref(h)))
+        self._h = h
+        self.domain = domain
+        self.precision = precision
+        info = GridInfo()
+        check(lib().ibk_plan_info(h, ctypes.byref(info)))
+        self.info = info
+        self.dims = info.dims
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibk_plan_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    def sizes(self):
+        return [int(self.info.size[c]) for c in range(self.dims)]
+
+    def reserve(self, max_points: int):
+        check(lib().ibk_plan_reserve(self._h, int(max_points)))
+
+    def _comp_ptrs(self, arrs):
+        P = (_vp * 3)()
+        for c in range(self.dims):
+            P[c] = _ptr(arrs[c])
+        return P
+
+    def spread(self, n, x, fl, fe, stream=None):
+        check(lib().ibk_spread(self._h, int(n), _ptr(x), _ptr(fl), self._comp_ptrs(fe),
+                               _stream_handle(stream)))
+
+    def interpolate(self, n, x, ue, ul, stream=None):
+        check(lib().ibk_interpolate(self._h, int(n), _ptr(x), self._comp_ptrs(ue), _ptr(ul),
+                                    _stream_handle(stream)))
+
+    def set_profiling(self, enable: bool):
+        check(lib().ibk_plan_set_profiling(self._h, 1 if enable else 0))
+
+    def kernel_stats(self):
+        """{kernel name: (launches, total device ms)}; synchronises."""
+        buf = (KernelStat * 64)()
+        cnt = ctypes.c_int()
+        check(lib().ibk_plan_kernel_stats(self._h, buf, 64, ctypes.byref(cnt)))
+        return {buf[i].name.decode(): (int(buf[i].launches), float(buf[i].total_ms))
+                for i in range(min(cnt.value, 64))}
+
+    def reset_stats(self):
+        check(lib().ibk_plan_reset_stats(self._h))
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        check(lib().ibk_plan_launch_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def sort_keys(self, comp, n, x, keys, stream=None):
+        check(lib().ibk_sort_keys(self._h, int(comp), int(n), _ptr(x), _ptr(keys),
+                                  _stream_handle(stream)))
+
+
+def _points(x, dims):
+    return x.numel() // dims
+
+
+class Spread:
+    """ib::spread{tag, domain, delta} (include/ib/novel.h:193-250)."""
+
+    def __init__(self, tag: Mac, domain: Domain, delta: DeltaFn, precision: int = FP64):
+        self.plan = Plan(tag, domain, delta, precision)
+
+    def __call__(self, *args, stream=None):
+        import torch
+        dims = self.plan.dims
+        if len(args) == 4:                     # (n, x, fl, fe): overwrite fe
+            n, x, fl, fe = args
+        elif len(args) == 3 and isinstance(args[0], int):   # (n, x, fl): new fe
+            n, x, fl = args
+            fe = None
+        elif len(args) == 3:                   # (x, fl, fe)
+            x, fl, fe = args
+            n = _points(x, dims)
+        elif len(args) == 2:                   # (x, fl)
+            x, fl = args
+            n, fe = _points(x, dims), None
+        else:
+            raise TypeError("spread(n, x, fl[, fe]) or spread(x, fl[, fe])")
+        if fe is None:
+            fe = [torch.zeros(s, dtype=torch.float64, device=x.device) for s in self.plan.sizes()]
+        self.plan.spread(n, x, fl, fe, stream)
+        return fe
+
+
+class Interpolate:
+    """ib::interpolate{tag, domain, delta} (include/ib/interpolate.h:88-138)."""
+
+    def __init__(self, tag: Mac, domain: Domain, delta: DeltaFn, precision: int = FP64):
+        self.plan = Plan(tag, domain, delta, precision)
+
+    def __call__(self, *args, stream=None):
+        import torch
+        dims = self.plan.dims
+        if len(args) == 4:                     # (n, x, ue, ul)
+            n, x, ue, ul = args
+        elif len(args) == 3 and isinstance(args[0], int):   # (n, x, ue) -> ul
+            n, x, ue = args
+            ul = None
+        elif len(args) == 3:                   # (x, ue, ul)
+            x, ue, ul = args
+            n = _points(x, dims)
+        elif len(args) == 2:                   # (x, ue) -> ul
+            x, ue = args
+            n, ul = _points(x, dims), None
+        else:
+            raise TypeError("interpolate(n, x, ue[, ul]) or interpolate(x, ue[, ul])")
+        if ul is None:
+            ul = torch.empty(x.numel(), dtype=torch.float64, device=x.device)
+        self.plan.interpolate(n, x, ue, ul, stream)
+        return ul

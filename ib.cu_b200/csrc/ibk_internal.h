@@ -1,0 +1,84 @@
+// Host-side internals shared by the library's translation units.
+#pragma once
+#include <cuda_runtime.h>
+#include <string>
+#include <vector>
+#include "ibk.h"
+#include "ibk_device.cuh"
+
+namespace ibk {
+
+// Launch context handed to every operator implementation.
+struct OpArgs {
+	const GridGeom* g;
+	int n;
+	const double* x;
+	cudaStream_t stream;
+};
+
+struct Plan;
+
+// Implementation entry points (one instantiation per delta / dims / precision).
+using SpreadFn = ibk_status (*)(Plan&, const OpArgs&, const double* fl, CompPtrs fe);
+using InterpFn = ibk_status (*)(Plan&, const OpArgs&, ConstCompPtrs ue, double* ul);
+using KeysFn = ibk_status (*)(Plan&, const OpArgs&, int comp, int* keys);
+
+struct OpTable {
+	SpreadFn spread;
+	InterpFn interp;
+	KeysFn keys;
+};
+
+// Device scratch owned by a plan: grown on demand outside stream capture,
+// released with the plan.
+struct Scratch {
+	void* ptr = nullptr;
+	size_t bytes = 0;
+};
+
+struct TimedLaunch {
+	int stat;            // index into Plan::stats
+	cudaEvent_t start, stop;
+};
+
+struct Plan {
+	GridGeom g{};
+	ibk_grid_info info{};
+	int delta_kind = 0, delta_order = 0, precision = 0;
+	int device = 0;
+	int reserved_points = 0;
+	OpTable ops{};
+	Scratch scratch[8];
+	int* d_status = nullptr;   // device-side error word written by kernel checks
+	// instrumentation
+	long long launches = 0;
+	bool profiling = false;
+	std::vector<ibk_kernel_stat> stats;
+	std::vector<TimedLaunch> pending;
+	std::vector<cudaEvent_t> event_pool;
+};
+
+// Bracket one kernel launch: counts it and, when profiling, records events.
+ibk_status launch_begin(Plan& plan, const char* name, cudaStream_t stream, int& slot);
+ibk_status launch_end(Plan& plan, const char* name, cudaStream_t stream, int slot);
+
+template <typename F>
+ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
+{
+	int slot = -1;
+	ibk_status s = launch_begin(plan, name, stream, slot);
+	if (s != IBK_OK) return s;
+	body();
+	return launch_end(plan, name, stream, slot);
+}
+
+// Returns the table for (kind, order, dims, precision) or nullptr.
+const OpTable* find_ops(int kind, int order, int dims, int precision);
+
+// Grow scratch slot `slot` of the plan to at least `bytes`.
+ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t stream);
+
+ibk_status set_error(ibk_status s, const std::string& msg);
+ibk_status check_launch(const char* what);
+
+} // namespace ibk

@@ -1,0 +1,92 @@
+/*
+ * CPU oracle for the immersed-boundary coupling operators (TEST INFRASTRUCTURE).
+ *
+ * This is a plain-C restatement of sonwell/ib.cu's spread / interpolate path,
+ * used only as the checker by tests/, by __graft_entry__.smoke() and by the
+ * cpu_baseline / --impl reference legs of bench.py.  The product path (the
+ * CUDA library under ib.cu_b200/) never links or calls it.
+ *
+ * Every function cites the reference file:line it restates.  Parity of the
+ * index / weight core is pinned against the reference's own headers compiled
+ * on the host (oracle/ref_bridge.cc -> oracle/_ref/libibref.so) and against
+ * the committed fixtures in tests/golden/.
+ */
+#ifndef IBK_ORACLE_H
+#define IBK_ORACLE_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+enum { IBO_PERIODIC = 0, IBO_SOLID = 1 };
+enum { IBO_TAG_MAC = 0, IBO_TAG_CENTERED = 1 };
+enum { IBO_BSPLINE = 0, IBO_PESKIN = 1, IBO_ROMA = 2, IBO_COSINE = 3, IBO_HAT = 4 };
+enum { IBO_STANDARD_PATTERN = 0, IBO_EVERY_OTHER_PATTERN = 1 };
+
+typedef struct {
+	int dims;                 /* 1..3 */
+	int delta_kind, delta_order;
+	int meshwidths;           /* M */
+	int values;               /* V = M^dims */
+	int pattern;              /* IBO_*_PATTERN */
+	int per_sweep, sweeps;    /* include/ib/novel.h:33-45, :100 */
+	double unit;              /* fd::domain::unit()  (GCD of lengths) */
+	double resolution;        /* refinement / unit */
+	double length[3];
+	int solid[3];
+	/* per component c, per dimension d */
+	int cells[3][3];
+	int points[3][3];
+	double shift[3][3];
+	long long size[3];        /* product of points over d */
+} ibo_geom;
+
+/* fd::grid / fd::discretization geometry (include/fd/grid.h:232-239,
+ * include/fd/discretization.h:113-164, include/fd/domain.h:30-32). */
+int ibo_geometry(int dims, const double* length, const int* solid, int tag,
+                 int refinement, int delta_kind, int delta_order, ibo_geom* g);
+
+/* delta functions phi(r) (include/ib/{bspline,peskin,roma,cosine,hat}.h) */
+double ibo_phi(int delta_kind, int delta_order, double r);
+
+/* stencil offset of entry `e` along each dimension (include/ib/delta.h:97-147) */
+void ibo_pattern(const ibo_geom* g, int e, int* s);
+
+/* ib::sweep::sort (include/ib/sweep.h:64-77): one sort key per point. */
+void ibo_sort_keys(const ibo_geom* g, int comp, int n, const double* x, int* keys);
+
+/* Per-point stencil data for component `comp`:
+ *   base[p*dims+d]   = decompose(key) (include/ib/indexing.h:239-250)
+ *   delta[p*dims+d]  = sweep::difference (include/ib/sweep.h:49-62)
+ *   weights[p*V+e]   = sweep::values, entry order = pattern (sweep.h:98-112)
+ *   sidx[p*V+e]      = spread grid index, -1 = dropped (errors_negative)
+ *   iidx[p*V+e]      = interpolation grid index (clamped)
+ * Any output pointer may be NULL. */
+void ibo_stencil(const ibo_geom* g, int comp, int n, const double* x,
+                 int* base, double* delta, double* weights, int* sidx, int* iidx);
+
+/* ib::novel::spread::operator() (include/ib/novel.h:197-227): the reference
+ * algorithm (stable sort by key, per-sweep segmented sums, per-sweep planes,
+ * combine).  fe[c] is overwritten (or accumulated into when per_sweep == 1,
+ * as the reference does).  fe_abs[c] (optional, may be NULL) receives the sum
+ * of |contribution| per face, the scale of the rounding-error bound. */
+int ibo_spread(const ibo_geom* g, int n, const double* x, const double* f,
+               double* const* fe, double* const* fe_abs);
+
+/* ib::interpolate::operator() (include/ib/interpolate.h:92-115): serial sum
+ * in pattern order.  ul[c*n+p] is overwritten.  ul_abs optional. */
+void ibo_interpolate(const ibo_geom* g, int n, const double* x,
+                     const double* const* ue, double* ul, double* ul_abs);
+
+/* Multi-threaded restatements of the same algorithms (CPU baseline only).
+ * nthreads <= 0 uses every available host thread. */
+int ibo_spread_mt(const ibo_geom* g, int n, const double* x, const double* f,
+                  double* const* fe, int nthreads);
+void ibo_interpolate_mt(const ibo_geom* g, int n, const double* x,
+                        const double* const* ue, double* ul, int nthreads);
+int ibo_max_threads(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

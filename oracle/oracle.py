@@ -1,0 +1,248 @@
+"""ctypes front end of the CPU oracle (TEST INFRASTRUCTURE).
+
+Only tests/, ``__graft_entry__.smoke()`` and bench.py's CPU legs import this
+module, and only as the checker / CPU baseline.  It wraps
+
+* ``libibk_oracle.so`` -- the plain-C restatement of sonwell/ib.cu's
+  spread / interpolate (``ibk_oracle.c``), always buildable with gcc;
+* ``_ref/libibref.so`` -- the reference's own host headers compiled from the
+  reference tree (``ref_bridge.cc``); present only where that tree exists.
+
+Array conventions follow the reference: positions and forces are ``dims x n``
+column blocks (``x[d*n + p]``, include/ib/novel.h:127-128), grid components
+are flat x-fastest vectors (include/ib/indexing.h:27-33).
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+import threading
+
+import numpy as np
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(HERE, "libibk_oracle.so")
+REF_PATH = os.path.join(HERE, "_ref", "libibref.so")
+
+PERIODIC, SOLID = 0, 1
+TAG_MAC, TAG_CENTERED = 0, 1
+BSPLINE, PESKIN, ROMA, COSINE, HAT = 0, 1, 2, 3, 4
+DELTA_NAMES = {"bspline": BSPLINE, "peskin": PESKIN, "roma": ROMA, "cosine": COSINE, "hat": HAT}
+
+_lock = threading.Lock()
+_lib = None
+_ref = None
+
+_dp = ctypes.POINTER(ctypes.c_double)
+_ip = ctypes.POINTER(ctypes.c_int)
+
+
+class Geom(ctypes.Structure):
+    _fields_ = [
+        ("dims", ctypes.c_int),
+        ("delta_kind", ctypes.c_int),
+        ("delta_order", ctypes.c_int),
+        ("meshwidths", ctypes.c_int),
+        ("values", ctypes.c_int),
+        ("pattern", ctypes.c_int),
+        ("per_sweep", ctypes.c_int),
+        ("sweeps", ctypes.c_int),
+        ("unit", ctypes.c_double),
+        ("resolution", ctypes.c_double),
+        ("length", ctypes.c_double * 3),
+        ("solid", ctypes.c_int * 3),
+        ("cells", (ctypes.c_int * 3) * 3),
+        ("points", (ctypes.c_int * 3) * 3),
+        ("shift", (ctypes.c_double * 3) * 3),
+        ("size", ctypes.c_longlong * 3),
+    ]
+
+    def comp_points(self, c):
+        return [self.points[c][d] for d in range(self.dims)]
+
+    def comp_shape(self, c):
+        """numpy shape of component c (reversed: slowest dimension first)."""
+        return tuple(reversed(self.comp_points(c)))
+
+
+def build(force: bool = False) -> None:
+    """Compile the oracle (and, where the reference tree exists, its bridge)."""
+    if force or not os.path.exists(LIB_PATH):
+        subprocess.run(["make", "-s", "-C", HERE, "libibk_oracle.so"], check=True)
+
+
+def build_ref() -> bool:
+    ref_root = os.environ.get("IBK_REFERENCE_ROOT", "/root/reference")
+    if not os.path.isdir(os.path.join(ref_root, "include", "ib")):
+        return os.path.exists(REF_PATH)
+    subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
+    return os.path.exists(REF_PATH)
+
+
+def lib():
+    global _lib
+    with _lock:
+        if _lib is None:
+            build()
+            L = ctypes.CDLL(LIB_PATH)
+            L.ibo_geometry.argtypes = [ctypes.c_int, _dp, _ip, ctypes.c_int, ctypes.c_int,
+                                       ctypes.c_int, ctypes.c_int, ctypes.POINTER(Geom)]
+            L.ibo_geometry.restype = ctypes.c_int
+            L.ibo_phi.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+            L.ibo_phi.restype = ctypes.c_double
+            L.ibo_sort_keys.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, ctypes.c_int, _dp, _ip]
+            L.ibo_stencil.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, ctypes.c_int, _dp,
+                                      _ip, _dp, _dp, _ip, _ip]
+            L.ibo_spread.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, _dp, _dp,
+                                     ctypes.POINTER(_dp), ctypes.POINTER(_dp)]
+            L.ibo_spread.restype = ctypes.c_int
+            L.ibo_spread_mt.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, _dp, _dp,
+                                        ctypes.POINTER(_dp), ctypes.c_int]
+            L.ibo_spread_mt.restype = ctypes.c_int
+            L.ibo_interpolate.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, _dp,
+                                          ctypes.POINTER(_dp), _dp, _dp]
+            L.ibo_interpolate_mt.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, _dp,
+                                             ctypes.POINTER(_dp), _dp, ctypes.c_int]
+            L.ibo_max_threads.restype = ctypes.c_int
+            _lib = L
+    return _lib
+
+
+def ref():
+    """The reference-built bridge, or None where it cannot be built."""
+    global _ref
+    with _lock:
+        if _ref is None:
+            if not os.path.exists(REF_PATH):
+                try:
+                    build_ref()
+                except Exception:
+                    return None
+            if not os.path.exists(REF_PATH):
+                return None
+            R = ctypes.CDLL(REF_PATH)
+            R.ibref_stencil.argtypes = [ctypes.c_int, _dp, _ip, ctypes.c_int, ctypes.c_int,
+                                        ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                        _dp, _ip, _ip, _dp, _dp, _ip, _ip, _dp]
+            R.ibref_stencil.restype = ctypes.c_int
+            R.ibref_phi.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
+            R.ibref_phi.restype = ctypes.c_double
+            R.ibref_domain_unit.argtypes = [ctypes.c_int, _dp]
+            R.ibref_domain_unit.restype = ctypes.c_double
+            _ref = R
+    return _ref
+
+
+def _d(a):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _i(a):
+    return a.ctypes.data_as(_ip) if a is not None else None
+
+
+def geometry(dims, length, solid, tag=TAG_MAC, refinement=16, delta="bspline", order=3) -> Geom:
+    kind = DELTA_NAMES[delta] if isinstance(delta, str) else int(delta)
+    L = np.zeros(3, np.float64)
+    L[:dims] = length
+    S = np.zeros(3, np.int32)
+    S[:dims] = solid
+    g = Geom()
+    rc = lib().ibo_geometry(dims, _d(L), _i(S), tag, refinement, kind, order, ctypes.byref(g))
+    if rc != 0:
+        raise ValueError("unsupported geometry / delta")
+    g._length = L
+    g._solid = S
+    g._tag = tag
+    g._refinement = refinement
+    return g
+
+
+def _as_points(x, dims):
+    x = np.ascontiguousarray(x, dtype=np.float64).reshape(-1)
+    assert x.size % dims == 0
+    return x, x.size // dims
+
+
+def sort_keys(g: Geom, comp: int, x) -> np.ndarray:
+    x, n = _as_points(x, g.dims)
+    keys = np.empty(n, np.int32)
+    lib().ibo_sort_keys(ctypes.byref(g), comp, n, _d(x), _i(keys))
+    return keys
+
+
+def stencil(g: Geom, comp: int, x):
+    """(base[n,dims], delta[n,dims], weights[n,V], spread_idx[n,V], interp_idx[n,V])"""
+    x, n = _as_points(x, g.dims)
+    V = g.values
+    base = np.empty((n, g.dims), np.int32)
+    delta = np.empty((n, g.dims), np.float64)
+    w = np.empty((n, V), np.float64)
+    sidx = np.empty((n, V), np.int32)
+    iidx = np.empty((n, V), np.int32)
+    lib().ibo_stencil(ctypes.byref(g), comp, n, _d(x), _i(base), _d(delta), _d(w), _i(sidx), _i(iidx))
+    return base, delta, w, sidx, iidx
+
+
+def _ptr_array(arrs):
+    P = (_dp * 3)()
+    for c, a in enumerate(arrs):
+        P[c] = _d(a)
+    return P
+
+
+def spread(g: Geom, x, f, fe=None, with_abs=False, threads=1):
+    """Reference spread.  Returns list of flat component arrays (and abs sums)."""
+    x, n = _as_points(x, g.dims)
+    f = np.ascontiguousarray(f, dtype=np.float64).reshape(-1)
+    if fe is None:
+        fe = [np.zeros(int(g.size[c]), np.float64) for c in range(g.dims)]
+    absum = [np.zeros(int(g.size[c]), np.float64) for c in range(g.dims)] if with_abs else None
+    if threads == 1:
+        rc = lib().ibo_spread(ctypes.byref(g), n, _d(x), _d(f), _ptr_array(fe),
+                              _ptr_array(absum) if absum else None)
+    else:
+        rc = lib().ibo_spread_mt(ctypes.byref(g), n, _d(x), _d(f), _ptr_array(fe), threads)
+    if rc != 0:
+        raise MemoryError("oracle spread failed")
+    return (fe, absum) if with_abs else fe
+
+
+def interpolate(g: Geom, x, ue, with_abs=False, threads=1):
+    x, n = _as_points(x, g.dims)
+    ue = [np.ascontiguousarray(u, dtype=np.float64).reshape(-1) for u in ue]
+    ul = np.zeros(g.dims * n, np.float64)
+    ua = np.zeros(g.dims * n, np.float64) if with_abs else None
+    if threads == 1:
+        lib().ibo_interpolate(ctypes.byref(g), n, _d(x), _ptr_array(ue), _d(ul), _d(ua))
+    else:
+        lib().ibo_interpolate_mt(ctypes.byref(g), n, _d(x), _ptr_array(ue), _d(ul), threads)
+    return (ul, ua) if with_abs else ul
+
+
+def max_threads() -> int:
+    return int(lib().ibo_max_threads())
+
+
+def ref_stencil(g: Geom, comp: int, x):
+    """Same outputs as :func:`stencil`, computed by the reference's headers,
+    plus the geometry vector (unit, resolution, cells/points/shift per dim)."""
+    R = ref()
+    if R is None:
+        return None
+    x, n = _as_points(x, g.dims)
+    V = g.values
+    keys = np.empty(n, np.int32)
+    base = np.empty((n, g.dims), np.int32)
+    delta = np.empty((n, g.dims), np.float64)
+    w = np.empty((n, V), np.float64)
+    sidx = np.empty((n, V), np.int32)
+    iidx = np.empty((n, V), np.int32)
+    geo = np.zeros(2 + 3 * g.dims, np.float64)
+    rc = R.ibref_stencil(g.dims, _d(g._length), _i(g._solid), g._tag, g._refinement,
+                         g.delta_kind, g.delta_order, comp, n, _d(x), _i(keys), _i(base),
+                         _d(delta), _d(w), _i(sidx), _i(iidx), _d(geo))
+    if rc != 0:
+        raise ValueError("reference bridge does not cover this configuration")
+    return keys, base, delta, w, sidx, iidx, geo

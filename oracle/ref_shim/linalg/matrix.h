@@ -1,0 +1,3 @@
+/* host shim: see algo/types.h in this directory */
+#pragma once
+#include "algo/types.h"
