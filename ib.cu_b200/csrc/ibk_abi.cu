@@ -79,7 +79,7 @@ ibk_status check_launch(const char* what)
 	return IBK_OK;
 }
 
-ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t stream)
+ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t stream, bool zero)
 {
 	Scratch& s = plan.scratch[slot];
 	if (s.bytes >= bytes) return IBK_OK;
@@ -98,6 +98,10 @@ ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t strea
 	if (e != cudaSuccess) {
 		cudaGetLastError();
 		return set_error(IBK_ERR_OUT_OF_MEMORY, "cudaMalloc of plan scratch failed");
+	}
+	if (zero) {
+		e = cudaMemset(p, 0, want);
+		if (e != cudaSuccess) { cudaFree(p); return set_error(IBK_ERR_CUDA, std::string("cudaMemset: ") + cudaGetErrorString(e)); }
 	}
 	s.ptr = p;
 	s.bytes = want;
@@ -244,6 +248,7 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 		cg.size = size;
 		info.size[c] = size;
 	}
+	plan->tiles = make_tiles(g, tag, info.meshwidths);
 	cudaError_t e = cudaMalloc(&plan->d_status, sizeof(int) * 4);
 	if (e != cudaSuccess) { cudaGetLastError(); delete plan; return set_error(IBK_ERR_OUT_OF_MEMORY, "cudaMalloc failed"); }
 	cudaMemset(plan->d_status, 0, sizeof(int) * 4);

@@ -1,0 +1,154 @@
+// Binning: a counting sort of the Lagrangian points by (tile, reach class).
+//
+// Tiles are boxes of T0 x T1 x T2 grid cells.  A point's home tile is the
+// tile holding its stencil origin for the components staggered by 1/2 along
+// each axis; its reach class records, per axis, whether the stencil of ANY
+// component reaches into the lower (0) or upper (2) neighbouring tile or stays
+// inside (1).  Origins are the reference's exact ones (axis_step), so the
+// classes are exact: the owner-computes spread kernel reads exactly the bins
+// whose points can touch its faces.
+//
+//   bin_count_kernel    key = tile * 3^dims + class; warp-aggregated rank
+//   bin_scan_kernel     exclusive scan of the bin counts (resets the counts)
+//   bin_scatter_kernel  perm[offset[key] + rank] = point
+#pragma once
+#include "ibk_device.cuh"
+
+namespace ibk {
+
+// Exact stencil-node span of every component along axis d, relative to the
+// origin `bh` of the components staggered by 1/2 along d.
+template <int M>
+struct AxisReach {
+	int home;      // clamped origin used for the home tile
+	int node_lo;   // lowest node (unwrapped, relative to the same index space)
+	int node_hi;   // highest node
+};
+
+template <int M, int DIMS>
+__device__ __forceinline__ AxisReach<M> axis_reach(const GridGeom& g, const TileGeom& tg, int d, double x)
+{
+	constexpr int lo_off = (M - 1) >> 1;      // offsets run -lo_off .. M - 1 - lo_off
+	constexpr int hi_off = M - 1 - lo_off;
+	const int half_comp = tg.tag_mac ? (d + 1) % DIMS : 0;
+	const int bh = axis_step<M>(g, g.comp[half_comp], d, x).base;
+	int lo = bh, hi = bh;
+	if (tg.tag_mac) {
+		int bo = axis_step<M>(g, g.comp[d], d, x).base;
+		int diff = bo - bh;
+		if (!g.solid[d]) {
+			const int c = tg.cells[d];
+			if (2 * diff > c) diff -= c;
+			else if (2 * diff < -c) diff += c;
+		}
+		lo = min(bh, bh + diff);
+		hi = max(bh, bh + diff);
+	}
+	AxisReach<M> r;
+	r.home = bh < 0 ? 0 : (bh >= tg.cells[d] ? tg.cells[d] - 1 : bh);
+	r.node_lo = lo - lo_off;
+	r.node_hi = hi + hi_off;
+	return r;
+}
+
+template <int M, int DIMS>
+__global__ void __launch_bounds__(256)
+bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                 int* __restrict__ count, int2* __restrict__ key_rank)
+{
+	const int p = blockIdx.x * blockDim.x + threadIdx.x;
+	const bool active = p < n;
+	int key = 0;
+	if (active) {
+		int tile = 0, cls = 0, ts = 1, cs = 1;
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) {
+			AxisReach<M> r = axis_reach<M, DIMS>(g, tg, d, __ldg(x + (size_t) d * n + p));
+			const int t = r.home / tg.T[d];
+			const int tlo = t * tg.T[d];
+			const int thi = min(tlo + tg.T[d], tg.cells[d]);
+			int c = 1;
+			if (tg.ntiles[d] > 1) c = r.node_lo < tlo ? 0 : (r.node_hi >= thi ? 2 : 1);
+			tile += t * ts;
+			ts *= tg.ntiles[d];
+			cls += c * cs;
+			cs *= 3;
+		}
+		key = tile * tg.nclass + cls;
+	}
+	const unsigned mask = __ballot_sync(0xffffffffu, active);
+	if (!active) return;
+	const int lane = threadIdx.x & 31;
+	const unsigned peers = __match_any_sync(mask, key);
+	const int leader = __ffs(peers) - 1;
+	int base = 0;
+	if (lane == leader) base = atomicAdd(count + key, __popc(peers));
+	base = __shfl_sync(peers, base, leader);
+	const int rank = base + __popc(peers & ((1u << lane) - 1u));
+	key_rank[p] = make_int2(key, rank);
+}
+
+// Single-CTA exclusive scan over num_bins counts; writes offset[0..num_bins]
+// and zeroes the counts for the next call.
+constexpr int kScanThreads = 1024;
+
+__global__ void __launch_bounds__(kScanThreads)
+bin_scan_kernel(int* __restrict__ count, int* __restrict__ offset, int num_bins)
+{
+	__shared__ int warp_sums[32];
+	__shared__ int carry;
+	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+	if (tid == 0) carry = 0;
+	__syncthreads();
+	for (int base = 0; base < num_bins; base += kScanThreads * 4) {
+		const int i0 = base + tid * 4;
+		int v[4];
+#pragma unroll
+		for (int k = 0; k < 4; ++k) v[k] = (i0 + k < num_bins) ? count[i0 + k] : 0;
+		const int local = v[0] + v[1] + v[2] + v[3];
+		int incl = local;
+#pragma unroll
+		for (int o = 1; o < 32; o <<= 1) {
+			int t = __shfl_up_sync(0xffffffffu, incl, o);
+			if (lane >= o) incl += t;
+		}
+		if (lane == 31) warp_sums[warp] = incl;
+		__syncthreads();
+		if (warp == 0) {
+			int s = warp_sums[lane];
+#pragma unroll
+			for (int o = 1; o < 32; o <<= 1) {
+				int t = __shfl_up_sync(0xffffffffu, s, o);
+				if (lane >= o) s += t;
+			}
+			warp_sums[lane] = s;   // inclusive over warps
+		}
+		__syncthreads();
+		const int c0 = carry;
+		int run = c0 + (warp ? warp_sums[warp - 1] : 0) + incl - local;
+#pragma unroll
+		for (int k = 0; k < 4; ++k) {
+			if (i0 + k < num_bins) {
+				offset[i0 + k] = run;
+				count[i0 + k] = 0;
+			}
+			run += v[k];
+		}
+		__syncthreads();
+		if (tid == kScanThreads - 1) carry = c0 + warp_sums[31];
+		__syncthreads();
+	}
+	if (tid == 0) offset[num_bins] = carry;
+}
+
+__global__ void __launch_bounds__(256)
+bin_scatter_kernel(int n, const int2* __restrict__ key_rank, const int* __restrict__ offset,
+                   int* __restrict__ perm)
+{
+	const int p = blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	const int2 kr = key_rank[p];
+	perm[__ldg(offset + kr.x) + kr.y] = p;
+}
+
+} // namespace ibk

@@ -35,6 +35,19 @@ struct GridGeom {
 	CompGeom comp[kMaxDims];
 };
 
+// Tile decomposition of the cell grid (shared by every component).
+struct TileGeom {
+	int T[kMaxDims];        // tile extent in cells
+	int ntiles[kMaxDims];
+	int cells[kMaxDims];
+	int num_tiles;
+	int nclass;             // 3^dims
+	int num_bins;           // num_tiles * nclass
+	int tag_mac;            // fd::mac (1) or fd::centered (0)
+};
+
+__host__ __device__ inline int ipow3(int d) { return d == 1 ? 3 : d == 2 ? 9 : 27; }
+
 struct CompPtrs { double* p[kMaxDims]; };
 struct ConstCompPtrs { const double* p[kMaxDims]; };
 

@@ -43,6 +43,7 @@ struct TimedLaunch {
 
 struct Plan {
 	GridGeom g{};
+	TileGeom tiles{};
 	ibk_grid_info info{};
 	int delta_kind = 0, delta_order = 0, precision = 0;
 	int device = 0;
@@ -72,11 +73,17 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 	return launch_end(plan, name, stream, slot);
 }
 
+// Scratch slots of a plan.
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3 };
+
+// Tile decomposition of a plan's grid for stencil width M.
+TileGeom make_tiles(const GridGeom& g, int tag, int M);
+
 // Returns the table for (kind, order, dims, precision) or nullptr.
 const OpTable* find_ops(int kind, int order, int dims, int precision);
 
 // Grow scratch slot `slot` of the plan to at least `bytes`.
-ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t stream);
+ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t stream, bool zero = false);
 
 ibk_status set_error(ibk_status s, const std::string& msg);
 ibk_status check_launch(const char* what);

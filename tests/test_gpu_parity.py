@@ -19,6 +19,7 @@ pytestmark = pytest.mark.gpu
 GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "golden.npz")
 SPREAD_TOL = 1e-12
 COS_TOL = 1e-13
+FP32C_TOL = 1e-5      # normwise: max|err| <= 1e-5 * max|reference| per component
 
 
 @pytest.fixture(scope="module")
@@ -245,3 +246,81 @@ def test_reference_shaped_python_api(ibk, oracle, cuda):
     assert torch.allclose(ul, torch.ones_like(ul), atol=1e-15)
     for c in range(3):
         assert abs(float(fe[c].sum()) / 16 ** 3 - 2.0) < 1e-12
+
+
+def normwise(got, want):
+    """max |got - want| / max |want| (the accuracy metric of the FP32C form)."""
+    return float(np.abs(got - want).max() / max(np.abs(want).max(), 1e-300))
+
+
+@pytest.mark.parametrize("name", ["single-rbc", "channel"])
+def test_workload_accuracy_fp32c(ibk, oracle, cuda, name):
+    """FP32 weights/products with exact fixed-point (spread) and TwoSum-
+    compensated (interpolate) accumulation vs the FP64 oracle."""
+    from ib_cu_b200 import workloads as W
+    w = W.CONFIGS[name](seed=12)
+    g, plan, ue = _workload_case(ibk, oracle, w, cuda, precision=ibk.FP32C)
+    ul = device_interp(plan, w.x, ue, cuda)
+    want_ul = oracle.interpolate(g, w.x, ue)
+    fe = device_spread(plan, w.x, w.f, cuda)
+    want_fe = oracle.spread(g, w.x, w.f)
+    n = w.n
+    for c in range(3):
+        e = normwise(ul[c * n:(c + 1) * n], want_ul[c * n:(c + 1) * n])
+        assert e <= FP32C_TOL, ("interp", c, e)
+        e = normwise(fe[c], want_fe[c])
+        assert e <= FP32C_TOL, ("spread", c, e)
+        # faces no stencil touches stay exactly zero
+        assert np.all(fe[c][want_fe[c] == 0] == 0)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("lengths,solid,ref", [
+    ([2.0, 1.0, 1.0], [0, 1, 0], 17),   # 34 x 17 x 17 cells: tiles 14+14+6, one, one
+    ([2.0, 1.0, 1.0], [1, 0, 1], 9),    # 18 x 9 x 9: two tiles (14+4) along x
+    ([1.0, 1.0, 1.0], [0, 0, 0], 33),   # 33^3: tiles 14+14+5 on every axis
+    ([0.75, 0.5, 0.875], [0, 0, 0], 2), # 12 x 8 x 14: every axis a single wrapping tile
+])
+def test_tile_decompositions(ibk, oracle, cuda, precision, lengths, solid, ref):
+    rng = np.random.default_rng(21)
+    g = oracle.geometry(3, lengths, solid, oracle.TAG_MAC, ref)
+    plan = plan_for(ibk, 3, lengths, solid, 0, ref, 0, 3, precision)
+    assert [plan.info.cells[0][d] for d in range(3)] == [g.cells[0][d] for d in range(3)]
+    n = 3000
+    x = np.concatenate([rng.uniform(-0.1, l + 0.1, n) for l in lengths])
+    f = rng.normal(size=3 * n)
+    ue = [rng.normal(size=int(g.size[c])) for c in range(3)]
+    ul = device_interp(plan, x, ue, cuda)
+    want, ua = oracle.interpolate(g, x, ue, with_abs=True)
+    fe = device_spread(plan, x, f, cuda)
+    want_fe, fa = oracle.spread(g, x, f, with_abs=True)
+    if precision == 0:
+        check_interp(ul, want, ua)
+        check_spread(fe, want_fe, fa)
+    else:
+        for c in range(3):
+            assert normwise(ul[c * n:(c + 1) * n], want[c * n:(c + 1) * n]) <= FP32C_TOL
+            assert normwise(fe[c], want_fe[c]) <= FP32C_TOL
+
+
+@pytest.mark.parametrize("dims", [2, 3])
+@pytest.mark.parametrize("delta", [("bspline", 2), ("bspline", 3), ("bspline", 5), ("peskin", 0),
+                                   ("roma", 0), ("cosine", 0), ("hat", 0)])
+def test_every_delta_fp32c(ibk, oracle, cuda, dims, delta):
+    rng = np.random.default_rng(200 + dims)
+    L = [1.6, 0.8, 1.2][:dims]
+    solid = [0, 1, 0][:dims]
+    kind = oracle.DELTA_NAMES[delta[0]]
+    g = oracle.geometry(dims, L, solid, oracle.TAG_MAC, 32, kind, delta[1])
+    plan = plan_for(ibk, dims, L, solid, 0, 32, kind, delta[1], ibk.FP32C)
+    n = 2000
+    x = np.concatenate([rng.uniform(0, l, n) for l in L])
+    f = rng.normal(size=dims * n)
+    ue = [rng.normal(size=int(g.size[c])) for c in range(dims)]
+    ul = device_interp(plan, x, ue, cuda)
+    want = oracle.interpolate(g, x, ue)
+    fe = device_spread(plan, x, f, cuda)
+    want_fe = oracle.spread(g, x, f)
+    for c in range(dims):
+        assert normwise(ul[c * n:(c + 1) * n], want[c * n:(c + 1) * n]) <= FP32C_TOL
+        assert normwise(fe[c], want_fe[c]) <= FP32C_TOL
