@@ -214,7 +214,8 @@ def workload_config(w, precision):
             "grid": "x".join(str(int(round(l / 0.025))) for l in w.lengths),
             "boundaries": ["periodic" if b == 0 else "solid" for b in w.boundaries],
             "delta": "bspline<3>", "precision": precision,
-            "l2": "inputs larger than L2" if w.name.startswith("large") else "L2 flushed between steps"}
+            "l2": ("inputs larger than L2" if w.name.startswith(("large", "medium"))
+                   else "L2 flushed between steps")}
 
 
 # ----------------------------------------------------------- GPU arm
@@ -249,7 +250,7 @@ def run_ours(args):
     ue = [torch.randn(s, generator=gen, dtype=torch.float64, device=dev) * W.UM_PER_S for s in sizes]
     fe = [torch.empty(s, dtype=torch.float64, device=dev) for s in sizes]
     ul = torch.empty(3 * n, dtype=torch.float64, device=dev)
-    big = (8 * G) > 4 * L2_BYTES
+    big = (8 * G) > L2_BYTES
     flush = None if big else torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
     def step():
@@ -388,7 +389,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="large-channel",
-                    choices=["large-channel", "channel", "single-rbc"])
+                    choices=["large-channel", "medium-channel", "channel", "single-rbc"])
     ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp64")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)

@@ -215,6 +215,7 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 	g.res = res;
 	for (int d = 0; d < dims; ++d) {
 		g.length[d] = domain->length[d];
+		g.length_safe[d] = domain->length[d] * (1.0 - 0x1p-52);
 		g.solid[d] = domain->boundary[d] != IBK_PERIODIC;
 	}
 	ibk_grid_info& info = plan->info;

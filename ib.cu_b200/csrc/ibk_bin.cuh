@@ -88,57 +88,90 @@ bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	key_rank[p] = make_int2(key, rank);
 }
 
-// Single-CTA exclusive scan over num_bins counts; writes offset[0..num_bins]
-// and zeroes the counts for the next call.
+// Exclusive scan of the bin counts in two launches.  Each CTA owns a chunk
+// of kScanChunk bins: the first kernel writes the chunk totals; the second
+// scans the (few thousand at most) chunk totals in every CTA to get its
+// chunk's offset, scans its chunk, and zeroes the counts for the next call.
 constexpr int kScanThreads = 1024;
+constexpr int kScanChunk = kScanThreads * 4;
 
-__global__ void __launch_bounds__(kScanThreads)
-bin_scan_kernel(int* __restrict__ count, int* __restrict__ offset, int num_bins)
+__device__ __forceinline__ int block_exclusive_scan(int v, int& total)
 {
 	__shared__ int warp_sums[32];
-	__shared__ int carry;
-	const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
-	if (tid == 0) carry = 0;
-	__syncthreads();
-	for (int base = 0; base < num_bins; base += kScanThreads * 4) {
-		const int i0 = base + tid * 4;
-		int v[4];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	int incl = v;
 #pragma unroll
-		for (int k = 0; k < 4; ++k) v[k] = (i0 + k < num_bins) ? count[i0 + k] : 0;
-		const int local = v[0] + v[1] + v[2] + v[3];
-		int incl = local;
+	for (int o = 1; o < 32; o <<= 1) {
+		int t = __shfl_up_sync(0xffffffffu, incl, o);
+		if (lane >= o) incl += t;
+	}
+	if (lane == 31) warp_sums[warp] = incl;
+	__syncthreads();
+	if (warp == 0) {
+		int s = lane < (int) (blockDim.x >> 5) ? warp_sums[lane] : 0;
 #pragma unroll
 		for (int o = 1; o < 32; o <<= 1) {
-			int t = __shfl_up_sync(0xffffffffu, incl, o);
-			if (lane >= o) incl += t;
+			int t = __shfl_up_sync(0xffffffffu, s, o);
+			if (lane >= o) s += t;
 		}
-		if (lane == 31) warp_sums[warp] = incl;
-		__syncthreads();
-		if (warp == 0) {
-			int s = warp_sums[lane];
-#pragma unroll
-			for (int o = 1; o < 32; o <<= 1) {
-				int t = __shfl_up_sync(0xffffffffu, s, o);
-				if (lane >= o) s += t;
-			}
-			warp_sums[lane] = s;   // inclusive over warps
-		}
-		__syncthreads();
-		const int c0 = carry;
-		int run = c0 + (warp ? warp_sums[warp - 1] : 0) + incl - local;
-#pragma unroll
-		for (int k = 0; k < 4; ++k) {
-			if (i0 + k < num_bins) {
-				offset[i0 + k] = run;
-				count[i0 + k] = 0;
-			}
-			run += v[k];
-		}
-		__syncthreads();
-		if (tid == kScanThreads - 1) carry = c0 + warp_sums[31];
-		__syncthreads();
+		warp_sums[lane] = s;
 	}
-	if (tid == 0) offset[num_bins] = carry;
+	__syncthreads();
+	total = warp_sums[31];
+	const int r = (warp ? warp_sums[warp - 1] : 0) + incl - v;
+	__syncthreads();
+	return r;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int num_bins)
+{
+	const int i0 = blockIdx.x * kScanChunk + threadIdx.x * 4;
+	int v = 0;
+	if (i0 + 3 < num_bins) {
+		const int4 q = *reinterpret_cast<const int4*>(count + i0);
+		v = q.x + q.y + q.z + q.w;
+	} else {
+		for (int k = 0; k < 4; ++k) if (i0 + k < num_bins) v += count[i0 + k];
+	}
+	int total;
+	block_exclusive_scan(v, total);
+	if (threadIdx.x == 0) chunk[blockIdx.x] = total;
+}
+
+__global__ void __launch_bounds__(kScanThreads)
+bin_scan_kernel(int* __restrict__ count, const int* __restrict__ chunk, int* __restrict__ offset,
+                int num_bins, int nchunks)
+{
+	// offset of this chunk = sum of the totals of the chunks before it
+	int pre = 0;
+	for (int c = threadIdx.x; c < blockIdx.x; c += kScanThreads) pre += chunk[c];
+	int base_total;
+	{
+		int dummy = block_exclusive_scan(pre, base_total);
+		(void) dummy;
+	}
+	const int i0 = blockIdx.x * kScanChunk + threadIdx.x * 4;
+	int v[4];
+	const bool full = i0 + 3 < num_bins;
+	if (full) {
+		const int4 q = *reinterpret_cast<const int4*>(count + i0);
+		v[0] = q.x; v[1] = q.y; v[2] = q.z; v[3] = q.w;
+	} else {
+		for (int k = 0; k < 4; ++k) v[k] = i0 + k < num_bins ? count[i0 + k] : 0;
+	}
+	int total;
+	int run = base_total + block_exclusive_scan(v[0] + v[1] + v[2] + v[3], total);
+	int o[4];
+#pragma unroll
+	for (int k = 0; k < 4; ++k) { o[k] = run; run += v[k]; }
+	if (full) {
+		*reinterpret_cast<int4*>(offset + i0) = make_int4(o[0], o[1], o[2], o[3]);
+		*reinterpret_cast<int4*>(count + i0) = make_int4(0, 0, 0, 0);
+	} else {
+		for (int k = 0; k < 4; ++k) if (i0 + k < num_bins) { offset[i0 + k] = o[k]; count[i0 + k] = 0; }
+	}
+	if (blockIdx.x == nchunks - 1 && threadIdx.x == kScanThreads - 1) offset[num_bins] = run;
 }
 
 __global__ void __launch_bounds__(256)

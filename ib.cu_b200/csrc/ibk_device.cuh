@@ -30,6 +30,7 @@ struct GridGeom {
 	int dims;
 	int solid[kMaxDims];
 	double length[kMaxDims];
+	double length_safe[kMaxDims]; // length * (1 - 2^-52): below it, t / length < 1
 	double r;                  // resolution = refinement / domain unit
 	double res;                // product of resolutions (1/h^dims), novel.h:101-103
 	CompGeom comp[kMaxDims];
@@ -203,6 +204,16 @@ struct Pattern {
 
 // ------------------------------------------------------ index step ---
 
+// (i + cells) % cells, C remainder semantics (discretization.h:155), without
+// an integer division for the indices that occur here (i in [-cells, 2 cells)).
+__device__ __forceinline__ int wrap_index(int i, int cells) {
+	if (i >= -cells && i < 2 * cells) {
+		const int j = i + cells;
+		return j >= 2 * cells ? j - 2 * cells : (j >= cells ? j - cells : j);
+	}
+	return (i + cells) % cells;
+}
+
 // Per point, per component: the reference's stencil origin ("base", from the
 // clamped sort key, include/ib/indexing.h:10-33,239-250) and fractional offset
 // (sweep::difference, include/ib/sweep.h:49-62), bit-exact.
@@ -217,7 +228,10 @@ template <int M>
 __device__ __forceinline__ AxisStep<M> axis_step(const GridGeom& g, const CompGeom& cg, int d, double x) {
 	const double s = cg.shift[d];
 	double t = __dsub_rn(x, cg.s_over_r[d]);                 // x - s / r
-	if (!g.solid[d]) t = ref_modulo(t, g.length[d]);         // dimension::clamp
+	// dimension::clamp.  For 0 <= t <= length*(1 - 2^-52) the quotient t/L
+	// rounds below 1, floor gives 0 and modulo returns t itself: skip the
+	// division there (same value, bit for bit).
+	if (!g.solid[d] && !(t >= 0.0 && t <= g.length_safe[d])) t = ref_modulo(t, g.length[d]);
 	double u = __dadd_rn(__dmul_rn(t, g.r), s);               // * r + s
 	double diff = __dsub_rn(u, s);                             // units(x) - shift
 	constexpr double rounding = 0.5 * (M & 1);
@@ -225,7 +239,7 @@ __device__ __forceinline__ AxisStep<M> axis_step(const GridGeom& g, const CompGe
 	AxisStep<M> a;
 	a.delta = __dsub_rn((double) i, diff);
 	int j = i;
-	if (!g.solid[d]) j = (i + cg.cells[d]) % cg.cells[d];   // discretization::index
+	if (!g.solid[d]) j = wrap_index(i, cg.cells[d]);         // discretization::index
 	const int solid = g.solid[d];
 	const int w = cg.points[d] + solid;
 	int k = j + solid;
@@ -238,8 +252,7 @@ __device__ __forceinline__ AxisStep<M> axis_step(const GridGeom& g, const CompGe
 // discretization::index for a stencil node (include/fd/discretization.h:151-156)
 __device__ __forceinline__ int node_index(const GridGeom& g, const CompGeom& cg, int d, int i) {
 	if (g.solid[d]) return i;
-	const int c = cg.cells[d];
-	return (i + c) % c;
+	return wrap_index(i, cg.cells[d]);
 }
 
 // ------------------------------------------------- compensated FP32 ---

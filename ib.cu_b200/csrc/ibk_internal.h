@@ -74,7 +74,7 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 }
 
 // Scratch slots of a plan.
-enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3 };
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4 };
 
 // Tile decomposition of a plan's grid for stencil width M.
 TileGeom make_tiles(const GridGeom& g, int tag, int M);

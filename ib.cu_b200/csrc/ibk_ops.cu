@@ -1,5 +1,7 @@
 // Operator implementations and the (delta, dims, precision) dispatch table.
 #include <cstdio>
+#include <cstdint>
+#include <cuda.h>
 #include "ibk_internal.h"
 #include "ibk_direct.cuh"
 #include "ibk_tiled.cuh"
@@ -32,8 +34,14 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
 		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr);
 	})) != IBK_OK) return s;
+	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
+	if ((s = ensure_scratch(plan, kSlotChunk, sizeof(int) * ((size_t) nchunks + 1), a.stream)) != IBK_OK) return s;
+	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
+	if ((s = launch(plan, "bin_chunk_sum_kernel", a.stream, [&] {
+		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins);
+	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scan_kernel", a.stream, [&] {
-		bin_scan_kernel<<<1, kScanThreads, 0, a.stream>>>(count, off, tg.num_bins);
+		bin_scan_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, off, tg.num_bins, nchunks);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scatter_kernel", a.stream, [&] {
 		bin_scatter_kernel<<<nb, 256, 0, a.stream>>>(a.n, kr, off, perm);
@@ -43,13 +51,13 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out
 	return IBK_OK;
 }
 
+// Opt the kernel in to `bytes` of dynamic shared memory (static shared
+// memory counts against the 48 KB default too, so this is always set).
 template <typename K>
 ibk_status set_smem(K kernel, size_t bytes)
 {
-	if (bytes > 48 * 1024) {
-		cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
-		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
-	}
+	cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) bytes);
+	if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaFuncSetAttribute: ") + cudaGetErrorString(e));
 	return IBK_OK;
 }
 
@@ -63,12 +71,60 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off);
 	if (s != IBK_OK) return s;
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
-	const size_t smem = sizeof(acc_t) * (size_t) DIMS * tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
+	const size_t words = PREC == IBK_PRECISION_FP32C ? 2 : 1;   // FP32C: high + low words
+	const size_t smem = words * sizeof(acc_t) * (size_t) tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
 	auto kern = spread_tile_kernel<D, DIMS, PREC>;
 	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
 	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<tg.num_tiles, kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, fe);
+		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, fe);
 	});
+}
+
+// cuTensorMapEncodeTiled through the runtime's driver entry point (no link
+// dependency on libcuda).
+using EncodeTiledFn = CUresult (*)(CUtensorMap*, CUtensorMapDataType, cuuint32_t, void*,
+                                   const cuuint64_t*, const cuuint64_t*, const cuuint32_t*,
+                                   const cuuint32_t*, CUtensorMapInterleave, CUtensorMapSwizzle,
+                                   CUtensorMapL2promotion, CUtensorMapFloatOOBfill);
+
+EncodeTiledFn encode_fn()
+{
+	static EncodeTiledFn fn = [] {
+		void* p = nullptr;
+		cudaDriverEntryPointQueryResult q{};
+		if (cudaGetDriverEntryPoint("cuTensorMapEncodeTiled", &p, cudaEnableDefault, &q) != cudaSuccess ||
+		    q != cudaDriverEntryPointSuccess) {
+			cudaGetLastError();
+			return (EncodeTiledFn) nullptr;
+		}
+		return reinterpret_cast<EncodeTiledFn>(p);
+	}();
+	return fn;
+}
+
+// Tensor map of one FP64 component grid with box `box` (elements per axis).
+// False when the grid or box violates a TMA rule (16-byte base and strides,
+// box rows a multiple of 16 bytes, at most 256 elements per box axis).
+bool grid_tensor_map(CUtensorMap* map, const double* base, const CompGeom& cg, int dims, const int* box)
+{
+	EncodeTiledFn fn = encode_fn();
+	if (!fn || (reinterpret_cast<uintptr_t>(base) & 15) != 0) return false;
+	if ((cg.points[0] * sizeof(double)) % 16 != 0 || (box[0] * sizeof(double)) % 16 != 0) return false;
+	cuuint64_t gdim[3], gstride[2];
+	cuuint32_t bdim[3], estride[3] = {1, 1, 1};
+	cuuint64_t stride = sizeof(double);
+	for (int d = 0; d < dims; ++d) {
+		if (box[d] > 256 || box[d] > cg.points[d]) return false;
+		gdim[d] = (cuuint64_t) cg.points[d];
+		bdim[d] = (cuuint32_t) box[d];
+		if (d > 0) gstride[d - 1] = stride;
+		stride *= (cuuint64_t) cg.points[d];
+	}
+	CUresult r = fn(map, CU_TENSOR_MAP_DATA_TYPE_FLOAT64, (cuuint32_t) dims, const_cast<double*>(base),
+	                gdim, gstride, bdim, estride, CU_TENSOR_MAP_INTERLEAVE_NONE,
+	                CU_TENSOR_MAP_SWIZZLE_NONE, CU_TENSOR_MAP_L2_PROMOTION_L2_128B,
+	                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
+	return r == CUDA_SUCCESS;
 }
 
 template <int KIND, int ORDER, int DIMS, int PREC>
@@ -80,15 +136,24 @@ ibk_status interp_impl(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul
 	int *perm = nullptr, *off = nullptr;
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off);
 	if (s != IBK_OK) return s;
-	using val_t = typename InterpStage<PREC>::val_t;
-	constexpr int HL = Halo<D::M>::lo, HH = Halo<D::M>::hi;
+	constexpr int HL = Halo<D::M>::lo;
+	int box[3] = {1, 1, 1};
 	size_t ev = 1;
-	for (int d = 0; d < DIMS; ++d) ev *= (size_t) (tg.T[d] + HL + HH);
-	const size_t smem = sizeof(val_t) * ev;
+	for (int d = 0; d < DIMS; ++d) {
+		box[d] = region_extent<D::M>(tg.T[d], d);
+		ev *= (size_t) box[d];
+	}
+	const size_t smem = sizeof(double) * ev;
+	// TMA needs every region's x origin (tile origin - halo) on a 16-byte boundary
+	TmaMaps maps{};
+	int use_tma = (tg.T[0] % 2 == 0) && (HL % 2 == 0);
+	for (int c = 0; c < DIMS && use_tma; ++c)
+		use_tma = grid_tensor_map(&maps.map[c], ue.p[c], g.comp[c], DIMS, box);
 	auto kern = interp_tile_kernel<D, DIMS, PREC>;
 	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
 	return launch(plan, "interp_tile_kernel", a.stream, [&] {
-		kern<<<tg.num_tiles, kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, perm, off, ue, ul);
+		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, perm, off, ue, ul,
+		                                                                   maps, use_tma, plan.d_status);
 	});
 }
 

@@ -9,23 +9,26 @@
 //   memory, and writes every face of its tile exactly once (zeros included).
 //   No global atomics, no zero-fill pass: each face is written by one CTA.
 //     FP64:  FP64 shared-memory accumulation.
-//     FP32C: FP32 weights and products accumulated EXACTLY in 32-bit fixed
-//            point with integer shared atomics.  The tile's scale is the
+//     FP32C: FP32 weights and products accumulated EXACTLY in 64-bit fixed
+//            point held as two 32-bit words per face (a signed high part and
+//            an unsigned 16-bit low part, each summed with integer shared
+//            atomics, recombined at the end).  The tile's scale is the
 //            largest power of two for which a sure bound on every face sum
-//            (sum over candidate points of max|w| * res * |F|) fits in 2^30,
-//            so the sum is error-free and order-independent; the only
-//            rounding is each product's quantisation.
+//            (sum over candidate points of max|w| * res * |F|) stays below
+//            2^46, so the sum is error-free and order-independent; the only
+//            rounding is each product's quantisation to 2^-47 of that bound.
 //
-// interp_tile_kernel  -- the CTA stages, per component, the tile plus its
-//   stencil halo in shared memory (periodic halos wrapped, wall halos clamped
-//   exactly as the reference clamps node indices), then every point of the
-//   tile gathers its M^dims nodes from shared memory.
-//     FP64:  FP64 staging, sums in the reference's pattern order (bit-exact).
-//     FP32C: FP32 staging, FP32 weights, x-rows summed with FMA, the rows
-//            combined with TwoProd/TwoSum compensation, FP64 result.
+// interp_tile_kernel  -- one CTA per (tile, component) stages the tile plus
+//   its stencil halo in shared memory: one TMA bulk tensor copy when the box
+//   lies inside the grid, otherwise row copies that wrap periodic halos and
+//   clamp wall halos exactly as the reference clamps node indices.  Every
+//   point of the tile then gathers its M^dims nodes from shared memory.
+//     FP64:  exact weights, sums in the reference's pattern order (bit-exact).
+//     FP32C: FP32 weights applied to the FP64 values, FP64 accumulation.
 #pragma once
 #include "ibk_device.cuh"
 #include "ibk_bin.cuh"
+#include "ibk_tma.cuh"
 
 namespace ibk {
 
@@ -162,6 +165,16 @@ __device__ __forceinline__ int range_lookup(const RangeTable& rt, int item)
 
 // ------------------------------------------------------------ spread ---
 
+// arr[m] for a run-time m without dynamic register indexing.
+template <int M, typename T>
+__device__ __forceinline__ T select_m(const T* arr, int m)
+{
+	T r = arr[0];
+#pragma unroll
+	for (int k = 1; k < M; ++k) r = (m == k) ? arr[k] : r;
+	return r;
+}
+
 template <typename D, int DIMS, int PREC>
 struct SpreadSmem;
 template <typename D, int DIMS>
@@ -169,166 +182,154 @@ struct SpreadSmem<D, DIMS, IBK_PRECISION_FP64> { using acc_t = double; };
 template <typename D, int DIMS>
 struct SpreadSmem<D, DIMS, IBK_PRECISION_FP32C> { using acc_t = int; };
 
+// Fixed-point split: value * scale = hi * 2^16 + lo, lo in [0, 2^16).
+constexpr int kFixLoBits = 16;
+constexpr float kFixLo = 65536.0f;
+
+// Adds s (already scaled) to the face's fixed-point pair.  Tiles with 2^16 or
+// more candidate points could overflow the low words; they accumulate in the
+// high word alone, under a scale 2^17 times smaller (still exact integer
+// sums; coarser quantisation).
+__device__ __forceinline__ void fix_add(int* hi_word, unsigned* lo_word, float s, bool two_word)
+{
+	if (!two_word) {
+		atomicAdd(hi_word, __float2int_rn(s));
+		return;
+	}
+	const float h = floorf(s * (1.0f / kFixLo));
+	const float l = fmaf(-h, kFixLo, s);         // in [0, 2^16]; rounded to the nearest unit below
+	atomicAdd(hi_word, (int) h);
+	atomicAdd(lo_word, __float2uint_rn(l));
+}
+
 template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads)
 spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const double* __restrict__ fl, const int* __restrict__ perm,
                    const int* __restrict__ off, CompPtrs fe)
 {
+	// grid: (tile, component)
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ RangeTable rt;
-	__shared__ float scale_s[kMaxDims];
-	__shared__ float bound_part[kTileThreads / 32][kMaxDims];
+	__shared__ float scale_s;
+	__shared__ float bound_part[kTileThreads / 32];
 
+	const int c = blockIdx.y;
+	const CompGeom& cg = g.comp[c];
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
 	const int TV = T0 * T1 * T2;
-	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw);     // [DIMS][TV]
+	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw);                 // FP32C: high words
+	unsigned* acc_lo = reinterpret_cast<unsigned*>(acc + TV);        // FP32C: low words
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, blockIdx.x, tc);
-	int lo[3], hi[3][3];   // hi[c][d]
+	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
 		lo[d] = tc[d] * tg.T[d];
-#pragma unroll
-		for (int c = 0; c < DIMS; ++c) hi[c][d] = min(lo[d] + tg.T[d], g.comp[c].points[d]);
+		hi[d] = min(lo[d] + tg.T[d], cg.points[d]);
 	}
-	for (int i = threadIdx.x; i < DIMS * TV; i += kTileThreads) acc[i] = (acc_t) 0;
+	for (int i = threadIdx.x; i < TV; i += kTileThreads) acc[i] = (acc_t) 0;
+	if constexpr (PREC == IBK_PRECISION_FP32C)
+		for (int i = threadIdx.x; i < TV; i += kTileThreads) acc_lo[i] = 0u;
 	build_ranges<DIMS>(g, tg, tc, off, rt, true);
 	const int total = rt.pref[rt.count];
+	const bool two_word = total < 65536;
+	const double* __restrict__ fc = fl + (size_t) c * n;
 
-	float scale[kMaxDims] = {1.f, 1.f, 1.f};
+	float scale = 1.0f;
 	if constexpr (PREC == IBK_PRECISION_FP32C) {
-		// Sure bound on every face sum of this tile, per component.
-		float b[kMaxDims] = {0.f, 0.f, 0.f};
-		for (int it = threadIdx.x; it < total; it += kTileThreads) {
-			const int p = __ldg(perm + range_lookup(rt, it));
+		// Sure bound on every face sum of this tile: max|w| * res * sum|F|.
+		float b = 0.f;
+		for (int it = threadIdx.x; it < total; it += kTileThreads)
+			b += fabsf((float) __ldg(fc + __ldg(perm + range_lookup(rt, it))));
 #pragma unroll
-			for (int c = 0; c < DIMS; ++c) b[c] += fabsf((float) __ldg(fl + (size_t) c * n + p));
-		}
-#pragma unroll
-		for (int c = 0; c < DIMS; ++c) {
-#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) b[c] += __shfl_xor_sync(0xffffffffu, b[c], o);
-			if ((threadIdx.x & 31) == 0) bound_part[threadIdx.x >> 5][c] = b[c];
-		}
+		for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
+		if ((threadIdx.x & 31) == 0) bound_part[threadIdx.x >> 5] = b;
 		__syncthreads();
-		if (threadIdx.x < DIMS) {
-			float s = 0.f;
-			for (int w = 0; w < kTileThreads / 32; ++w) s += bound_part[w][threadIdx.x];
-			// bound on |face| in force units: max_w * res * sum|F| (+ slack for
-			// the float sum and the per-term rounding)
-			const float bound = s * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
+		if (threadIdx.x == 0) {
+			float sum = 0.f;
+			for (int w = 0; w < kTileThreads / 32; ++w) sum += bound_part[w];
+			const float bound = sum * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
 			int e;
 			frexpf(bound, &e);                      // bound < 2^e
-			// scale * bound <= 2^29, leaving room for n/2 rounding units
-			scale_s[threadIdx.x] = ldexpf(1.0f, 29 - e);
+			// scale * bound <= 2^46: high words stay below 2^30 plus one unit
+			// per term; low words (< 2^16 each) below 2^32 for < 2^16 terms.
+			scale_s = ldexpf(1.0f, min((two_word ? 46 : 29) - e, 126));
 		}
 		__syncthreads();
-#pragma unroll
-		for (int c = 0; c < DIMS; ++c) scale[c] = scale_s[c];
+		scale = scale_s;
 	} else {
 		__syncthreads();
 	}
 
 	for (int it = threadIdx.x; it < total; it += kTileThreads) {
 		const int p = __ldg(perm + range_lookup(rt, it));
-		double z[DIMS];
+		int lb[DIMS];            // local index of stencil node m is lb[d] + m (in-tile m only)
+		int mlo[DIMS], mhi[DIMS];
+		double dl[DIMS];
+		bool any = true;
 #pragma unroll
-		for (int d = 0; d < DIMS; ++d) z[d] = __ldg(x + (size_t) d * n + p);
-#pragma unroll 1
-		for (int c = 0; c < DIMS; ++c) {
-			const CompGeom& cg = g.comp[c];
-			int loc[DIMS][M];
-			unsigned mask[DIMS];
-			double dl[DIMS];
-			bool any = true;
+		for (int d = 0; d < DIMS; ++d) {
+			AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+			dl[d] = a.delta;
+			unsigned mk = 0;
+			int l0 = 0;
 #pragma unroll
-			for (int d = 0; d < DIMS; ++d) {
-				AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
-				dl[d] = a.delta;
-				unsigned mk = 0;
-#pragma unroll
-				for (int m = 0; m < M; ++m) {
-					int j = node_index(g, cg, d, a.base + m - sh);
-					// spread drops nodes outside [0, points) (errors_negative);
-					// the tile owns [lo, hi)
-					const bool in = j >= lo[d] && j < hi[c][d];
-					loc[d][m] = j - lo[d];
-					mk |= (unsigned) in << m;
-				}
-				mask[d] = mk;
-				any = any && mk;
+			for (int m = 0; m < M; ++m) {
+				// spread drops nodes outside [0, points) (errors_negative);
+				// this tile owns [lo, hi).  The in-tile nodes are consecutive.
+				const int j = node_index(g, cg, d, a.base + m - sh);
+				const bool in = j >= lo[d] && j < hi[d];
+				if (in && !mk) l0 = j - lo[d] - m;
+				mk |= (unsigned) in << m;
 			}
-			if (!any) continue;
-			acc_t* A = acc + c * TV;
-			if constexpr (PREC == IBK_PRECISION_FP64) {
-				const double f = __dmul_rn(g.res, __ldg(fl + (size_t) c * n + p));
-				double w[DIMS][M];
+			lb[d] = l0;
+			mlo[d] = __ffs(mk) - 1;
+			mhi[d] = 32 - __clz(mk);
+			any = any && mk;
+		}
+		if (!any) continue;
+		if constexpr (PREC == IBK_PRECISION_FP64) {
+			const double f = __dmul_rn(g.res, __ldg(fc + p));
+			double w[DIMS][M];
 #pragma unroll
-				for (int d = 0; d < DIMS; ++d)
+			for (int d = 0; d < DIMS; ++d)
 #pragma unroll
-					for (int m = 0; m < M; ++m)
-						w[d][m] = (mask[d] >> m & 1u) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
-				if constexpr (DIMS == 3) {
+				for (int m = 0; m < M; ++m)
+					w[d][m] = (m >= mlo[d] && m < mhi[d]) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
 #pragma unroll
-					for (int m2 = 0; m2 < M; ++m2) {
-						if (!(mask[2] >> m2 & 1u)) continue;
+			for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
+			const int m2lo = DIMS == 3 ? mlo[2] : 0, m2hi = DIMS == 3 ? mhi[2] : 1;
+			for (int m2 = m2lo; m2 < m2hi; ++m2) {
+				const double w2 = DIMS == 3 ? select_m<M>(w[DIMS - 1], m2) : 1.0;
+				for (int m1 = mlo[1]; m1 < mhi[1]; ++m1) {
+					const double w12 = __dmul_rn(select_m<M>(w[1], m1), w2);
+					const int row = ((DIMS == 3 ? (lb[DIMS - 1] + m2) * T1 : 0) + lb[1] + m1) * T0 + lb[0];
 #pragma unroll
-						for (int m1 = 0; m1 < M; ++m1) {
-							if (!(mask[1] >> m1 & 1u)) continue;
-							const double w12 = __dmul_rn(w[1][m1], w[2][m2]);
-							const int row = (loc[2][m2] * T1 + loc[1][m1]) * T0;
-#pragma unroll
-							for (int m0 = 0; m0 < M; ++m0)
-								if (mask[0] >> m0 & 1u)
-									atomicAdd(A + row + loc[0][m0], __dmul_rn(__dmul_rn(w[0][m0], w12), f));
-						}
-					}
-				} else {
-#pragma unroll
-					for (int m1 = 0; m1 < M; ++m1) {
-						if (!(mask[1] >> m1 & 1u)) continue;
-						const int row = loc[1][m1] * T0;
-#pragma unroll
-						for (int m0 = 0; m0 < M; ++m0)
-							if (mask[0] >> m0 & 1u)
-								atomicAdd(A + row + loc[0][m0], __dmul_rn(__dmul_rn(w[0][m0], w[1][m1]), f));
-					}
+					for (int m0 = 0; m0 < M; ++m0)
+						if (m0 >= mlo[0] && m0 < mhi[0])
+							atomicAdd(acc + row + m0, __dmul_rn(w[0][m0], w12));
 				}
-			} else {
-				const float f = (float) (g.res * __ldg(fl + (size_t) c * n + p)) * scale[c];
-				float w[DIMS][M];
+			}
+		} else {
+			const float f = (float) (g.res * __ldg(fc + p)) * scale;
+			float w[DIMS][M];
 #pragma unroll
-				for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
+			for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
 #pragma unroll
-				for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
-				if constexpr (DIMS == 3) {
+			for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
+			const int m2lo = DIMS == 3 ? mlo[2] : 0, m2hi = DIMS == 3 ? mhi[2] : 1;
+			for (int m2 = m2lo; m2 < m2hi; ++m2) {
+				const float w2 = DIMS == 3 ? select_m<M>(w[DIMS - 1], m2) : 1.0f;
+				for (int m1 = mlo[1]; m1 < mhi[1]; ++m1) {
+					const float w12 = select_m<M>(w[1], m1) * w2;
+					const int row = ((DIMS == 3 ? (lb[DIMS - 1] + m2) * T1 : 0) + lb[1] + m1) * T0 + lb[0];
 #pragma unroll
-					for (int m2 = 0; m2 < M; ++m2) {
-						if (!(mask[2] >> m2 & 1u)) continue;
-#pragma unroll
-						for (int m1 = 0; m1 < M; ++m1) {
-							if (!(mask[1] >> m1 & 1u)) continue;
-							const float w12 = w[1][m1] * w[2][m2];
-							const int row = (loc[2][m2] * T1 + loc[1][m1]) * T0;
-#pragma unroll
-							for (int m0 = 0; m0 < M; ++m0)
-								if (mask[0] >> m0 & 1u)
-									atomicAdd(A + row + loc[0][m0], __float2int_rn(w[0][m0] * w12));
-						}
-					}
-				} else {
-#pragma unroll
-					for (int m1 = 0; m1 < M; ++m1) {
-						if (!(mask[1] >> m1 & 1u)) continue;
-						const int row = loc[1][m1] * T0;
-#pragma unroll
-						for (int m0 = 0; m0 < M; ++m0)
-							if (mask[0] >> m0 & 1u)
-								atomicAdd(A + row + loc[0][m0], __float2int_rn(w[0][m0] * w[1][m1]));
-					}
+					for (int m0 = 0; m0 < M; ++m0)
+						if (m0 >= mlo[0] && m0 < mhi[0])
+							fix_add(acc + row + m0, acc_lo + row + m0, w[0][m0] * w12, two_word);
 				}
 			}
 		}
@@ -336,35 +337,27 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	__syncthreads();
 
 	// every face of the tile, written once
-#pragma unroll 1
-	for (int c = 0; c < DIMS; ++c) {
-		const CompGeom& cg = g.comp[c];
-		const acc_t* A = acc + c * TV;
-		const int e0 = hi[c][0] - lo[0];
-		const int e1 = hi[c][1] - lo[1];
-		const int e2 = DIMS == 3 ? hi[c][2] - lo[2] : 1;
-		const double inv = 1.0 / (double) scale[c];
-		double* __restrict__ out = fe.p[c];
-		const int rows = e1 * e2;
-		for (int i = threadIdx.x; i < rows * T0; i += kTileThreads) {
-			const int l0 = i % T0;
-			const int r = i / T0;
-			if (l0 >= e0) continue;
-			const int l1 = r % e1, l2 = r / e1;
-			const size_t gi = (size_t) (lo[0] + l0) + (size_t) cg.points[0] *
-				((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
-			const acc_t v = A[(l2 * T1 + l1) * T0 + l0];
-			if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = v;
-			else out[gi] = (double) v * inv;
+	const int e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = DIMS == 3 ? hi[2] - lo[2] : 1;
+	const double inv = 1.0 / (double) scale;
+	double* __restrict__ out = fe.p[c];
+	for (int i = threadIdx.x; i < e1 * e2 * T0; i += kTileThreads) {
+		const int l0 = i % T0;
+		const int r = i / T0;
+		if (l0 >= e0) continue;
+		const int l1 = r % e1, l2 = r / e1;
+		const size_t gi = (size_t) (lo[0] + l0) + (size_t) cg.points[0] *
+			((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
+		const int li = (l2 * T1 + l1) * T0 + l0;
+		if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = acc[li];
+		else {
+			const long long q = two_word ?
+				(long long) acc[li] * (1LL << kFixLoBits) + (long long) acc_lo[li] : (long long) acc[li];
+			out[gi] = (double) q * inv;
 		}
 	}
 }
 
 // ------------------------------------------------------------ interp ---
-
-template <int PREC> struct InterpStage;
-template <> struct InterpStage<IBK_PRECISION_FP64> { using val_t = double; };
-template <> struct InterpStage<IBK_PRECISION_FP32C> { using val_t = float; };
 
 // Halo of the staged region around the tile, per side.
 template <int M> struct Halo {
@@ -372,165 +365,182 @@ template <int M> struct Halo {
 	static constexpr int hi = 1 + M / 2;
 };
 
+// Fold a region coordinate onto the grid: wrap periodic axes, clamp walls.
+__device__ __forceinline__ int fold(const GridGeom& g, const CompGeom& cg, int d, int v)
+{
+	const int pd = cg.points[d];
+	if (g.solid[d]) return v < 0 ? 0 : (v >= pd ? pd - 1 : v);
+	if (v < 0 || v >= pd) v = wrap_index(v, cg.cells[d]);
+	return v;
+}
+
+// Staged-region geometry shared by host and device: the x extent is padded to
+// an even count so a TMA box row is a multiple of 16 bytes.
+template <int M>
+__host__ __device__ inline int region_extent(int T, int d)
+{
+	const int e = T + Halo<M>::lo + Halo<M>::hi;
+	return d == 0 ? (e + 1) & ~1 : e;
+}
+
 template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads)
+__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
 interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const int* __restrict__ perm, const int* __restrict__ off,
-                   ConstCompPtrs ue, double* __restrict__ ul)
+                   ConstCompPtrs ue, double* __restrict__ ul,
+                   const __grid_constant__ TmaMaps maps, int use_tma, int* status)
 {
-	using val_t = typename InterpStage<PREC>::val_t;
+	// grid: (tile, component)
 	using P = Pattern<D::M, DIMS, D::every_other>;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
-	constexpr int HL = Halo<M>::lo, HH = Halo<M>::hi;
-	extern __shared__ __align__(16) unsigned char smem_raw[];
-	val_t* reg = reinterpret_cast<val_t*>(smem_raw);
+	constexpr int HL = Halo<M>::lo;
+	extern __shared__ __align__(128) unsigned char smem_raw[];
+	double* reg = reinterpret_cast<double*>(smem_raw);
+	__shared__ __align__(8) uint64_t bar;
 
 	const int t = blockIdx.x;
+	const int c = blockIdx.y;
 	const int start = __ldg(off + t * tg.nclass);
 	const int end = __ldg(off + (t + 1) * tg.nclass);
 	if (start == end) return;
+	const CompGeom& cg = g.comp[c];
+	const double* __restrict__ u = ue.p[c];
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, t, tc);
-	int rlo[3], E[3];
+	int rlo[3] = {0, 0, 0}, E[3] = {1, 1, 1};
+	bool interior = use_tma != 0;
 #pragma unroll
-	for (int d = 0; d < 3; ++d) {
-		rlo[d] = d < DIMS ? tc[d] * tg.T[d] - HL : 0;
-		E[d] = d < DIMS ? tg.T[d] + HL + HH : 1;
+	for (int d = 0; d < DIMS; ++d) {
+		rlo[d] = tc[d] * tg.T[d] - HL;
+		E[d] = region_extent<M>(tg.T[d], d);
+		interior = interior && rlo[d] >= 0 && rlo[d] + E[d] <= cg.points[d];
 	}
-	const int EV = E[0] * E[1] * E[2];
-
-#pragma unroll 1
-	for (int c = 0; c < DIMS; ++c) {
-		const CompGeom& cg = g.comp[c];
-		const double* __restrict__ u = ue.p[c];
-		// stage the region: wrap periodic, clamp solid (interpolate.h:16-22)
-		for (int i = threadIdx.x; i < EV; i += kTileThreads) {
-			int l0 = i % E[0];
-			int r = i / E[0];
-			int l1 = r % E[1], l2 = r / E[1];
-			int gc[3] = {rlo[0] + l0, rlo[1] + l1, rlo[2] + l2};
-			size_t gi = 0, stride = 1;
-#pragma unroll
-			for (int d = 0; d < DIMS; ++d) {
-				int v = gc[d];
-				const int pd = cg.points[d];
-				if (g.solid[d]) v = v < 0 ? 0 : (v >= pd ? pd - 1 : v);
-				else { v %= cg.cells[d]; if (v < 0) v += cg.cells[d]; }
-				gi += (size_t) v * stride;
-				stride *= (size_t) pd;
-			}
-			reg[i] = (val_t) __ldg(u + gi);
+	if (interior) {
+		// the region lies inside the grid: one bulk tensor copy
+		if (threadIdx.x == 0) mbar_init(&bar, 1);
+		__syncthreads();
+		if (threadIdx.x == 0) {
+			mbar_arrive_expect_tx(&bar, (unsigned) (sizeof(double) * E[0] * E[1] * E[2]));
+			if constexpr (DIMS == 3) tma_load_3d(reg, &maps.map[c], rlo[0], rlo[1], rlo[2], &bar);
+			else tma_load_2d(reg, &maps.map[c], rlo[0], rlo[1], &bar);
+		}
+		if (!mbar_wait_bounded(&bar, 0, status)) return;
+	} else {
+		// domain edge: wrap periodic, clamp solid (interpolate.h:16-22), row by row
+		const int rows = E[1] * E[2];
+		const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+		for (int r = warp; r < rows; r += kTileThreads / 32) {
+			const int l1 = r % E[1], l2 = r / E[1];
+			size_t rb = (size_t) fold(g, cg, 1, rlo[1] + l1);
+			if (DIMS == 3) rb += (size_t) cg.points[1] * (size_t) fold(g, cg, 2, rlo[2] + l2);
+			rb *= (size_t) cg.points[0];
+			double* dst = reg + (size_t) r * E[0];
+			for (int l0 = lane; l0 < E[0]; l0 += 32)
+				dst[l0] = __ldg(u + rb + fold(g, cg, 0, rlo[0] + l0));
 		}
 		__syncthreads();
-		for (int it = start + threadIdx.x; it < end; it += kTileThreads) {
-			const int p = __ldg(perm + it);
-			double z[DIMS];
+	}
+	double* __restrict__ out = ul + (size_t) c * n;
+	for (int it = start + threadIdx.x; it < end; it += kTileThreads) {
+		const int p = __ldg(perm + it);
+		int loc[DIMS];          // local index of the stencil's first node
+		double dl[DIMS];
+		bool inside = true;
 #pragma unroll
-			for (int d = 0; d < DIMS; ++d) z[d] = __ldg(x + (size_t) d * n + p);
-			int loc[DIMS];          // local index of the stencil's first node
-			double dl[DIMS];
-			bool inside = true;
-#pragma unroll
-			for (int d = 0; d < DIMS; ++d) {
-				AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
-				dl[d] = a.delta;
-				int b = a.base;
-				if (!g.solid[d] && tg.ntiles[d] > 1) {
-					const int cells = cg.cells[d];
-					int diff = b - (rlo[d] + HL);
-					if (2 * diff > cells) b -= cells;
-					else if (2 * diff < -cells) b += cells;
-				}
-				const int l = b - sh - rlo[d];
-				loc[d] = l;
-				inside = inside && l >= 0 && l + M <= E[d];
+		for (int d = 0; d < DIMS; ++d) {
+			AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+			dl[d] = a.delta;
+			int b = a.base;
+			if (!g.solid[d] && tg.ntiles[d] > 1) {
+				const int cells = cg.cells[d];
+				const int diff = b - (rlo[d] + HL);
+				if (2 * diff > cells) b -= cells;
+				else if (2 * diff < -cells) b += cells;
 			}
-			double v;
-			if (inside) {
-				if constexpr (PREC == IBK_PRECISION_FP64) {
-					double w[DIMS][M];
-#pragma unroll
-					for (int d = 0; d < DIMS; ++d)
-#pragma unroll
-						for (int m = 0; m < M; ++m) w[d][m] = D::phi64(__dadd_rn(dl[d], (double) (m - sh)));
-					const int base = DIMS == 3 ? (loc[2] * E[1] + loc[1]) * E[0] + loc[0] : loc[1] * E[0] + loc[0];
-					v = 0.0;
-#pragma unroll
-					for (int e = 0; e < P::V; ++e) {
-						const int m0 = P::m(e, 0), m1 = P::m(e, 1);
-						double wt;
-						int k;
-						if constexpr (DIMS == 3) {
-							const int m2 = P::m(e, 2);
-							wt = __dmul_rn(w[0][m0], __dmul_rn(w[1][m1], w[2][m2]));
-							k = base + (m2 * E[1] + m1) * E[0] + m0;
-						} else {
-							wt = __dmul_rn(w[0][m0], w[1][m1]);
-							k = base + m1 * E[0] + m0;
-						}
-						v = __dadd_rn(v, __dmul_rn(wt, (double) reg[k]));   // interpolate.h:71-72
-					}
-				} else {
-					float w[DIMS][M];
-#pragma unroll
-					for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
-					const int base = DIMS == 3 ? (loc[2] * E[1] + loc[1]) * E[0] + loc[0] : loc[1] * E[0] + loc[0];
-					float s = 0.f, comp = 0.f;
-					constexpr int R = DIMS == 3 ? M * M : M;
-#pragma unroll
-					for (int r = 0; r < R; ++r) {
-						const int m1 = r % M, m2 = r / M;
-						const float* row = reinterpret_cast<const float*>(reg) + base +
-							(DIMS == 3 ? (m2 * E[1] + m1) * E[0] : m1 * E[0]);
-						float rs = 0.f;
-#pragma unroll
-						for (int m0 = 0; m0 < M; ++m0) rs = fmaf(w[0][m0], row[m0], rs);
-						const float wr = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-						// TwoProd (FMA) + TwoSum (Knuth)
-						const float pr = wr * rs;
-						const float pe = fmaf(wr, rs, -pr);
-						float ns, se;
-						two_sum(s, pr, ns, se);
-						s = ns;
-						comp += pe + se;
-					}
-					v = (double) s + (double) comp;
-				}
-			} else {
-				// stencil leaves the staged region: exact global gather
-				int gidx[DIMS][M];
+			const int l = b - sh - rlo[d];
+			loc[d] = l;
+			inside = inside && l >= 0 && l + M <= E[d];
+		}
+		double v;
+		if (inside) {
+			const int base = DIMS == 3 ? (loc[2] * E[1] + loc[1]) * E[0] + loc[0] : loc[1] * E[0] + loc[0];
+			if constexpr (PREC == IBK_PRECISION_FP64) {
 				double w[DIMS][M];
 #pragma unroll
-				for (int d = 0; d < DIMS; ++d) {
-					AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
+				for (int d = 0; d < DIMS; ++d)
 #pragma unroll
-					for (int m = 0; m < M; ++m) {
-						int j = node_index(g, cg, d, a.base + m - sh);
-						const int pd = cg.points[d];
-						gidx[d][m] = j < 0 ? 0 : (j >= pd ? pd - 1 : j);
-						w[d][m] = D::phi64(__dadd_rn(a.delta, (double) (m - sh)));
-					}
-				}
+					for (int m = 0; m < M; ++m) w[d][m] = D::phi64(__dadd_rn(dl[d], (double) (m - sh)));
 				v = 0.0;
 #pragma unroll
 				for (int e = 0; e < P::V; ++e) {
 					const int m0 = P::m(e, 0), m1 = P::m(e, 1);
 					double wt;
-					long long k;
+					int k;
 					if constexpr (DIMS == 3) {
 						const int m2 = P::m(e, 2);
 						wt = __dmul_rn(w[0][m0], __dmul_rn(w[1][m1], w[2][m2]));
-						k = gidx[0][m0] + (long long) cg.points[0] * (gidx[1][m1] + (long long) cg.points[1] * gidx[2][m2]);
+						k = base + (m2 * E[1] + m1) * E[0] + m0;
 					} else {
 						wt = __dmul_rn(w[0][m0], w[1][m1]);
-						k = gidx[0][m0] + (long long) cg.points[0] * gidx[1][m1];
+						k = base + m1 * E[0] + m0;
 					}
-					v = __dadd_rn(v, __dmul_rn(wt, __ldg(u + k)));
+					v = __dadd_rn(v, __dmul_rn(wt, reg[k]));   // interpolate.h:71-72
+				}
+			} else {
+				// FP32 delta weights applied to the FP64 values, FP64 accumulation
+				float w32[DIMS][M];
+				double w[DIMS][M];
+#pragma unroll
+				for (int d = 0; d < DIMS; ++d) {
+					weights32<D>((float) dl[d], w32[d]);
+#pragma unroll
+					for (int m = 0; m < M; ++m) w[d][m] = (double) w32[d][m];
+				}
+				v = 0.0;
+				constexpr int R = DIMS == 3 ? M * M : M;
+#pragma unroll
+				for (int r = 0; r < R; ++r) {
+					const int m1 = r % M, m2 = r / M;
+					const double* row = reg + base + (DIMS == 3 ? (m2 * E[1] + m1) * E[0] : m1 * E[0]);
+					double rs = 0.0;
+#pragma unroll
+					for (int m0 = 0; m0 < M; ++m0) rs = fma(w[0][m0], row[m0], rs);
+					v = fma(DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1], rs, v);
 				}
 			}
-			ul[(size_t) c * n + p] = v;
+		} else {
+			// stencil leaves the staged region: exact global gather
+			int gidx[DIMS][M];
+			double w[DIMS][M];
+#pragma unroll
+			for (int d = 0; d < DIMS; ++d) {
+				AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+#pragma unroll
+				for (int m = 0; m < M; ++m) {
+					const int j = node_index(g, cg, d, a.base + m - sh);
+					const int pd = cg.points[d];
+					gidx[d][m] = j < 0 ? 0 : (j >= pd ? pd - 1 : j);
+					w[d][m] = D::phi64(__dadd_rn(a.delta, (double) (m - sh)));
+				}
+			}
+			v = 0.0;
+#pragma unroll
+			for (int e = 0; e < P::V; ++e) {
+				const int m0 = P::m(e, 0), m1 = P::m(e, 1);
+				double wt;
+				long long k;
+				if constexpr (DIMS == 3) {
+					const int m2 = P::m(e, 2);
+					wt = __dmul_rn(w[0][m0], __dmul_rn(w[1][m1], w[2][m2]));
+					k = gidx[0][m0] + (long long) cg.points[0] * (gidx[1][m1] + (long long) cg.points[1] * gidx[2][m2]);
+				} else {
+					wt = __dmul_rn(w[0][m0], w[1][m1]);
+					k = gidx[0][m0] + (long long) cg.points[0] * gidx[1][m1];
+				}
+				v = __dadd_rn(v, __dmul_rn(wt, __ldg(u + k)));
+			}
 		}
-		__syncthreads();
+		out[p] = v;
 	}
 }
 

@@ -203,6 +203,15 @@ def large_channel(seed: int = 0) -> Workload:
     return w
 
 
+def medium_channel(seed: int = 0) -> Workload:
+    """64 x 32 x 64 um channel, MAC 256x128x256, 412 RBCs + 750 platelets
+    (1/8 of the large channel; its fields still exceed L2)."""
+    w = channel(seed, box_um=(64.0, 32.0, 64.0), refinement=128, n_rbc=412, n_plt=750,
+                name="medium-channel-256x128x256")
+    w.velocity = "gaussian"
+    return w
+
+
 GRID_SIDES = (32, 48, 64, 96, 128)
 CELL_CHOICES = (("rbc", 864), ("rbc", 2210), ("rbc", 8832), ("platelet", 386), ("platelet", 1552))
 
@@ -254,5 +263,6 @@ def grid_velocity(w: Workload, sizes, points, rng: np.random.Generator | None = 
 CONFIGS = {
     "single-rbc": single_rbc,
     "channel": channel,
+    "medium-channel": medium_channel,
     "large-channel": large_channel,
 }
