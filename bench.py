@@ -265,6 +265,7 @@ def run_ours(args):
     for _ in range(max(args.warmup, 3)):
         step()
     barrier()
+    plan.check()
 
     # ---- timed region: device-resident inputs, CUDA events on the stream
     launches0 = plan.launch_count()

@@ -43,7 +43,7 @@ ABI_SYMBOLS = (
     "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
     "ibk_spread", "ibk_interpolate", "ibk_sort_keys",
     "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
-    "ibk_plan_launch_count",
+    "ibk_plan_launch_count", "ibk_plan_check",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
 
@@ -109,12 +109,14 @@ def lib() -> ctypes.CDLL:
                                             ctypes.POINTER(ctypes.c_int)]
         L.ibk_plan_reset_stats.argtypes = [_vp]
         L.ibk_plan_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.ibk_plan_check.argtypes = [_vp]
         L.ibk_last_error.restype = ctypes.c_char_p
         L.ibk_status_string.restype = ctypes.c_char_p
         L.ibk_status_string.argtypes = [ctypes.c_int]
         for name in ("ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
                      "ibk_spread", "ibk_interpolate", "ibk_sort_keys", "ibk_plan_set_profiling",
-                     "ibk_plan_kernel_stats", "ibk_plan_reset_stats", "ibk_plan_launch_count"):
+                     "ibk_plan_kernel_stats", "ibk_plan_reset_stats", "ibk_plan_launch_count",
+                     "ibk_plan_check"):
             getattr(L, name).restype = ctypes.c_int
         _lib = L
     return _lib
@@ -279,6 +281,10 @@ class Plan:
 
     def reset_stats(self):
         check(lib().ibk_plan_reset_stats(self._h))
+
+    def check(self):
+        """Raise if a kernel's own device-side check tripped since the last call."""
+        check(lib().ibk_plan_check(self._h))
 
     def launch_count(self) -> int:
         v = ctypes.c_longlong()

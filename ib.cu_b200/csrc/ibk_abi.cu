@@ -365,6 +365,19 @@ ibk_status ibk_plan_launch_count(ibk_plan handle, long long* launches)
 	return IBK_OK;
 }
 
+ibk_status ibk_plan_check(ibk_plan handle)
+{
+	Plan* plan = reinterpret_cast<Plan*>(handle);
+	if (!plan) return set_error(IBK_ERR_INVALID_ARGUMENT, "null plan");
+	int st[4] = {0, 0, 0, 0};
+	cudaError_t e = cudaMemcpy(st, plan->d_status, sizeof(st), cudaMemcpyDeviceToHost);
+	if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemcpy: ") + cudaGetErrorString(e));
+	if (st[0] == 0) return IBK_OK;
+	cudaMemset(plan->d_status, 0, sizeof(st));
+	return set_error(IBK_ERR_DEVICE_CHECK, st[0] == 1 ? "a bounded device wait timed out" :
+	                 "a TMA precondition failed on the device (staged by plain loads instead)");
+}
+
 const char* ibk_last_error(void) { return g_last_error.c_str(); }
 
 const char* ibk_status_string(ibk_status s)

@@ -143,7 +143,7 @@ ibk_status interp_impl(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul
 		box[d] = region_extent<D::M>(tg.T[d], d);
 		ev *= (size_t) box[d];
 	}
-	const size_t smem = sizeof(double) * ev;
+	const size_t smem = sizeof(double) * ev + 128;   // + slack for 128-byte alignment
 	// TMA needs every region's x origin (tile origin - halo) on a 16-byte boundary
 	TmaMaps maps{};
 	int use_tma = (tg.T[0] % 2 == 0) && (HL % 2 == 0);

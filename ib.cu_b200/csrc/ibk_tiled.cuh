@@ -266,7 +266,7 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 
 	for (int it = threadIdx.x; it < total; it += kTileThreads) {
 		const int p = __ldg(perm + range_lookup(rt, it));
-		int lb[DIMS];            // local index of stencil node m is lb[d] + m (in-tile m only)
+		int loc[DIMS][M];        // local (in-tile) index of node m; valid where in-tile
 		int mlo[DIMS], mhi[DIMS];
 		double dl[DIMS];
 		bool any = true;
@@ -275,17 +275,15 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
 			dl[d] = a.delta;
 			unsigned mk = 0;
-			int l0 = 0;
 #pragma unroll
 			for (int m = 0; m < M; ++m) {
 				// spread drops nodes outside [0, points) (errors_negative);
-				// this tile owns [lo, hi).  The in-tile nodes are consecutive.
+				// this tile owns [lo, hi).  The in-tile nodes form one run of
+				// m (their indices may wrap when the tile spans the axis).
 				const int j = node_index(g, cg, d, a.base + m - sh);
-				const bool in = j >= lo[d] && j < hi[d];
-				if (in && !mk) l0 = j - lo[d] - m;
-				mk |= (unsigned) in << m;
+				loc[d][m] = j - lo[d];
+				mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
 			}
-			lb[d] = l0;
 			mlo[d] = __ffs(mk) - 1;
 			mhi[d] = 32 - __clz(mk);
 			any = any && mk;
@@ -304,13 +302,14 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			const int m2lo = DIMS == 3 ? mlo[2] : 0, m2hi = DIMS == 3 ? mhi[2] : 1;
 			for (int m2 = m2lo; m2 < m2hi; ++m2) {
 				const double w2 = DIMS == 3 ? select_m<M>(w[DIMS - 1], m2) : 1.0;
+				const int plane = DIMS == 3 ? select_m<M>(loc[DIMS - 1], m2) * T1 : 0;
 				for (int m1 = mlo[1]; m1 < mhi[1]; ++m1) {
 					const double w12 = __dmul_rn(select_m<M>(w[1], m1), w2);
-					const int row = ((DIMS == 3 ? (lb[DIMS - 1] + m2) * T1 : 0) + lb[1] + m1) * T0 + lb[0];
+					const int row = (plane + select_m<M>(loc[1], m1)) * T0;
 #pragma unroll
 					for (int m0 = 0; m0 < M; ++m0)
 						if (m0 >= mlo[0] && m0 < mhi[0])
-							atomicAdd(acc + row + m0, __dmul_rn(w[0][m0], w12));
+							atomicAdd(acc + row + loc[0][m0], __dmul_rn(w[0][m0], w12));
 				}
 			}
 		} else {
@@ -323,13 +322,14 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			const int m2lo = DIMS == 3 ? mlo[2] : 0, m2hi = DIMS == 3 ? mhi[2] : 1;
 			for (int m2 = m2lo; m2 < m2hi; ++m2) {
 				const float w2 = DIMS == 3 ? select_m<M>(w[DIMS - 1], m2) : 1.0f;
+				const int plane = DIMS == 3 ? select_m<M>(loc[DIMS - 1], m2) * T1 : 0;
 				for (int m1 = mlo[1]; m1 < mhi[1]; ++m1) {
 					const float w12 = select_m<M>(w[1], m1) * w2;
-					const int row = ((DIMS == 3 ? (lb[DIMS - 1] + m2) * T1 : 0) + lb[1] + m1) * T0 + lb[0];
+					const int row = (plane + select_m<M>(loc[1], m1)) * T0;
 #pragma unroll
 					for (int m0 = 0; m0 < M; ++m0)
 						if (m0 >= mlo[0] && m0 < mhi[0])
-							fix_add(acc + row + m0, acc_lo + row + m0, w[0][m0] * w12, two_word);
+							fix_add(acc + row + loc[0][m0], acc_lo + row + loc[0][m0], w[0][m0] * w12, two_word);
 				}
 			}
 		}
@@ -394,8 +394,10 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	using P = Pattern<D::M, DIMS, D::every_other>;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	constexpr int HL = Halo<M>::lo;
-	extern __shared__ __align__(128) unsigned char smem_raw[];
-	double* reg = reinterpret_cast<double*>(smem_raw);
+	// The region pointer is aligned to 128 bytes by hand (TMA destination);
+	// the launch adds 128 bytes of slack for it.
+	extern __shared__ __align__(16) unsigned char interp_smem[];
+	double* reg = reinterpret_cast<double*>(interp_smem + ((128u - (smem_addr(interp_smem) & 127u)) & 127u));
 	__shared__ __align__(8) uint64_t bar;
 
 	const int t = blockIdx.x;
@@ -414,6 +416,13 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 		rlo[d] = tc[d] * tg.T[d] - HL;
 		E[d] = region_extent<M>(tg.T[d], d);
 		interior = interior && rlo[d] >= 0 && rlo[d] + E[d] <= cg.points[d];
+	}
+	// self-check of the TMA preconditions: 128-byte destination, x origin
+	// on a 16-byte boundary; a violation is recorded and the region staged
+	// by plain loads instead
+	if (interior && (((smem_addr(reg) & 127u) != 0u) || (rlo[0] & 1) != 0)) {
+		if (threadIdx.x == 0 && status) atomicExch(status, 2);
+		interior = false;
 	}
 	if (interior) {
 		// the region lies inside the grid: one bulk tensor copy

@@ -143,6 +143,12 @@ ibk_status ibk_plan_kernel_stats(ibk_plan plan, ibk_kernel_stat* out, int capaci
 ibk_status ibk_plan_reset_stats(ibk_plan plan);
 ibk_status ibk_plan_launch_count(ibk_plan plan, long long* launches);
 
+/* Reads (synchronising the device) and clears the plan's device status word,
+ * which kernels set instead of faulting when one of their own checks trips
+ * (a bounded wait that timed out, a copy precondition that failed).
+ * IBK_OK when clean, IBK_ERR_DEVICE_CHECK otherwise. */
+ibk_status ibk_plan_check(ibk_plan plan);
+
 /* Human-readable text of the last error on the calling host thread. */
 const char* ibk_last_error(void);
 const char* ibk_status_string(ibk_status status);

@@ -58,6 +58,7 @@ def device_spread(plan, x, f, device, prefill=np.nan):
     fe = [torch.full((s,), prefill, dtype=torch.float64, device=device) for s in plan.sizes()]
     plan.spread(n, dev(x, device), dev(f, device), fe)
     torch.cuda.synchronize()
+    plan.check()
     return [t.cpu().numpy() for t in fe]
 
 
@@ -67,6 +68,7 @@ def device_interp(plan, x, ue, device, prefill=np.nan):
     ul = torch.full((plan.dims * n,), prefill, dtype=torch.float64, device=device)
     plan.interpolate(n, dev(x, device), [dev(u, device) for u in ue], ul)
     torch.cuda.synchronize()
+    plan.check()
     return ul.cpu().numpy()
 
 
