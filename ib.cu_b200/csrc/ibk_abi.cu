@@ -250,6 +250,8 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 		info.size[c] = size;
 	}
 	plan->tiles = make_tiles(g, tag, info.meshwidths);
+	for (int d = 0; d < dims; ++d)
+		if (g.comp[0].cells[d] < info.meshwidths) plan->tiled = false;
 	cudaError_t e = cudaMalloc(&plan->d_status, sizeof(int) * 4);
 	if (e != cudaSuccess) { cudaGetLastError(); delete plan; return set_error(IBK_ERR_OUT_OF_MEMORY, "cudaMalloc failed"); }
 	cudaMemset(plan->d_status, 0, sizeof(int) * 4);

@@ -51,13 +51,25 @@ __device__ __forceinline__ AxisReach<M> axis_reach(const GridGeom& g, const Tile
 	return r;
 }
 
+// With f != nullptr (spread) the kernel also reduces max|F| per component
+// into fmax (non-negative floats compare like their bit patterns).
 template <int M, int DIMS>
 __global__ void __launch_bounds__(256)
 bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                 int* __restrict__ count, int2* __restrict__ key_rank)
+                 int* __restrict__ count, int2* __restrict__ key_rank,
+                 const double* __restrict__ f, float* __restrict__ fmax)
 {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	const bool active = p < n;
+	if (f != nullptr) {
+#pragma unroll
+		for (int c = 0; c < DIMS; ++c) {
+			float a = active ? fabsf((float) __ldg(f + (size_t) c * n + p)) : 0.0f;
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
+			if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(fmax) + c, __float_as_int(a));
+		}
+	}
 	int key = 0;
 	if (active) {
 		int tile = 0, cls = 0, ts = 1, cs = 1;

@@ -44,6 +44,7 @@ struct TimedLaunch {
 struct Plan {
 	GridGeom g{};
 	TileGeom tiles{};
+	bool tiled = true;         // false: an axis has fewer cells than the stencil width
 	ibk_grid_info info{};
 	int delta_kind = 0, delta_order = 0, precision = 0;
 	int device = 0;
@@ -74,7 +75,7 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 }
 
 // Scratch slots of a plan.
-enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4 };
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotFmax = 5 };
 
 // Tile decomposition of a plan's grid for stencil width M.
 TileGeom make_tiles(const GridGeom& g, int tag, int M);

@@ -14,9 +14,33 @@ constexpr int kThreads = 128;
 
 inline int blocks_for(long long n, int threads) { return (int) ((n + threads - 1) / threads); }
 
+// Per-point kernels for degenerate grids (an axis with fewer cells than the
+// stencil is wide, where one stencil would reach the same face twice).
+template <typename D, int DIMS>
+ibk_status spread_direct(Plan& plan, const OpArgs& a, const double* fl, CompPtrs fe)
+{
+	const GridGeom& g = *a.g;
+	for (int c = 0; c < DIMS; ++c) {
+		cudaError_t e = cudaMemsetAsync(fe.p[c], 0, sizeof(double) * (size_t) g.comp[c].size, a.stream);
+		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+	}
+	return launch(plan, "spread_direct_kernel", a.stream, [&] {
+		spread_direct_kernel<D, DIMS><<<blocks_for(a.n, kThreads), kThreads, 0, a.stream>>>(g, a.n, a.x, fl, fe);
+	});
+}
+
+template <typename D, int DIMS>
+ibk_status interp_direct(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul)
+{
+	return launch(plan, "interp_direct_kernel", a.stream, [&] {
+		interp_direct_kernel<D, DIMS><<<blocks_for(a.n, kThreads), kThreads, 0, a.stream>>>(*a.g, a.n, a.x, ue, ul);
+	});
+}
+
 // Counting sort of the points by (tile, reach class): perm + bin offsets.
 template <int M, int DIMS>
-ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out)
+ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out,
+                      const double* f = nullptr, float** fmax_out = nullptr)
 {
 	const TileGeom& tg = plan.tiles;
 	ibk_status s;
@@ -31,8 +55,16 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out
 	int* perm = static_cast<int*>(plan.scratch[kSlotPerm].ptr);
 	const GridGeom& g = *a.g;
 	const int nb = blocks_for(a.n, 256);
+	float* fmax = nullptr;
+	if (f) {
+		if ((s = ensure_scratch(plan, kSlotFmax, sizeof(float) * kMaxDims, a.stream)) != IBK_OK) return s;
+		fmax = static_cast<float*>(plan.scratch[kSlotFmax].ptr);
+		cudaError_t e = cudaMemsetAsync(fmax, 0, sizeof(float) * kMaxDims, a.stream);
+		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+		*fmax_out = fmax;
+	}
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
-		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr);
+		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, f, fmax);
 	})) != IBK_OK) return s;
 	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
 	if ((s = ensure_scratch(plan, kSlotChunk, sizeof(int) * ((size_t) nchunks + 1), a.stream)) != IBK_OK) return s;
@@ -67,8 +99,10 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	using D = Delta<KIND, ORDER>;
 	const GridGeom& g = *a.g;
 	const TileGeom& tg = plan.tiles;
+	if (!plan.tiled) return spread_direct<D, DIMS>(plan, a, fl, fe);
 	int *perm = nullptr, *off = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off);
+	float* fmax = nullptr;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off, fl, &fmax);
 	if (s != IBK_OK) return s;
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	const size_t words = PREC == IBK_PRECISION_FP32C ? 2 : 1;   // FP32C: high + low words
@@ -76,7 +110,7 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	auto kern = spread_tile_kernel<D, DIMS, PREC>;
 	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
 	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, fe);
+		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, fmax, fe);
 	});
 }
 
@@ -133,6 +167,7 @@ ibk_status interp_impl(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul
 	using D = Delta<KIND, ORDER>;
 	const GridGeom& g = *a.g;
 	const TileGeom& tg = plan.tiles;
+	if (!plan.tiled) return interp_direct<D, DIMS>(plan, a, ue, ul);
 	int *perm = nullptr, *off = nullptr;
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off);
 	if (s != IBK_OK) return s;

@@ -9,14 +9,14 @@
 //   memory, and writes every face of its tile exactly once (zeros included).
 //   No global atomics, no zero-fill pass: each face is written by one CTA.
 //     FP64:  FP64 shared-memory accumulation.
-//     FP32C: FP32 weights and products accumulated EXACTLY in 64-bit fixed
-//            point held as two 32-bit words per face (a signed high part and
-//            an unsigned 16-bit low part, each summed with integer shared
-//            atomics, recombined at the end).  The tile's scale is the
-//            largest power of two for which a sure bound on every face sum
-//            (sum over candidate points of max|w| * res * |F|) stays below
-//            2^46, so the sum is error-free and order-independent; the only
-//            rounding is each product's quantisation to 2^-47 of that bound.
+//     FP32C: FP32 weights and products accumulated EXACTLY in fixed point
+//            held as two 32-bit words per face (high and low parts, each
+//            summed with integer shared atomics, carried and recombined
+//            exactly).  The tile's scale is the largest power of two for
+//            which a sure bound on every face sum (candidates * max|F| *
+//            max|w| * res) stays below 2^42, so the sum is error-free and
+//            order-independent; the only rounding is each product's
+//            quantisation to 2^-43 of that bound.
 //
 // interp_tile_kernel  -- one CTA per (tile, component) stages the tile plus
 //   its stencil halo in shared memory: one TMA bulk tensor copy when the box
@@ -182,46 +182,50 @@ struct SpreadSmem<D, DIMS, IBK_PRECISION_FP64> { using acc_t = double; };
 template <typename D, int DIMS>
 struct SpreadSmem<D, DIMS, IBK_PRECISION_FP32C> { using acc_t = int; };
 
-// Fixed-point split: value * scale = hi * 2^16 + lo, lo in [0, 2^16).
-constexpr int kFixLoBits = 16;
-constexpr float kFixLo = 65536.0f;
+// Fixed point of the FP32C spread.  A scaled contribution s (|s| <= 2^42) is
+// split exactly as s = h * 2^21 + l with h = rint(s / 2^21) and
+// |l| <= 2^20; h goes to the high word and rint(l) to the low word of the
+// face.  Rounding uses the float magic number 1.5 * 2^23 (x + magic carries
+// rint(x) in its low mantissa bits for |x| < 2^22), keeping the conversion
+// on the FMA/ALU pipes.  Low words are carried into high words every
+// kFixChunk candidates, so neither word can overflow.
+constexpr int kFixShift = 21;
+constexpr float kFixUnit = 2097152.0f;          // 2^21
+constexpr float kFixInvUnit = 1.0f / 2097152.0f;
+constexpr float kMagic = 12582912.0f;           // 1.5 * 2^23
+constexpr int kMagicBits = 0x4B400000;
+constexpr int kFixChunk = 2 * kTileThreads;     // candidates between carries
+constexpr int kFixScaleLog2 = 42;               // bound * scale <= 2^42
 
-// Adds s (already scaled) to the face's fixed-point pair.  Tiles with 2^16 or
-// more candidate points could overflow the low words; they accumulate in the
-// high word alone, under a scale 2^17 times smaller (still exact integer
-// sums; coarser quantisation).
-__device__ __forceinline__ void fix_add(int* hi_word, unsigned* lo_word, float s, bool two_word)
+__device__ __forceinline__ void fix_add(int* hi_word, int* lo_word, float s)
 {
-	if (!two_word) {
-		atomicAdd(hi_word, __float2int_rn(s));
-		return;
-	}
-	const float h = floorf(s * (1.0f / kFixLo));
-	const float l = fmaf(-h, kFixLo, s);         // in [0, 2^16]; rounded to the nearest unit below
-	atomicAdd(hi_word, (int) h);
-	atomicAdd(lo_word, __float2uint_rn(l));
+	const float th = fmaf(s, kFixInvUnit, kMagic);
+	const float h = th - kMagic;                          // rint(s / 2^21), exact
+	const float l = fmaf(-h, kFixUnit, s);                // exact, |l| <= 2^20
+	const int hb = __float_as_int(th) - kMagicBits;
+	const int lb = __float_as_int(l + kMagic) - kMagicBits;  // rint(l)
+	atomicAdd(hi_word, hb);
+	atomicAdd(lo_word, lb);
 }
 
 template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads)
 spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const double* __restrict__ fl, const int* __restrict__ perm,
-                   const int* __restrict__ off, CompPtrs fe)
+                   const int* __restrict__ off, const float* __restrict__ fmax, CompPtrs fe)
 {
 	// grid: (tile, component)
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ RangeTable rt;
-	__shared__ float scale_s;
-	__shared__ float bound_part[kTileThreads / 32];
 
 	const int c = blockIdx.y;
 	const CompGeom& cg = g.comp[c];
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
 	const int TV = T0 * T1 * T2;
 	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw);                 // FP32C: high words
-	unsigned* acc_lo = reinterpret_cast<unsigned*>(acc + TV);        // FP32C: low words
+	int* acc_lo = reinterpret_cast<int*>(acc + TV);                  // FP32C: low words
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, blockIdx.x, tc);
 	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
@@ -232,106 +236,98 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	}
 	for (int i = threadIdx.x; i < TV; i += kTileThreads) acc[i] = (acc_t) 0;
 	if constexpr (PREC == IBK_PRECISION_FP32C)
-		for (int i = threadIdx.x; i < TV; i += kTileThreads) acc_lo[i] = 0u;
+		for (int i = threadIdx.x; i < TV; i += kTileThreads) acc_lo[i] = 0;
 	build_ranges<DIMS>(g, tg, tc, off, rt, true);
 	const int total = rt.pref[rt.count];
-	const bool two_word = total < 65536;
 	const double* __restrict__ fc = fl + (size_t) c * n;
 
+	// FP32C: sure bound on every face sum of the tile,
+	// (candidates) * max|F| * max|w| * res, scaled to at most 2^42
 	float scale = 1.0f;
 	if constexpr (PREC == IBK_PRECISION_FP32C) {
-		// Sure bound on every face sum of this tile: max|w| * res * sum|F|.
-		float b = 0.f;
-		for (int it = threadIdx.x; it < total; it += kTileThreads)
-			b += fabsf((float) __ldg(fc + __ldg(perm + range_lookup(rt, it))));
-#pragma unroll
-		for (int o = 16; o > 0; o >>= 1) b += __shfl_xor_sync(0xffffffffu, b, o);
-		if ((threadIdx.x & 31) == 0) bound_part[threadIdx.x >> 5] = b;
-		__syncthreads();
-		if (threadIdx.x == 0) {
-			float sum = 0.f;
-			for (int w = 0; w < kTileThreads / 32; ++w) sum += bound_part[w];
-			const float bound = sum * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
-			int e;
-			frexpf(bound, &e);                      // bound < 2^e
-			// scale * bound <= 2^46: high words stay below 2^30 plus one unit
-			// per term; low words (< 2^16 each) below 2^32 for < 2^16 terms.
-			scale_s = ldexpf(1.0f, min((two_word ? 46 : 29) - e, 126));
-		}
-		__syncthreads();
-		scale = scale_s;
-	} else {
-		__syncthreads();
+		const float bound = (float) total * __ldg(fmax + c) * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
+		int e;
+		frexpf(bound, &e);                      // bound < 2^e
+		scale = ldexpf(1.0f, min(kFixScaleLog2 - e, 126));
 	}
 
-	for (int it = threadIdx.x; it < total; it += kTileThreads) {
-		const int p = __ldg(perm + range_lookup(rt, it));
-		int loc[DIMS][M];        // local (in-tile) index of node m; valid where in-tile
-		int mlo[DIMS], mhi[DIMS];
-		double dl[DIMS];
-		bool any = true;
+	const int chunk = PREC == IBK_PRECISION_FP32C ? kFixChunk : total;
+	for (int base = 0; base < total; base += chunk) {
+		const int stop = min(total, base + chunk);
+		for (int it = base + threadIdx.x; it < stop; it += kTileThreads) {
+			const int p = __ldg(perm + range_lookup(rt, it));
+			int loc[DIMS][M];
+			unsigned mask[DIMS];
+			double dl[DIMS];
+			bool any = true;
 #pragma unroll
-		for (int d = 0; d < DIMS; ++d) {
-			AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
-			dl[d] = a.delta;
-			unsigned mk = 0;
+			for (int d = 0; d < DIMS; ++d) {
+				AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+				dl[d] = a.delta;
+				unsigned mk = 0;
 #pragma unroll
-			for (int m = 0; m < M; ++m) {
-				// spread drops nodes outside [0, points) (errors_negative);
-				// this tile owns [lo, hi).  The in-tile nodes form one run of
-				// m (their indices may wrap when the tile spans the axis).
-				const int j = node_index(g, cg, d, a.base + m - sh);
-				loc[d][m] = j - lo[d];
-				mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
+				for (int m = 0; m < M; ++m) {
+					// spread drops nodes outside [0, points) (errors_negative);
+					// this tile owns [lo, hi)
+					const int j = node_index(g, cg, d, a.base + m - sh);
+					loc[d][m] = j - lo[d];
+					mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
+				}
+				mask[d] = mk;
+				any = any && mk;
 			}
-			mlo[d] = __ffs(mk) - 1;
-			mhi[d] = 32 - __clz(mk);
-			any = any && mk;
-		}
-		if (!any) continue;
-		if constexpr (PREC == IBK_PRECISION_FP64) {
-			const double f = __dmul_rn(g.res, __ldg(fc + p));
-			double w[DIMS][M];
+			if (!any) continue;
+			if constexpr (PREC == IBK_PRECISION_FP64) {
+				const double f = __dmul_rn(g.res, __ldg(fc + p));
+				double w[DIMS][M];
 #pragma unroll
-			for (int d = 0; d < DIMS; ++d)
+				for (int d = 0; d < DIMS; ++d)
 #pragma unroll
-				for (int m = 0; m < M; ++m)
-					w[d][m] = (m >= mlo[d] && m < mhi[d]) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
+					for (int m = 0; m < M; ++m)
+						w[d][m] = (mask[d] >> m & 1u) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
 #pragma unroll
-			for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
-			const int m2lo = DIMS == 3 ? mlo[2] : 0, m2hi = DIMS == 3 ? mhi[2] : 1;
-			for (int m2 = m2lo; m2 < m2hi; ++m2) {
-				const double w2 = DIMS == 3 ? select_m<M>(w[DIMS - 1], m2) : 1.0;
-				const int plane = DIMS == 3 ? select_m<M>(loc[DIMS - 1], m2) * T1 : 0;
-				for (int m1 = mlo[1]; m1 < mhi[1]; ++m1) {
-					const double w12 = __dmul_rn(select_m<M>(w[1], m1), w2);
-					const int row = (plane + select_m<M>(loc[1], m1)) * T0;
+				for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
+#pragma unroll
+				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+					const int m1 = r % M, m2 = r / M;
+					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+					const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
+					const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
 #pragma unroll
 					for (int m0 = 0; m0 < M; ++m0)
-						if (m0 >= mlo[0] && m0 < mhi[0])
+						if ((mask[0] >> m0) & rm)
 							atomicAdd(acc + row + loc[0][m0], __dmul_rn(w[0][m0], w12));
 				}
-			}
-		} else {
-			const float f = (float) (g.res * __ldg(fc + p)) * scale;
-			float w[DIMS][M];
+			} else {
+				const float f = (float) (g.res * __ldg(fc + p)) * scale;
+				float w[DIMS][M];
 #pragma unroll
-			for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
+				for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
 #pragma unroll
-			for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
-			const int m2lo = DIMS == 3 ? mlo[2] : 0, m2hi = DIMS == 3 ? mhi[2] : 1;
-			for (int m2 = m2lo; m2 < m2hi; ++m2) {
-				const float w2 = DIMS == 3 ? select_m<M>(w[DIMS - 1], m2) : 1.0f;
-				const int plane = DIMS == 3 ? select_m<M>(loc[DIMS - 1], m2) * T1 : 0;
-				for (int m1 = mlo[1]; m1 < mhi[1]; ++m1) {
-					const float w12 = select_m<M>(w[1], m1) * w2;
-					const int row = (plane + select_m<M>(loc[1], m1)) * T0;
+				for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
+#pragma unroll
+				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+					const int m1 = r % M, m2 = r / M;
+					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+					const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
 #pragma unroll
 					for (int m0 = 0; m0 < M; ++m0)
-						if (m0 >= mlo[0] && m0 < mhi[0])
-							fix_add(acc + row + loc[0][m0], acc_lo + row + loc[0][m0], w[0][m0] * w12, two_word);
+						if ((mask[0] >> m0) & rm)
+							fix_add(acc + row + loc[0][m0], acc_lo + row + loc[0][m0], w[0][m0] * w12);
 				}
 			}
+		}
+		if constexpr (PREC == IBK_PRECISION_FP32C) {
+			// carry the low words into the high words
+			__syncthreads();
+			for (int i = threadIdx.x; i < TV; i += kTileThreads) {
+				const int l = acc_lo[i];
+				const int carry = l >> kFixShift;           // arithmetic shift: floor(l / 2^21)
+				acc[i] += carry;
+				acc_lo[i] = l - carry * (1 << kFixShift);
+			}
+			__syncthreads();
 		}
 	}
 	__syncthreads();
@@ -349,11 +345,7 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
 		const int li = (l2 * T1 + l1) * T0 + l0;
 		if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = acc[li];
-		else {
-			const long long q = two_word ?
-				(long long) acc[li] * (1LL << kFixLoBits) + (long long) acc_lo[li] : (long long) acc[li];
-			out[gi] = (double) q * inv;
-		}
+		else out[gi] = (double) ((long long) acc[li] * (1LL << kFixShift) + (long long) acc_lo[li]) * inv;
 	}
 }
 
@@ -424,6 +416,15 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 		if (threadIdx.x == 0 && status) atomicExch(status, 2);
 		interior = false;
 	}
+	// first point of this thread, fetched while the region is staged
+	int it = start + threadIdx.x;
+	int p_next = 0;
+	double z_next[DIMS];
+	if (it < end) {
+		p_next = __ldg(perm + it);
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
+	}
 	if (interior) {
 		// the region lies inside the grid: one bulk tensor copy
 		if (threadIdx.x == 0) mbar_init(&bar, 1);
@@ -450,14 +451,22 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 		__syncthreads();
 	}
 	double* __restrict__ out = ul + (size_t) c * n;
-	for (int it = start + threadIdx.x; it < end; it += kTileThreads) {
-		const int p = __ldg(perm + it);
+	for (; it < end; it += kTileThreads) {
+		const int p = p_next;
+		double z[DIMS];
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) z[d] = z_next[d];
+		if (it + kTileThreads < end) {          // prefetch the next point
+			p_next = __ldg(perm + it + kTileThreads);
+#pragma unroll
+			for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
+		}
 		int loc[DIMS];          // local index of the stencil's first node
 		double dl[DIMS];
 		bool inside = true;
 #pragma unroll
 		for (int d = 0; d < DIMS; ++d) {
-			AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+			AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
 			dl[d] = a.delta;
 			int b = a.base;
 			if (!g.solid[d] && tg.ntiles[d] > 1) {
@@ -523,7 +532,7 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			double w[DIMS][M];
 #pragma unroll
 			for (int d = 0; d < DIMS; ++d) {
-				AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+				AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
 #pragma unroll
 				for (int m = 0; m < M; ++m) {
 					const int j = node_index(g, cg, d, a.base + m - sh);
