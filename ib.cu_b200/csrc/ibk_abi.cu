@@ -250,6 +250,12 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 		info.size[c] = size;
 	}
 	plan->tiles = make_tiles(g, tag, info.meshwidths);
+	{
+		// spread: 32 x 16 x 16 cells per tile (two 32-bit words per face,
+		// 64 KB of shared memory) to cut the points visited twice
+		const int spread_pref[3] = {32, 16, 16};
+		plan->spread_tiles = make_tiles(g, tag, info.meshwidths, spread_pref);
+	}
 	for (int d = 0; d < dims; ++d)
 		if (g.comp[0].cells[d] < info.meshwidths) plan->tiled = false;
 	cudaError_t e = cudaMalloc(&plan->d_status, sizeof(int) * 4);

@@ -51,23 +51,30 @@ __device__ __forceinline__ AxisReach<M> axis_reach(const GridGeom& g, const Tile
 	return r;
 }
 
-// With f != nullptr (spread) the kernel also reduces max|F| per component
-// into fmax (non-negative floats compare like their bit patterns).
+// With f != nullptr (spread) the kernel also writes this block's max|F| per
+// component to fpart[block * 3 + c]; bin_chunk_sum_kernel folds the partials.
 template <int M, int DIMS>
 __global__ void __launch_bounds__(256)
 bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                  int* __restrict__ count, int2* __restrict__ key_rank,
-                 const double* __restrict__ f, float* __restrict__ fmax)
+                 const double* __restrict__ f, float* __restrict__ fpart)
 {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	const bool active = p < n;
 	if (f != nullptr) {
+		__shared__ float wmax[8][kMaxDims];
 #pragma unroll
 		for (int c = 0; c < DIMS; ++c) {
 			float a = active ? fabsf((float) __ldg(f + (size_t) c * n + p)) : 0.0f;
 #pragma unroll
 			for (int o = 16; o > 0; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
-			if ((threadIdx.x & 31) == 0) atomicMax(reinterpret_cast<int*>(fmax) + c, __float_as_int(a));
+			if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5][c] = a;
+		}
+		__syncthreads();
+		if (threadIdx.x < DIMS) {
+			float a = 0.0f;
+			for (int w = 0; w < (int) (blockDim.x >> 5); ++w) a = fmaxf(a, wmax[w][threadIdx.x]);
+			fpart[blockIdx.x * kMaxDims + threadIdx.x] = a;
 		}
 	}
 	int key = 0;
@@ -135,9 +142,31 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int& total)
 	return r;
 }
 
+// Also folds the per-block max|F| partials of bin_count_kernel (nparts
+// blocks; none when fpart is null) into fmax[0..2] with one atomic per CTA.
 __global__ void __launch_bounds__(kScanThreads)
-bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int num_bins)
+bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int num_bins,
+                     const float* __restrict__ fpart, int nparts, float* __restrict__ fmax)
 {
+	if (fpart != nullptr) {
+		__shared__ float red[32][kMaxDims];
+		float a[kMaxDims] = {0.f, 0.f, 0.f};
+		for (int b = blockIdx.x * kScanThreads + threadIdx.x; b < nparts; b += gridDim.x * kScanThreads)
+#pragma unroll
+			for (int c = 0; c < kMaxDims; ++c) a[c] = fmaxf(a[c], fpart[b * kMaxDims + c]);
+#pragma unroll
+		for (int c = 0; c < kMaxDims; ++c) {
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) a[c] = fmaxf(a[c], __shfl_xor_sync(0xffffffffu, a[c], o));
+			if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][c] = a[c];
+		}
+		__syncthreads();
+		if (threadIdx.x < kMaxDims) {
+			float m = 0.f;
+			for (int w = 0; w < kScanThreads / 32; ++w) m = fmaxf(m, red[w][threadIdx.x]);
+			atomicMax(reinterpret_cast<int*>(fmax) + threadIdx.x, __float_as_int(m));
+		}
+	}
 	const int i0 = blockIdx.x * kScanChunk + threadIdx.x * 4;
 	int v = 0;
 	if (i0 + 3 < num_bins) {

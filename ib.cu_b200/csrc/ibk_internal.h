@@ -43,7 +43,8 @@ struct TimedLaunch {
 
 struct Plan {
 	GridGeom g{};
-	TileGeom tiles{};
+	TileGeom tiles{};          // interpolation tiles (halo staged in shared memory)
+	TileGeom spread_tiles{};   // spread tiles (owner-computes accumulators)
 	bool tiled = true;         // false: an axis has fewer cells than the stencil width
 	ibk_grid_info info{};
 	int delta_kind = 0, delta_order = 0, precision = 0;
@@ -78,7 +79,8 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotFmax = 5 };
 
 // Tile decomposition of a plan's grid for stencil width M.
-TileGeom make_tiles(const GridGeom& g, int tag, int M);
+// pref_extent: preferred tile extent per axis (nullptr: 16 cells).
+TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent = nullptr);
 
 // Returns the table for (kind, order, dims, precision) or nullptr.
 const OpTable* find_ops(int kind, int order, int dims, int precision);

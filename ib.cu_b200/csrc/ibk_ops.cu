@@ -39,10 +39,9 @@ ibk_status interp_direct(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* 
 
 // Counting sort of the points by (tile, reach class): perm + bin offsets.
 template <int M, int DIMS>
-ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out,
+ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, int** perm_out, int** off_out,
                       const double* f = nullptr, float** fmax_out = nullptr)
 {
-	const TileGeom& tg = plan.tiles;
 	ibk_status s;
 	const int need = a.n > plan.reserved_points ? a.n : plan.reserved_points;
 	if ((s = ensure_scratch(plan, kSlotCount, sizeof(int) * (size_t) tg.num_bins, a.stream, true)) != IBK_OK) return s;
@@ -56,21 +55,24 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, int** perm_out, int** off_out
 	const GridGeom& g = *a.g;
 	const int nb = blocks_for(a.n, 256);
 	float* fmax = nullptr;
+	float* fpart = nullptr;
 	if (f) {
-		if ((s = ensure_scratch(plan, kSlotFmax, sizeof(float) * kMaxDims, a.stream)) != IBK_OK) return s;
+		// fmax[0..2] followed by one partial per bin_count block
+		if ((s = ensure_scratch(plan, kSlotFmax, sizeof(float) * kMaxDims * ((size_t) nb + 1), a.stream)) != IBK_OK) return s;
 		fmax = static_cast<float*>(plan.scratch[kSlotFmax].ptr);
+		fpart = fmax + kMaxDims;
 		cudaError_t e = cudaMemsetAsync(fmax, 0, sizeof(float) * kMaxDims, a.stream);
 		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
 		*fmax_out = fmax;
 	}
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
-		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, f, fmax);
+		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, f, fpart);
 	})) != IBK_OK) return s;
 	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
 	if ((s = ensure_scratch(plan, kSlotChunk, sizeof(int) * ((size_t) nchunks + 1), a.stream)) != IBK_OK) return s;
 	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
 	if ((s = launch(plan, "bin_chunk_sum_kernel", a.stream, [&] {
-		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins);
+		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins, fpart, nb, fmax);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scan_kernel", a.stream, [&] {
 		bin_scan_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, off, tg.num_bins, nchunks);
@@ -98,11 +100,11 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 {
 	using D = Delta<KIND, ORDER>;
 	const GridGeom& g = *a.g;
-	const TileGeom& tg = plan.tiles;
+	const TileGeom& tg = plan.spread_tiles;
 	if (!plan.tiled) return spread_direct<D, DIMS>(plan, a, fl, fe);
 	int *perm = nullptr, *off = nullptr;
 	float* fmax = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off, fl, &fmax);
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off, fl, &fmax);
 	if (s != IBK_OK) return s;
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	const size_t words = PREC == IBK_PRECISION_FP32C ? 2 : 1;   // FP32C: high + low words
@@ -169,7 +171,7 @@ ibk_status interp_impl(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul
 	const TileGeom& tg = plan.tiles;
 	if (!plan.tiled) return interp_direct<D, DIMS>(plan, a, ue, ul);
 	int *perm = nullptr, *off = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, &perm, &off);
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off);
 	if (s != IBK_OK) return s;
 	constexpr int HL = Halo<D::M>::lo;
 	int box[3] = {1, 1, 1};
@@ -230,7 +232,7 @@ const Entry kTable[] = {
 // Tile extent per axis: 16 cells where the last tile keeps at least M cells
 // (a stencil can then reach at most one neighbour per side), otherwise the
 // nearest size in [8, 20] that does; axes of at most 16 cells are one tile.
-TileGeom make_tiles(const GridGeom& g, int tag, int M)
+TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
 {
 	TileGeom tg{};
 	tg.tag_mac = tag == IBK_TAG_MAC;
@@ -240,14 +242,21 @@ TileGeom make_tiles(const GridGeom& g, int tag, int M)
 		if (d >= g.dims) { tg.T[d] = 1; tg.ntiles[d] = 1; tg.cells[d] = 1; continue; }
 		const int cells = g.comp[0].cells[d];
 		tg.cells[d] = cells;
+		const int want = pref_extent ? pref_extent[d] : 16;
 		int T = cells;
-		if (cells > 16) {
-			// <= 20 keeps the FP64 staging region within shared memory
+		if (cells > want) {
 			static const int prefs[] = {16, 14, 18, 12, 20, 10, 8, 9, 11, 13, 15, 17, 19};
 			T = 0;
-			for (int t : prefs) {
-				const int r = cells % t;
-				if (r == 0 || r >= minlast) { T = t; break; }
+			if (want != 16) {
+				// a larger preferred extent first, then the regular ladder
+				for (int t = want; t >= 22 && T == 0; t -= 2) {
+					const int r = cells % t;
+					if (r == 0 || r >= minlast) T = t;
+				}
+			}
+			for (int i = 0; i < (int) (sizeof(prefs) / sizeof(prefs[0])) && T == 0; ++i) {
+				const int r = cells % prefs[i];
+				if (r == 0 || r >= minlast) T = prefs[i];
 			}
 			if (T == 0) T = 8;   // unreachable for M <= 6: some t in [8, 20] leaves r == 0 or r >= M
 		}

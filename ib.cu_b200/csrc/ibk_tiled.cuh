@@ -291,6 +291,7 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
 					const int m1 = r % M, m2 = r / M;
 					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
 					const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
 					const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
 #pragma unroll
@@ -309,6 +310,7 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
 					const int m1 = r % M, m2 = r / M;
 					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
 					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
 					const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
 #pragma unroll
