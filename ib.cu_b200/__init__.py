@@ -43,7 +43,7 @@ ABI_SYMBOLS = (
     "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
     "ibk_spread", "ibk_interpolate", "ibk_sort_keys",
     "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
-    "ibk_plan_launch_count", "ibk_plan_check",
+    "ibk_plan_launch_count", "ibk_plan_check", "ibk_interpolate_noalloc",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
 
@@ -110,6 +110,10 @@ def lib() -> ctypes.CDLL:
         L.ibk_plan_reset_stats.argtypes = [_vp]
         L.ibk_plan_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
         L.ibk_plan_check.argtypes = [_vp]
+        L.ibk_interpolate_noalloc.argtypes = [ctypes.POINTER(_Domain), ctypes.c_int, ctypes.c_int,
+                                              _Delta, ctypes.c_int, ctypes.c_int, _vp,
+                                              ctypes.POINTER(_vp), _vp, _vp]
+        L.ibk_interpolate_noalloc.restype = ctypes.c_int
         L.ibk_last_error.restype = ctypes.c_char_p
         L.ibk_status_string.restype = ctypes.c_char_p
         L.ibk_status_string.argtypes = [ctypes.c_int]

@@ -11,6 +11,8 @@
 //   bin_count_kernel    key = tile * 3^dims + class; warp-aggregated rank
 //   bin_scan_kernel     exclusive scan of the bin counts (resets the counts)
 //   bin_scatter_kernel  perm[offset[key] + rank] = point
+// The non-template kernels are static: each translation unit that launches
+// them carries its own copy.
 #pragma once
 #include "ibk_device.cuh"
 
@@ -144,7 +146,7 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int& total)
 
 // Also folds the per-block max|F| partials of bin_count_kernel (nparts
 // blocks; none when fpart is null) into fmax[0..2] with one atomic per CTA.
-__global__ void __launch_bounds__(kScanThreads)
+static __global__ void __launch_bounds__(kScanThreads)
 bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int num_bins,
                      const float* __restrict__ fpart, int nparts, float* __restrict__ fmax)
 {
@@ -180,7 +182,7 @@ bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int
 	if (threadIdx.x == 0) chunk[blockIdx.x] = total;
 }
 
-__global__ void __launch_bounds__(kScanThreads)
+static __global__ void __launch_bounds__(kScanThreads)
 bin_scan_kernel(int* __restrict__ count, const int* __restrict__ chunk, int* __restrict__ offset,
                 int num_bins, int nchunks)
 {
@@ -215,7 +217,7 @@ bin_scan_kernel(int* __restrict__ count, const int* __restrict__ chunk, int* __r
 	if (blockIdx.x == nchunks - 1 && threadIdx.x == kScanThreads - 1) offset[num_bins] = run;
 }
 
-__global__ void __launch_bounds__(256)
+static __global__ void __launch_bounds__(256)
 bin_scatter_kernel(int n, const int2* __restrict__ key_rank, const int* __restrict__ offset,
                    int* __restrict__ perm)
 {

@@ -149,6 +149,21 @@ ibk_status ibk_plan_launch_count(ibk_plan plan, long long* launches);
  * IBK_OK when clean, IBK_ERR_DEVICE_CHECK otherwise. */
 ibk_status ibk_plan_check(ibk_plan plan);
 
+/* Interpolation that allocates no device memory (no counterpart in the
+ * reference).  For callers that may not call cudaMalloc -- a component that
+ * does not own the device's memory pool, a real-time loop where an
+ * allocation would synchronise the device, a host that keeps no plan.  Same
+ * arguments and result as ibk_interpolate, with the grid described directly
+ * instead of by a plan.  Its scratch is one fixed array of about 8 MB that
+ * every GPU loading this library holds until exit; calls beyond 524288
+ * points, or grids needing more than 262144 bins (tiles x 3^dims), return
+ * IBK_ERR_CAPACITY.  All calls share that array, so calls that overlap on the
+ * GPU race.  The first call on a device looks up the array's address; make
+ * it before any stream capture. */
+ibk_status ibk_interpolate_noalloc(const ibk_domain* domain, int tag, int refinement,
+                                   ibk_delta delta, int precision, int n, const double* x,
+                                   const double* const* ue, double* ul, void* stream);
+
 /* Human-readable text of the last error on the calling host thread. */
 const char* ibk_last_error(void);
 const char* ibk_status_string(ibk_status status);
