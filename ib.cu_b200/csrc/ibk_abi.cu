@@ -251,9 +251,9 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 	}
 	plan->tiles = make_tiles(g, tag, info.meshwidths);
 	{
-		// spread: 32 x 16 x 16 cells per tile (two 32-bit words per face,
-		// 64 KB of shared memory) to cut the points visited twice
-		const int spread_pref[3] = {32, 16, 16};
+		// spread: 16^3 cells per tile (12 bytes of shared memory per face in
+		// FP32C, 48 KB: four CTAs per SM)
+		const int spread_pref[3] = {16, 16, 16};
 		plan->spread_tiles = make_tiles(g, tag, info.meshwidths, spread_pref);
 	}
 	for (int d = 0; d < dims; ++d)

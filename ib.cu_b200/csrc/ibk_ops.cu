@@ -107,8 +107,9 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off, fl, &fmax);
 	if (s != IBK_OK) return s;
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
-	const size_t words = PREC == IBK_PRECISION_FP32C ? 2 : 1;   // FP32C: high + low words
-	const size_t smem = words * sizeof(acc_t) * (size_t) tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
+	// FP64: one double per face; FP32C: an FP64 total and a 32-bit working word
+	const size_t per_face = PREC == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
+	const size_t smem = per_face * (size_t) tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
 	auto kern = spread_tile_kernel<D, DIMS, PREC>;
 	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
 	return launch(plan, "spread_tile_kernel", a.stream, [&] {

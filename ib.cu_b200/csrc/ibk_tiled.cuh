@@ -9,20 +9,16 @@
 //   memory, and writes every face of its tile exactly once (zeros included).
 //   No global atomics, no zero-fill pass: each face is written by one CTA.
 //     FP64:  FP64 shared-memory accumulation.
-//     FP32C: FP32 weights and products accumulated EXACTLY in fixed point
-//            held as two 32-bit words per face (high and low parts, each
-//            summed with integer shared atomics, carried and recombined
-//            exactly).  The tile's scale is the largest power of two for
-//            which a sure bound on every face sum (candidates * max|F| *
-//            max|w| * res) stays below 2^42, so the sum is error-free and
-//            order-independent; the only rounding is each product's
-//            quantisation to 2^-43 of that bound.
+//     FP32C: FP32 weights and products, each quantised to fixed point and
+//            summed exactly (32-bit integer shared atomics folded into FP64
+//            totals; order-independent).  See fix_add below.
 //
 // interp_tile_kernel  -- one CTA per (tile, component) stages the tile plus
-//   its stencil halo in shared memory: one TMA bulk tensor copy when the box
-//   lies inside the grid, otherwise row copies that wrap periodic halos and
-//   clamp wall halos exactly as the reference clamps node indices.  Every
-//   point of the tile then gathers its M^dims nodes from shared memory.
+//   its stencil halo in shared memory with one TMA bulk tensor copy; at a
+//   domain edge the out-of-range slabs are then patched with loads that wrap
+//   periodic halos and clamp wall halos exactly as the reference clamps node
+//   indices.  Every point of the tile then gathers its M^dims nodes from
+//   shared memory.
 //     FP64:  exact weights, sums in the reference's pattern order (bit-exact).
 //     FP32C: FP32 weights applied to the FP64 values, FP64 accumulation.
 #pragma once
@@ -182,30 +178,25 @@ struct SpreadSmem<D, DIMS, IBK_PRECISION_FP64> { using acc_t = double; };
 template <typename D, int DIMS>
 struct SpreadSmem<D, DIMS, IBK_PRECISION_FP32C> { using acc_t = int; };
 
-// Fixed point of the FP32C spread.  A scaled contribution s (|s| <= 2^42) is
-// split exactly as s = h * 2^21 + l with h = rint(s / 2^21) and
-// |l| <= 2^20; h goes to the high word and rint(l) to the low word of the
-// face.  Rounding uses the float magic number 1.5 * 2^23 (x + magic carries
-// rint(x) in its low mantissa bits for |x| < 2^22), keeping the conversion
-// on the FMA/ALU pipes.  Low words are carried into high words every
-// kFixChunk candidates, so neither word can overflow.
-constexpr int kFixShift = 21;
-constexpr float kFixUnit = 2097152.0f;          // 2^21
-constexpr float kFixInvUnit = 1.0f / 2097152.0f;
+// Fixed point of the FP32C spread.  Each FP32 product is scaled so that the
+// largest possible term (max|w| * res * max|F|) is at most 2^21, rounded to
+// an integer with the float magic number 1.5 * 2^23 (x + magic carries rint(x)
+// in its low mantissa bits for |x| < 2^22: an FADD and an integer subtract,
+// no conversion instruction), and added to the face's 32-bit working word
+// with one integer shared atomic.  At most kFixChunk candidates are summed
+// between folds (kFixChunk * 2^21 < 2^31, so a working word cannot overflow);
+// each fold adds the working words exactly into an FP64 total per face
+// (integers below 2^53 are exact in FP64).  The sum is therefore exact and
+// order-independent; the only rounding is each product's quantisation to
+// 2^-22 of the largest possible term.
 constexpr float kMagic = 12582912.0f;           // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
-constexpr int kFixChunk = 2 * kTileThreads;     // candidates between carries
-constexpr int kFixScaleLog2 = 42;               // bound * scale <= 2^42
+constexpr int kFixChunk = 1000;                 // candidates between folds
+constexpr int kFixTermLog2 = 21;                // largest term * scale <= 2^21
 
-__device__ __forceinline__ void fix_add(int* hi_word, int* lo_word, float s)
+__device__ __forceinline__ void fix_add(int* word, float s)
 {
-	const float th = fmaf(s, kFixInvUnit, kMagic);
-	const float h = th - kMagic;                          // rint(s / 2^21), exact
-	const float l = fmaf(-h, kFixUnit, s);                // exact, |l| <= 2^20
-	const int hb = __float_as_int(th) - kMagicBits;
-	const int lb = __float_as_int(l + kMagic) - kMagicBits;  // rint(l)
-	atomicAdd(hi_word, hb);
-	atomicAdd(lo_word, lb);
+	atomicAdd(word, __float_as_int(s + kMagic) - kMagicBits);   // rint(s)
 }
 
 template <typename D, int DIMS, int PREC>
@@ -224,8 +215,10 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	const CompGeom& cg = g.comp[c];
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
 	const int TV = T0 * T1 * T2;
-	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw);                 // FP32C: high words
-	int* acc_lo = reinterpret_cast<int*>(acc + TV);                  // FP32C: low words
+	// FP64: acc[TV] doubles.  FP32C: total[TV] doubles, then acc[TV] working words.
+	double* total = reinterpret_cast<double*>(smem_raw);
+	acc_t* acc = PREC == IBK_PRECISION_FP64 ? reinterpret_cast<acc_t*>(smem_raw)
+	                                        : reinterpret_cast<acc_t*>(total + TV);
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, blockIdx.x, tc);
 	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
@@ -236,24 +229,24 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	}
 	for (int i = threadIdx.x; i < TV; i += kTileThreads) acc[i] = (acc_t) 0;
 	if constexpr (PREC == IBK_PRECISION_FP32C)
-		for (int i = threadIdx.x; i < TV; i += kTileThreads) acc_lo[i] = 0;
+		for (int i = threadIdx.x; i < TV; i += kTileThreads) total[i] = 0.0;
 	build_ranges<DIMS>(g, tg, tc, off, rt, true);
-	const int total = rt.pref[rt.count];
 	const double* __restrict__ fc = fl + (size_t) c * n;
 
-	// FP32C: sure bound on every face sum of the tile,
-	// (candidates) * max|F| * max|w| * res, scaled to at most 2^42
+	// FP32C: the largest possible single term, max|F| * max|w| * res, is
+	// scaled to at most 2^21
 	float scale = 1.0f;
 	if constexpr (PREC == IBK_PRECISION_FP32C) {
-		const float bound = (float) total * __ldg(fmax + c) * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
+		const float bound = __ldg(fmax + c) * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
 		int e;
 		frexpf(bound, &e);                      // bound < 2^e
-		scale = ldexpf(1.0f, min(kFixScaleLog2 - e, 126));
+		scale = ldexpf(1.0f, min(kFixTermLog2 - e, 126));
 	}
 
-	const int chunk = PREC == IBK_PRECISION_FP32C ? kFixChunk : total;
-	for (int base = 0; base < total; base += chunk) {
-		const int stop = min(total, base + chunk);
+	const int ncand = rt.pref[rt.count];
+	const int chunk = PREC == IBK_PRECISION_FP32C ? kFixChunk : max(ncand, 1);
+	for (int base = 0; base < ncand; base += chunk) {
+		const int stop = min(ncand, base + chunk);
 		for (int it = base + threadIdx.x; it < stop; it += kTileThreads) {
 			const int p = __ldg(perm + range_lookup(rt, it));
 			int loc[DIMS][M];
@@ -316,18 +309,16 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 #pragma unroll
 					for (int m0 = 0; m0 < M; ++m0)
 						if ((mask[0] >> m0) & rm)
-							fix_add(acc + row + loc[0][m0], acc_lo + row + loc[0][m0], w[0][m0] * w12);
+							fix_add(acc + row + loc[0][m0], w[0][m0] * w12);
 				}
 			}
 		}
 		if constexpr (PREC == IBK_PRECISION_FP32C) {
-			// carry the low words into the high words
+			// fold the working words into the exact FP64 totals
 			__syncthreads();
 			for (int i = threadIdx.x; i < TV; i += kTileThreads) {
-				const int l = acc_lo[i];
-				const int carry = l >> kFixShift;           // arithmetic shift: floor(l / 2^21)
-				acc[i] += carry;
-				acc_lo[i] = l - carry * (1 << kFixShift);
+				total[i] += (double) acc[i];
+				acc[i] = 0;
 			}
 			__syncthreads();
 		}
@@ -347,7 +338,7 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
 		const int li = (l2 * T1 + l1) * T0 + l0;
 		if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = acc[li];
-		else out[gi] = (double) ((long long) acc[li] * (1LL << kFixShift) + (long long) acc_lo[li]) * inv;
+		else out[gi] = total[li] * inv;
 	}
 }
 
@@ -404,7 +395,8 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, t, tc);
 	int rlo[3] = {0, 0, 0}, E[3] = {1, 1, 1};
-	bool interior = use_tma != 0;
+	bool tma = use_tma != 0;        // stage with one bulk tensor copy
+	bool interior = true;           // the region lies inside the grid
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
 		rlo[d] = tc[d] * tg.T[d] - HL;
@@ -414,9 +406,9 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	// self-check of the TMA preconditions: 128-byte destination, x origin
 	// on a 16-byte boundary; a violation is recorded and the region staged
 	// by plain loads instead
-	if (interior && (((smem_addr(reg) & 127u) != 0u) || (rlo[0] & 1) != 0)) {
+	if (tma && (((smem_addr(reg) & 127u) != 0u) || (rlo[0] & 1) != 0)) {
 		if (threadIdx.x == 0 && status) atomicExch(status, 2);
-		interior = false;
+		tma = false;
 	}
 	// first point of this thread, fetched while the region is staged
 	int it = start + threadIdx.x;
@@ -427,8 +419,10 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 #pragma unroll
 		for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
 	}
-	if (interior) {
-		// the region lies inside the grid: one bulk tensor copy
+	if (tma) {
+		// one bulk tensor copy of the box; at a domain edge the box starts at a
+		// negative or past-the-end coordinate and the copy zero-fills those
+		// elements, which are patched below
 		if (threadIdx.x == 0) mbar_init(&bar, 1);
 		__syncthreads();
 		if (threadIdx.x == 0) {
@@ -436,9 +430,49 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			if constexpr (DIMS == 3) tma_load_3d(reg, &maps.map[c], rlo[0], rlo[1], rlo[2], &bar);
 			else tma_load_2d(reg, &maps.map[c], rlo[0], rlo[1], &bar);
 		}
-		if (!mbar_wait_bounded(&bar, 0, status)) return;
+		// one thread polls the mbarrier; the others park at the CTA barrier
+		// (no issue slots spent spinning)
+		__shared__ int tma_ok;
+		if (threadIdx.x == 0) tma_ok = mbar_wait_bounded(&bar, 0, status) ? 1 : 0;
+		__syncthreads();
+		if (!tma_ok) return;
+		if (!interior) {
+			// out-of-range slabs: wrap periodic, clamp solid (interpolate.h:16-22)
+#pragma unroll 1
+			for (int d = 0; d < DIMS; ++d) {
+				const int below = max(0, -rlo[d]);
+				const int above_from = min(E[d], cg.points[d] - rlo[d]);
+				const int other = (E[0] * E[1] * E[2]) / E[d];
+#pragma unroll 1
+				for (int side = 0; side < 2; ++side) {
+					const int s0 = side == 0 ? 0 : max(above_from, 0);
+					const int s1 = side == 0 ? below : E[d];
+					const int cnt = (s1 - s0) * other;
+					for (int i = threadIdx.x; i < cnt; i += kTileThreads) {
+						// element i of the slab: coordinate along d, then the others
+						int l[3] = {0, 0, 0};
+						l[d] = s0 + i / other;
+						int rest = i % other;
+#pragma unroll
+						for (int e = 0; e < DIMS; ++e) {
+							if (e == d) continue;
+							l[e] = rest % E[e];
+							rest /= E[e];
+						}
+						size_t gi = 0, stride = 1;
+#pragma unroll
+						for (int e = 0; e < DIMS; ++e) {
+							gi += (size_t) fold(g, cg, e, rlo[e] + l[e]) * stride;
+							stride *= (size_t) cg.points[e];
+						}
+						reg[(DIMS == 3 ? (l[2] * E[1] + l[1]) : l[1]) * E[0] + l[0]] = __ldg(u + gi);
+					}
+				}
+			}
+			__syncthreads();
+		}
 	} else {
-		// domain edge: wrap periodic, clamp solid (interpolate.h:16-22), row by row
+		// plain row copies that wrap periodic and clamp solid halos
 		const int rows = E[1] * E[2];
 		const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
 		for (int r = warp; r < rows; r += kTileThreads / 32) {
