@@ -350,6 +350,73 @@ def run_ours(args):
         dist.all_reduce(te, op=dist.ReduceOp.MAX)
     e2e_value = world * n / (float(te.item()) / args.steps / 1000.0)
 
+    # ---- step-time distribution (each step bracketed by its own events)
+    per_step = []
+    for _ in range(args.steps):
+        if flush is not None:
+            flush.zero_()
+        a0 = torch.cuda.Event(enable_timing=True)
+        a1 = torch.cuda.Event(enable_timing=True)
+        a0.record(stream)
+        step()
+        a1.record(stream)
+        a1.synchronize()
+        per_step.append(a0.elapsed_time(a1))
+    per_step.sort()
+    p50 = per_step[len(per_step) // 2]
+    p99 = per_step[min(len(per_step) - 1, int(0.99 * len(per_step)))]
+
+    # ---- the plain FP64 path on the same inputs: throughput and the accuracy
+    # of the chosen form against it (the FP64 path matches the oracle: bit for
+    # bit in interpolation, to summation order in spread)
+    plain = None
+    if precision != ibk.FP64:
+        plan64 = ibk.Plan(ibk.Mac(w.refinement), dom, ibk.Bspline(3), ibk.FP64)
+        plan64.reserve(n)
+        fe64 = [torch.empty(s_, dtype=torch.float64, device=dev) for s_ in sizes]
+        ul64 = torch.empty(3 * n, dtype=torch.float64, device=dev)
+
+        def step64():
+            plan64.spread(n, x, f, fe64, stream)
+            plan64.interpolate(n, x, ue, ul64, stream)
+
+        for _ in range(2):
+            step64()
+        step()
+        barrier()
+        err = {"spread_max": 0.0, "spread_rms": 0.0, "interp_max": 0.0, "interp_rms": 0.0}
+        for c in range(3):
+            ref_f = fe64[c]
+            scale = float(ref_f.abs().max())
+            d = (fe[c] - ref_f)
+            err["spread_max"] = max(err["spread_max"], float(d.abs().max()) / scale)
+            err["spread_rms"] = max(err["spread_rms"], float(d.square().mean().sqrt()) / float(ref_f.square().mean().sqrt()))
+            ref_u = ul64[c * n:(c + 1) * n]
+            du = ul[c * n:(c + 1) * n] - ref_u
+            err["interp_max"] = max(err["interp_max"], float(du.abs().max()) / float(ref_u.abs().max()))
+            err["interp_rms"] = max(err["interp_rms"], float(du.square().mean().sqrt()) / float(ref_u.square().mean().sqrt()))
+        k64 = max(3, args.steps // 2)
+        b0 = torch.cuda.Event(enable_timing=True)
+        b1 = torch.cuda.Event(enable_timing=True)
+        b0.record(stream)
+        for _ in range(k64):
+            step64()
+        b1.record(stream)
+        torch.cuda.synchronize()
+        ms64 = b0.elapsed_time(b1) / k64
+        plain = {"value": world * n / (ms64 / 1000.0), "unit": "points/s", "ms_per_step": ms64,
+                 "steps": k64, "speedup": ms64 / ms_step,
+                 "accuracy_vs_fp64": {k: v for k, v in err.items()},
+                 "accuracy_note": "normwise: max|err|/max|ref| and rms(err)/rms(ref), worst component"}
+        del fe64, ul64, plan64
+
+    extras = {}
+    if not args.no_extras:
+        del fe, ul
+        torch.cuda.empty_cache()
+        extras["batched"] = run_batched(ibk, W, dev, seed=rank, steps=max(5, args.steps // 2))
+        extras["serving"] = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
+
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
         cpu = cpu_measure(w, seconds_budget=args.cpu_seconds)
@@ -364,7 +431,7 @@ def run_ours(args):
         "metric": METRIC, "value": value, "unit": "points/s", "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_step,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
-        "dtype": "f64" if args.precision == "fp64" else "f32+f64-index",
+        "dtype": "f64" if args.precision == "fp64" else "f32",
         "data": "synthetic (seeded RBC / platelet surfaces, iid N(0,1) forces and velocities)",
         "config": dict(workload_config(w, args.precision), parallelism=f"replicas{world}"),
         "faces_per_s": world * G / (ms_step / 1000.0),
@@ -376,11 +443,161 @@ def run_ours(args):
         "e2e": {"value": e2e_value, "unit": "points/s", "h2d_bytes_per_step": 2 * 8 * 3 * n,
                 "d2h_bytes_per_step": 8 * 3 * n,
                 "note": "x and F copied in from pinned host memory, U copied out; grid fields stay device-resident"},
+        "p50_ms": p50, "p99_ms": p99,
+        "plain_fp64": plain,
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
+    line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------------------ batched and serving legs
+def ensemble_arrays(ibk, W, insts_w, precision, dev, seed):
+    """Batch + device arrays of an ensemble (one dict per instance)."""
+    import torch
+    insts = [ibk.Instance(ibk.Mac(w.refinement),
+                          ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)]))
+             for w in insts_w]
+    total = sum(w.n for w in insts_w)
+    batch = ibk.Batch(insts, ibk.Bspline(3), precision, max_points=total)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(seed)
+    io = []
+    for i, w in enumerate(insts_w):
+        sizes = batch.sizes(i)
+        io.append({"n": w.n, "x": torch.from_numpy(w.x).to(dev), "fl": torch.from_numpy(w.f).to(dev),
+                   "ue": [torch.randn(s_, generator=gen, dtype=torch.float64, device=dev) * W.UM_PER_S
+                          for s_ in sizes],
+                   "fe": [torch.empty(s_, dtype=torch.float64, device=dev) for s_ in sizes],
+                   "ul": torch.empty(3 * w.n, dtype=torch.float64, device=dev)})
+    batch.bind(io)
+    return batch, io, total
+
+
+def time_batch(batch, ops, steps, stream):
+    import torch
+    for _ in range(3):
+        for op in ops:
+            batch.run(op, stream)
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(steps):
+        for op in ops:
+            batch.run(op, stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    return e0.elapsed_time(e1) / steps
+
+
+def run_batched(ibk, W, dev, seed, steps):
+    """256 independent instances (cube grids of 32^3..128^3, 1-50 cells), one
+    persistent graph-captured launch per operator; FP32C vs FP64 batches and
+    a loop of single plans for comparison."""
+    import torch
+    stream = torch.cuda.current_stream()
+    insts_w = W.ensemble(seed=seed, count=256)
+    ops = (ibk.OP_SPREAD, ibk.OP_INTERPOLATE)
+    out = {"instances": len(insts_w)}
+    batch, io, total = ensemble_arrays(ibk, W, insts_w, ibk.FP32C, dev, 2000 + seed)
+    faces = sum(sum(batch.sizes(i)) for i in range(len(insts_w)))
+    t_default = time_batch(batch, ops, steps, stream)
+    cfg_s = batch.tune(ibk.OP_SPREAD, stream)
+    cfg = batch.tune(ibk.OP_INTERPOLATE, stream)
+    for op in ops:
+        batch.capture(op)
+    l0 = batch.launch_count()
+    ms = time_batch(batch, ops, steps, stream)
+    launches = (batch.launch_count() - l0) // (steps + 3)
+    out.update({"points": total, "faces": faces, "value": total / (ms / 1000.0), "unit": "points/s",
+                "ms_per_step": ms, "faces_per_s": faces / (ms / 1000.0), "ms_default_config": t_default,
+                "tuned_config": cfg, "launches_per_step": launches,
+                "roofline_bytes_per_step": 2 * algorithmic_bytes(total, faces)})
+    # FP64 batch (the plain path, batched) on the same inputs
+    b64 = ibk.Batch([ibk.Instance(ibk.Mac(w.refinement),
+                                  ibk.Domain(*[ibk.Dimension(l, b_) for l, b_ in zip(w.lengths, w.boundaries)]))
+                     for w in insts_w], ibk.Bspline(3), ibk.FP64, max_points=total)
+    fe64 = [[torch.empty_like(a) for a in e["fe"]] for e in io]
+    ul64 = [torch.empty_like(e["ul"]) for e in io]
+    b64.bind([dict(e, fe=fe64[i], ul=ul64[i]) for i, e in enumerate(io)])
+    for op in ops:
+        b64.capture(op)
+    ms64 = time_batch(b64, ops, max(3, steps // 2), stream)
+    err_s = err_u = 0.0
+    for i, e in enumerate(io):
+        for c in range(3):
+            ref = fe64[i][c]
+            err_s = max(err_s, float((e["fe"][c] - ref).abs().max()) / max(float(ref.abs().max()), 1e-300))
+        n_i = e["n"]
+        for c in range(3):
+            ref = ul64[i][c * n_i:(c + 1) * n_i]
+            err_u = max(err_u, float((e["ul"][c * n_i:(c + 1) * n_i] - ref).abs().max())
+                        / max(float(ref.abs().max()), 1e-300))
+    out["plain_fp64"] = {"value": total / (ms64 / 1000.0), "ms_per_step": ms64, "speedup": ms64 / ms,
+                         "accuracy_vs_fp64": {"spread_max": err_s, "interp_max": err_u}}
+    del b64, fe64, ul64
+    # a loop of single FP32C plans (one per instance), for the batching gain
+    plans = [ibk.Plan(ibk.Mac(w.refinement),
+                      ibk.Domain(*[ibk.Dimension(l, b_) for l, b_ in zip(w.lengths, w.boundaries)]),
+                      ibk.Bspline(3), ibk.FP32C) for w in insts_w]
+
+    def loop():
+        for p_, e in zip(plans, io):
+            p_.spread(e["n"], e["x"], e["fl"], e["fe"], stream)
+            p_.interpolate(e["n"], e["x"], e["ue"], e["ul"], stream)
+
+    for _ in range(2):
+        loop()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(max(2, steps // 4)):
+        loop()
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_loop = e0.elapsed_time(e1) / max(2, steps // 4)
+    out["plan_loop"] = {"ms_per_step": ms_loop, "batch_speedup": ms_loop / ms}
+    del plans, batch, io
+    torch.cuda.empty_cache()
+    return out
+
+
+def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=2):
+    """Serving sweep: 256 ensemble members resident on the device, Poisson
+    step requests (interpolate, advect dt = 1 us, spring k = 1 pN/um,
+    spread) at each offered rate, continuous batching on `slots` streams."""
+    insts_w = W.ensemble(seed=seed, count=256)
+    insts = [ibk.Instance(ibk.Mac(w.refinement),
+                          ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)]))
+             for w in insts_w]
+    dt = 1e-6 * 1e3            # 1 us in the internal time unit (1 ms)
+    k = W.PN / W.UM            # 1 pN/um
+    srv = ibk.Server(insts, ibk.Bspline(3), ibk.FP32C, slots=slots, dt=dt, k=k,
+                     hbm_budget=150 * 10**9, max_points=sum(w.n for w in insts_w))
+    rng = np.random.default_rng(3000 + seed)
+    for i, w in enumerate(insts_w):
+        info = ibk.Plan(ibk.Mac(w.refinement),
+                        ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)]),
+                        ibk.Bspline(3), ibk.FP32C).sizes()
+        srv.admit(i, w.x, [rng.normal(size=s_) * W.UM_PER_S for s_ in info])
+    srv.run_poisson(rate=500.0, requests=100, seed=1)          # warm-up
+    sweep = []
+    for r in rates:
+        nreq = int(max(200, min(20000, r * seconds_per_rate)))
+        st = srv.run_poisson(rate=float(r), requests=nreq, seed=int(r))
+        sweep.append({"offered_per_s": r, "requests": st["requests"], "p50_ms": st["p50_ms"],
+                      "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                      "served_per_s": st["requests"] / max(st["wall_s"], 1e-9),
+                      "points_per_s": st["points"] / max(st["wall_s"], 1e-9),
+                      "launches": st["launches"]})
+    admitted = srv.stats()["admitted_bytes"]
+    srv.close()
+    return {"members": len(insts_w), "slots": slots, "admitted_bytes": admitted,
+            "hbm_budget_bytes": 150 * 10**9, "sweep": sweep}
 
 
 def main():
@@ -391,9 +608,11 @@ def main():
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
     ap.add_argument("--workload", default="large-channel",
                     choices=["large-channel", "medium-channel", "channel", "single-rbc"])
-    ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp64")
+    ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--no-extras", action="store_true",
+                    help="skip the batched (256 instances) and serving legs")
     args = ap.parse_args()
     if args.impl == "reference":
         run_reference(args)

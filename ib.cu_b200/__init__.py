@@ -44,8 +44,15 @@ ABI_SYMBOLS = (
     "ibk_spread", "ibk_interpolate", "ibk_sort_keys",
     "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
     "ibk_plan_launch_count", "ibk_plan_check", "ibk_interpolate_noalloc",
+    "ibk_batch_create", "ibk_batch_destroy", "ibk_batch_info", "ibk_batch_bind",
+    "ibk_batch_set_step", "ibk_batch_run", "ibk_batch_capture", "ibk_batch_configure",
+    "ibk_batch_get_config", "ibk_batch_tune", "ibk_batch_launch_count", "ibk_batch_check",
+    "ibk_server_create", "ibk_server_destroy", "ibk_server_admit", "ibk_server_retire",
+    "ibk_server_submit", "ibk_server_progress", "ibk_server_drain", "ibk_server_clock",
+    "ibk_server_read", "ibk_server_get_stats", "ibk_server_reset_stats", "ibk_server_run_poisson",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
+OP_SPREAD, OP_INTERPOLATE, OP_STEP = 1, 2, 3
 
 
 class IbkError(RuntimeError):
@@ -76,6 +83,42 @@ class GridInfo(ctypes.Structure):
 
     def comp_points(self, c):
         return [self.points[c][d] for d in range(self.dims)]
+
+
+class _InstanceDesc(ctypes.Structure):
+    _fields_ = [("domain", _Domain), ("tag", ctypes.c_int), ("refinement", ctypes.c_int)]
+
+
+class _InstanceIO(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_int), ("x", ctypes.c_void_p), ("fl", ctypes.c_void_p),
+                ("fe", ctypes.c_void_p * 3), ("ue", ctypes.c_void_p * 3), ("ul", ctypes.c_void_p),
+                ("xn", ctypes.c_void_p), ("xref", ctypes.c_void_p), ("fs", ctypes.c_void_p)]
+
+
+class BatchConfig(ctypes.Structure):
+    _fields_ = [("spread_tile", ctypes.c_int * 3), ("interp_tile", ctypes.c_int * 3),
+                ("spread_ctas_per_sm", ctypes.c_int), ("interp_ctas_per_sm", ctypes.c_int)]
+
+    def as_dict(self):
+        return {"spread_tile": list(self.spread_tile), "interp_tile": list(self.interp_tile),
+                "spread_ctas_per_sm": self.spread_ctas_per_sm,
+                "interp_ctas_per_sm": self.interp_ctas_per_sm}
+
+
+class ServerConfig(ctypes.Structure):
+    _fields_ = [("delta", _Delta), ("precision", ctypes.c_int), ("slots", ctypes.c_int),
+                ("dt", ctypes.c_double), ("k", ctypes.c_double), ("hbm_budget", ctypes.c_longlong),
+                ("max_points", ctypes.c_int)]
+
+
+class ServerStats(ctypes.Structure):
+    _fields_ = [("requests", ctypes.c_longlong), ("launches", ctypes.c_longlong),
+                ("points", ctypes.c_longlong), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
+                ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("wall_s", ctypes.c_double),
+                ("admitted_bytes", ctypes.c_longlong)]
+
+    def as_dict(self):
+        return {name: getattr(self, name) for name, _ in self._fields_}
 
 
 _lib = None
@@ -114,6 +157,37 @@ def lib() -> ctypes.CDLL:
                                               _Delta, ctypes.c_int, ctypes.c_int, _vp,
                                               ctypes.POINTER(_vp), _vp, _vp]
         L.ibk_interpolate_noalloc.restype = ctypes.c_int
+        L.ibk_batch_create.argtypes = [ctypes.c_int, ctypes.POINTER(_InstanceDesc), _Delta, ctypes.c_int,
+                                       ctypes.c_int, ctypes.POINTER(_vp)]
+        L.ibk_batch_destroy.argtypes = [_vp]
+        L.ibk_batch_info.argtypes = [_vp, ctypes.c_int, ctypes.POINTER(GridInfo)]
+        L.ibk_batch_bind.argtypes = [_vp, ctypes.POINTER(_InstanceIO), _vp]
+        L.ibk_batch_set_step.argtypes = [_vp, ctypes.c_double, ctypes.c_double]
+        L.ibk_batch_run.argtypes = [_vp, ctypes.c_int, _vp]
+        L.ibk_batch_capture.argtypes = [_vp, ctypes.c_int]
+        L.ibk_batch_configure.argtypes = [_vp, ctypes.POINTER(BatchConfig)]
+        L.ibk_batch_get_config.argtypes = [_vp, ctypes.POINTER(BatchConfig)]
+        L.ibk_batch_tune.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(BatchConfig)]
+        L.ibk_batch_launch_count.argtypes = [_vp, ctypes.POINTER(ctypes.c_longlong)]
+        L.ibk_batch_check.argtypes = [_vp]
+        L.ibk_server_create.argtypes = [ctypes.c_int, ctypes.POINTER(_InstanceDesc),
+                                        ctypes.POINTER(ServerConfig), ctypes.POINTER(_vp)]
+        L.ibk_server_destroy.argtypes = [_vp]
+        L.ibk_server_admit.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, ctypes.POINTER(_vp)]
+        L.ibk_server_retire.argtypes = [_vp, ctypes.c_int]
+        L.ibk_server_submit.argtypes = [_vp, ctypes.c_int, ctypes.c_double]
+        L.ibk_server_progress.argtypes = [_vp, ctypes.POINTER(ctypes.c_int)]
+        L.ibk_server_drain.argtypes = [_vp]
+        L.ibk_server_clock.argtypes = [_vp]
+        L.ibk_server_clock.restype = ctypes.c_double
+        L.ibk_server_read.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_vp)]
+        L.ibk_server_get_stats.argtypes = [_vp, ctypes.POINTER(ServerStats)]
+        L.ibk_server_reset_stats.argtypes = [_vp]
+        L.ibk_server_run_poisson.argtypes = [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
+                                             ctypes.POINTER(ServerStats)]
+        for name in ABI_SYMBOLS:
+            if name.startswith(("ibk_batch_", "ibk_server_")) and name != "ibk_server_clock":
+                getattr(L, name).restype = ctypes.c_int
         L.ibk_last_error.restype = ctypes.c_char_p
         L.ibk_status_string.restype = ctypes.c_char_p
         L.ibk_status_string.argtypes = [ctypes.c_int]
@@ -358,3 +432,193 @@ class Interpolate:
             ul = torch.empty(x.numel(), dtype=torch.float64, device=x.device)
         self.plan.interpolate(n, x, ue, ul, stream)
         return ul
+
+
+# ------------------------------------------------------------------ batches
+class Instance:
+    """One grid of a batch: its domain and tag (fd::mac{refinement})."""
+
+    def __init__(self, tag: Mac, domain: Domain):
+        self.tag = tag
+        self.domain = domain
+
+
+class Batch:
+    """Owner of one ``ibk_batch``: many independent grids, one persistent
+    kernel per operator (no counterpart in the reference, which runs one
+    operator object per grid).
+
+    ``bind(io)`` takes one dict per instance with any of the keys ``n, x, fl,
+    fe, ue, ul, xn, xref, fs`` (torch CUDA float64 tensors; fe and ue are
+    per-component lists); ``run(op)`` runs OP_SPREAD, OP_INTERPOLATE or
+    OP_STEP over every instance."""
+
+    def __init__(self, instances, delta: DeltaFn, precision: int = FP32C, max_points: int = 0):
+        count = len(instances)
+        descs = (_InstanceDesc * count)()
+        for i, inst in enumerate(instances):
+            descs[i].domain = inst.domain._abi()
+            descs[i].tag = inst.tag.tag
+            descs[i].refinement = inst.tag.refinement
+        d = _Delta()
+        d.kind, d.order = delta.kind, delta.order
+        h = _vp()
+        check(lib().ibk_batch_create(count, descs, d, int(precision), int(max_points), ctypes.byref(h)))
+        self._h = h
+        self.count = count
+        self.precision = precision
+        self.infos = []
+        for i in range(count):
+            info = GridInfo()
+            check(lib().ibk_batch_info(h, i, ctypes.byref(info)))
+            self.infos.append(info)
+        self._bound = None     # keeps the bound tensors alive
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibk_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def sizes(self, i):
+        info = self.infos[i]
+        return [int(info.size[c]) for c in range(info.dims)]
+
+    def bind(self, io, stream=None):
+        tab = (_InstanceIO * self.count)()
+        for i, e in enumerate(io):
+            t = tab[i]
+            t.n = int(e.get("n", 0))
+            for key in ("x", "fl", "ul", "xn", "xref", "fs"):
+                setattr(t, key, _ptr(e.get(key)))
+            for key in ("fe", "ue"):
+                arrs = e.get(key)
+                if arrs is not None:
+                    for c, a in enumerate(arrs):
+                        getattr(t, key)[c] = _ptr(a)
+        check(lib().ibk_batch_bind(self._h, tab, _stream_handle(stream)))
+        self._bound = io
+
+    def set_step(self, dt: float, k: float):
+        check(lib().ibk_batch_set_step(self._h, float(dt), float(k)))
+
+    def run(self, op: int, stream=None):
+        check(lib().ibk_batch_run(self._h, int(op), _stream_handle(stream)))
+
+    def capture(self, op: int):
+        check(lib().ibk_batch_capture(self._h, int(op)))
+
+    def configure(self, spread_tile=(16, 16, 16), interp_tile=(16, 16, 16),
+                  spread_ctas_per_sm=0, interp_ctas_per_sm=0):
+        c = BatchConfig()
+        for d in range(3):
+            c.spread_tile[d] = int(spread_tile[d])
+            c.interp_tile[d] = int(interp_tile[d])
+        c.spread_ctas_per_sm = int(spread_ctas_per_sm)
+        c.interp_ctas_per_sm = int(interp_ctas_per_sm)
+        check(lib().ibk_batch_configure(self._h, ctypes.byref(c)))
+
+    def config(self) -> dict:
+        c = BatchConfig()
+        check(lib().ibk_batch_get_config(self._h, ctypes.byref(c)))
+        return c.as_dict()
+
+    def tune(self, op: int, stream=None) -> dict:
+        c = BatchConfig()
+        check(lib().ibk_batch_tune(self._h, int(op), _stream_handle(stream), ctypes.byref(c)))
+        return c.as_dict()
+
+    def launch_count(self) -> int:
+        v = ctypes.c_longlong()
+        check(lib().ibk_batch_launch_count(self._h, ctypes.byref(v)))
+        return int(v.value)
+
+    def check(self):
+        check(lib().ibk_batch_check(self._h))
+
+
+# ------------------------------------------------------------------ serving
+class Server:
+    """Owner of one ``ibk_server``: device-resident ensemble members stepped
+    (interpolate, advect, spring force, spread) as requests arrive, packed
+    into batched launches on ``slots`` streams (continuous batching)."""
+
+    def __init__(self, instances, delta: DeltaFn, precision: int = FP32C, slots: int = 2,
+                 dt: float = 1e-3, k: float = 1e-3, hbm_budget: int = 150 * 10**9, max_points: int = 0):
+        count = len(instances)
+        descs = (_InstanceDesc * count)()
+        for i, inst in enumerate(instances):
+            descs[i].domain = inst.domain._abi()
+            descs[i].tag = inst.tag.tag
+            descs[i].refinement = inst.tag.refinement
+        cfg = ServerConfig()
+        cfg.delta.kind, cfg.delta.order = delta.kind, delta.order
+        cfg.precision, cfg.slots, cfg.dt, cfg.k = int(precision), int(slots), float(dt), float(k)
+        cfg.hbm_budget, cfg.max_points = int(hbm_budget), int(max_points)
+        h = _vp()
+        check(lib().ibk_server_create(count, descs, ctypes.byref(cfg), ctypes.byref(h)))
+        self._h = h
+        self.count = count
+
+    def close(self):
+        if getattr(self, "_h", None):
+            lib().ibk_server_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def admit(self, member: int, x, ue):
+        """x: host float64 array (dims*n); ue: per-component host float64 arrays."""
+        import numpy as np
+        x = np.ascontiguousarray(x, dtype=np.float64)
+        ue = [np.ascontiguousarray(u, dtype=np.float64) for u in ue]
+        P = (_vp * 3)(*[u.ctypes.data for u in ue])
+        check(lib().ibk_server_admit(self._h, int(member), x.size // len(ue), x.ctypes.data, P))
+
+    def retire(self, member: int):
+        check(lib().ibk_server_retire(self._h, int(member)))
+
+    def submit(self, member: int, t_arrival: float = -1.0):
+        check(lib().ibk_server_submit(self._h, int(member), float(t_arrival)))
+
+    def progress(self) -> int:
+        p = ctypes.c_int()
+        check(lib().ibk_server_progress(self._h, ctypes.byref(p)))
+        return int(p.value)
+
+    def drain(self):
+        check(lib().ibk_server_drain(self._h))
+
+    def clock(self) -> float:
+        return float(lib().ibk_server_clock(self._h))
+
+    def read(self, member: int, n: int, sizes):
+        """(positions, [force grid per component]) as host numpy arrays."""
+        import numpy as np
+        x = np.empty(3 * n, dtype=np.float64)
+        fe = [np.empty(s, dtype=np.float64) for s in sizes]
+        P = (_vp * 3)(*[a.ctypes.data for a in fe])
+        check(lib().ibk_server_read(self._h, int(member), x.ctypes.data, P))
+        return x, fe
+
+    def stats(self) -> dict:
+        st = ServerStats()
+        check(lib().ibk_server_get_stats(self._h, ctypes.byref(st)))
+        return st.as_dict()
+
+    def reset_stats(self):
+        check(lib().ibk_server_reset_stats(self._h))
+
+    def run_poisson(self, rate: float, requests: int, seed: int = 0) -> dict:
+        st = ServerStats()
+        check(lib().ibk_server_run_poisson(self._h, float(rate), int(requests), int(seed), ctypes.byref(st)))
+        return st.as_dict()

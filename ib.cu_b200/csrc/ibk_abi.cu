@@ -51,6 +51,8 @@ double gcd_fp(double a, double b)
 	return gcd_impl(1.0, b / a) * a;
 }
 
+} // namespace
+
 int meshwidths_of(int kind, int order)
 {
 	switch (kind) {
@@ -63,7 +65,72 @@ int meshwidths_of(int kind, int order)
 	return 0;
 }
 
-} // namespace
+ibk_status check_domain(const ibk_domain* domain, int tag, int refinement)
+{
+	const int dims = domain->dims;
+	if (dims < 2 || dims > 3) return set_error(IBK_ERR_UNSUPPORTED, "dims must be 2 or 3");
+	if (refinement <= 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "refinement must be positive");
+	if (tag != IBK_TAG_MAC && tag != IBK_TAG_CENTERED) return set_error(IBK_ERR_INVALID_ARGUMENT, "unknown grid tag");
+	for (int d = 0; d < dims; ++d)
+		if (!(domain->length[d] > 0) || !(domain->length[d] < 1e300))
+			return set_error(IBK_ERR_INVALID_ARGUMENT, "dimension lengths must be positive and finite");
+	return IBK_OK;
+}
+
+// fd::domain / fd::grid / fd::discretization geometry of every component
+// (include/fd/domain.h:30-32, include/algo/gcd.h:27-34, include/fd/grid.h:39-46,
+// include/fd/discretization.h:113-164).  The domain is validated by the caller.
+ibk_status make_geometry(const ibk_domain* domain, int tag, int refinement, int meshwidths, GridGeom& g,
+                         ibk_grid_info& info)
+{
+	const int dims = domain->dims;
+	g = GridGeom{};
+	info = ibk_grid_info{};
+	g.dims = dims;
+	double unit = domain->length[0];
+	for (int d = 1; d < dims; ++d) unit = gcd_fp(unit, domain->length[d]);
+	const double r = (double) refinement / unit;
+	g.r = r;
+	double res = 1;
+	for (int d = dims - 1; d >= 0; --d) res = r * res;
+	g.res = res;
+	for (int d = 0; d < dims; ++d) {
+		g.length[d] = domain->length[d];
+		g.length_safe[d] = domain->length[d] * (1.0 - 0x1p-52);
+		g.solid[d] = domain->boundary[d] != IBK_PERIODIC;
+	}
+	info.dims = dims;
+	info.meshwidths = meshwidths;
+	info.unit = unit;
+	info.resolution = r;
+	for (int c = 0; c < dims; ++c) {
+		CompGeom& cg = g.comp[c];
+		long long size = 1;
+		for (int d = 0; d < dims; ++d) {
+			double al = (tag == IBK_TAG_MAC && c == d) ? host_modulo(0.5 + 0.5, 1.0) : 0.5;
+			al = host_modulo(al, 1.0);
+			const int on_boundary = !al;
+			const double cells_f = domain->length[d] * r + 0.5;
+			if (!(cells_f < 2147483647.0)) return set_error(IBK_ERR_INVALID_ARGUMENT, "grid too large");
+			const int cells = (int) cells_f;
+			const int points = cells - (on_boundary && g.solid[d]);
+			if (points < 1) return set_error(IBK_ERR_INVALID_ARGUMENT, "grid has no points along a dimension");
+			const double shift = al + (double) (g.solid[d] && on_boundary);
+			cg.cells[d] = cells;
+			cg.points[d] = points;
+			cg.shift[d] = shift;
+			cg.s_over_r[d] = shift / r;
+			info.cells[c][d] = cells;
+			info.points[c][d] = points;
+			info.shift[c][d] = shift;
+			size *= points;
+		}
+		if (size >= (1LL << 31)) return set_error(IBK_ERR_INVALID_ARGUMENT, "component grid exceeds 2^31 faces (32-bit reference indices)");
+		cg.size = size;
+		info.size[c] = size;
+	}
+	return IBK_OK;
+}
 
 ibk_status set_error(ibk_status s, const std::string& msg)
 {
@@ -186,13 +253,9 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 {
 	if (!domain || !out) return set_error(IBK_ERR_INVALID_ARGUMENT, "null domain or output pointer");
 	*out = nullptr;
+	ibk_status cs = check_domain(domain, tag, refinement);
+	if (cs != IBK_OK) return cs;
 	const int dims = domain->dims;
-	if (dims < 2 || dims > 3) return set_error(IBK_ERR_UNSUPPORTED, "dims must be 2 or 3");
-	if (refinement <= 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "refinement must be positive");
-	if (tag != IBK_TAG_MAC && tag != IBK_TAG_CENTERED) return set_error(IBK_ERR_INVALID_ARGUMENT, "unknown grid tag");
-	for (int d = 0; d < dims; ++d)
-		if (!(domain->length[d] > 0) || !(domain->length[d] < 1e300))
-			return set_error(IBK_ERR_INVALID_ARGUMENT, "dimension lengths must be positive and finite");
 	const OpTable* ops = find_ops(delta.kind, delta.order, dims, precision);
 	if (!ops) return set_error(IBK_ERR_UNSUPPORTED, "delta / dims / precision combination not built");
 
@@ -204,51 +267,11 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 	plan->precision = precision;
 	cudaGetDevice(&plan->device);
 
-	GridGeom& g = plan->g;
-	g.dims = dims;
-	double unit = domain->length[0];
-	for (int d = 1; d < dims; ++d) unit = gcd_fp(unit, domain->length[d]);
-	const double r = (double) refinement / unit;
-	g.r = r;
-	double res = 1;
-	for (int d = dims - 1; d >= 0; --d) res = r * res;
-	g.res = res;
-	for (int d = 0; d < dims; ++d) {
-		g.length[d] = domain->length[d];
-		g.length_safe[d] = domain->length[d] * (1.0 - 0x1p-52);
-		g.solid[d] = domain->boundary[d] != IBK_PERIODIC;
-	}
-	ibk_grid_info& info = plan->info;
-	info.dims = dims;
-	info.meshwidths = meshwidths_of(delta.kind, plan->delta_order);
-	info.unit = unit;
-	info.resolution = r;
-	for (int c = 0; c < dims; ++c) {
-		CompGeom& cg = g.comp[c];
-		long long size = 1;
-		for (int d = 0; d < dims; ++d) {
-			double al = (tag == IBK_TAG_MAC && c == d) ? host_modulo(0.5 + 0.5, 1.0) : 0.5;
-			al = host_modulo(al, 1.0);
-			const int on_boundary = !al;
-			const double cells_f = domain->length[d] * r + 0.5;
-			if (!(cells_f < 2147483647.0)) { delete plan; return set_error(IBK_ERR_INVALID_ARGUMENT, "grid too large"); }
-			const int cells = (int) cells_f;
-			const int points = cells - (on_boundary && g.solid[d]);
-			if (points < 1) { delete plan; return set_error(IBK_ERR_INVALID_ARGUMENT, "grid has no points along a dimension"); }
-			const double shift = al + (double) (g.solid[d] && on_boundary);
-			cg.cells[d] = cells;
-			cg.points[d] = points;
-			cg.shift[d] = shift;
-			cg.s_over_r[d] = shift / r;
-			info.cells[c][d] = cells;
-			info.points[c][d] = points;
-			info.shift[c][d] = shift;
-			size *= points;
-		}
-		if (size >= (1LL << 31)) { delete plan; return set_error(IBK_ERR_INVALID_ARGUMENT, "component grid exceeds 2^31 faces (32-bit reference indices)"); }
-		cg.size = size;
-		info.size[c] = size;
-	}
+	ibk_status gs = make_geometry(domain, tag, refinement, meshwidths_of(delta.kind, plan->delta_order),
+	                              plan->g, plan->info);
+	if (gs != IBK_OK) { delete plan; return gs; }
+	const GridGeom& g = plan->g;
+	const ibk_grid_info& info = plan->info;
 	plan->tiles = make_tiles(g, tag, info.meshwidths);
 	{
 		// spread: 16^3 cells per tile (12 bytes of shared memory per face in

@@ -1,0 +1,883 @@
+// Batches: spread / interpolate / coupled step over many independent grids,
+// one persistent kernel per operator.
+//
+// The reference builds one operator object per grid and runs its kernels
+// grid by grid (include/ib/novel.h:197-227, include/ib/interpolate.h:92-115).
+// Here every instance of a batch is binned into one global bin space
+// (instance i owns bins [bin_base_i, bin_base_i + tiles_i * 3^dims)), the
+// points of all instances are numbered consecutively, and the tile kernels'
+// bodies (spread_tile / interp_tile) run inside persistent CTAs that take
+// (instance, tile, component) work items from a device counter.  The work
+// list is that of the instances bound with points: each bind uploads the
+// list of active instances and the prefix sums of their item counts, and a
+// CTA maps item k to (instance, tile, component) by a binary search.  Per
+// item the CTA copies the instance's geometry and bound arrays into shared
+// memory.  Nothing here waits on another CTA: a CTA only takes items until
+// the list is exhausted.
+//
+// All device memory is allocated at create / configure time; a run launches
+// a fixed sequence (memsets, four binning kernels and one persistent kernel
+// per operator) whose grids depend only on the batch's capacity and
+// configuration (the binning kernels stride over the bound points), so it
+// can be captured once as a CUDA graph and replayed with new bindings.
+#include <algorithm>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+#include "ibk_internal.h"
+#include "ibk_tiled.cuh"
+
+namespace ibk {
+
+// Static description of one instance (per configuration).
+struct BatchInst {
+	GridGeom g;
+	TileGeom ts;            // spread tiles
+	TileGeom ti;            // interpolation tiles
+	int bin_s, bin_i;       // first bin of the instance in each bin space
+};
+
+// Bound arrays of one instance (per bind).
+struct BatchIO {
+	int n, pbase;           // points; index of the first point in the batch numbering
+	const double* x;
+	const double* fl;
+	double* fe[kMaxDims];
+	const double* ue[kMaxDims];
+	double* ul;
+	double* xn;
+	const double* xref;
+	double* fs;
+};
+
+// Per-bind header of the device table.
+struct BatchHeader {
+	int total_points;       // bound points of all instances
+	int num_active;         // instances bound with points
+	int items_s, items_i;   // work items of the active instances
+};
+
+// Device views of the bound table (all in one allocation).
+struct BatchTable {
+	const BatchHeader* hdr;
+	const BatchIO* io;      // [count]
+	const int* pstart;      // [count + 1]: first batch point of each instance
+	const int* active;      // [num_active]: instances bound with points
+	const int* spre;        // [num_active + 1]: prefix of their spread items
+	const int* ipre;        // [num_active + 1]: prefix of their interpolation items
+	int count;
+};
+
+namespace {
+
+constexpr int kBinThreads = 256;
+constexpr int kRing = 4;
+
+// The last i in [0, count) with pre[i] <= k: the instance holding batch
+// point k (pre = pstart; instances with no points have pstart[i] ==
+// pstart[i + 1]), or the active instance holding work item k (pre = spre or
+// ipre).
+__device__ __forceinline__ int find_instance(const int* __restrict__ pstart, int count, int gp, int lo = 0)
+{
+	int hi = count - 1;
+	while (lo < hi) {
+		const int mid = (lo + hi + 1) >> 1;
+		if (__ldg(pstart + mid) <= gp) lo = mid;
+		else hi = mid - 1;
+	}
+	return lo;
+}
+
+// Copy a trivially copyable descriptor into shared memory, 4 bytes per thread.
+template <typename T>
+__device__ __forceinline__ void copy_to_shared(T* dst, const T* src)
+{
+	static_assert(sizeof(T) % 4 == 0, "descriptor size");
+	const int* s = reinterpret_cast<const int*>(src);
+	int* d = reinterpret_cast<int*>(dst);
+	for (int i = threadIdx.x; i < (int) (sizeof(T) / 4); i += blockDim.x) d[i] = __ldg(s + i);
+}
+
+// Binning of every bound point of the batch (grid-stride over the bound
+// points).  spread: bin by the spread tiles (else the interpolation tiles);
+// moved: positions xn (else x); forces: 1 = fl, 2 = fs (per-bin max|F| into
+// binmax), 0 = none.
+template <int M, int DIMS>
+__global__ void __launch_bounds__(kBinThreads)
+batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved, int forces,
+                       int* __restrict__ counts, int2* __restrict__ key_rank, unsigned* __restrict__ binmax)
+{
+	const int total = __ldg(&t.hdr->total_points);
+	for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
+		const int gp = base + threadIdx.x;
+		const bool active = gp < total;
+		// one binary search per warp (its first point), then only the lanes
+		// past an instance boundary search again, from there
+		const int lane = threadIdx.x & 31;
+		const int wfirst = base + (threadIdx.x & ~31);
+		int i0 = 0;
+		if (lane == 0 && wfirst < total) i0 = find_instance(t.pstart, t.count, wfirst);
+		i0 = __shfl_sync(0xffffffffu, i0, 0);
+		int key = 0, n = 0, p = 0;
+		const double* f = nullptr;
+		if (active) {
+			const int i = gp < __ldg(t.pstart + i0 + 1) ? i0 : find_instance(t.pstart, t.count, gp, i0 + 1);
+			const BatchInst& bi = insts[i];
+			const BatchIO& o = t.io[i];
+			n = o.n;
+			p = gp - o.pbase;
+			const double* x = moved ? o.xn : o.x;
+			key = spread ? bi.bin_s + bin_key<M, DIMS>(bi.g, bi.ts, x, n, p)
+			             : bi.bin_i + bin_key<M, DIMS>(bi.g, bi.ti, x, n, p);
+			f = forces == 1 ? o.fl : o.fs;
+		}
+		const unsigned mask = __ballot_sync(0xffffffffu, active);
+		// forces is uniform, and a bound instance with points has its force array
+		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + gp, forces ? f : nullptr, n, p, binmax);
+	}
+}
+
+__global__ void __launch_bounds__(kBinThreads)
+batch_bin_scatter_kernel(BatchTable t, const int2* __restrict__ key_rank, const int* __restrict__ offset,
+                         int* __restrict__ perm)
+{
+	const int total = __ldg(&t.hdr->total_points);
+	for (int gp = blockIdx.x * blockDim.x + threadIdx.x; gp < total; gp += gridDim.x * blockDim.x) {
+		const int2 kr = key_rank[gp];
+		perm[__ldg(offset + kr.x) + kr.y] = gp;
+	}
+}
+
+// Thread 0 takes the next work item of the active instances: instance and
+// item index within it (tile * dims + component), or instance -1 when the
+// list is exhausted.
+__device__ __forceinline__ void next_item(int* next, int nitems, int nact, const int* __restrict__ pre,
+                                          const int* __restrict__ active, int* inst, int* local)
+{
+	const int k = atomicAdd(next, 1);
+	if (k >= nitems) { *inst = -1; *local = 0; return; }
+	const int j = find_instance(pre, nact, k);
+	*inst = __ldg(active + j);
+	*local = k - __ldg(pre + j);
+}
+
+// Persistent spread over the active instances' (tile, component) items.
+template <typename D, int DIMS, int PREC>
+__global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
+batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
+                    const int* __restrict__ perm, const int* __restrict__ off,
+                    const unsigned* __restrict__ binmax, int step)
+{
+	__shared__ int cur_inst, cur_local;
+	__shared__ BatchInst si;
+	__shared__ BatchIO so;
+	const int nitems = __ldg(&t.hdr->items_s), nact = __ldg(&t.hdr->num_active);
+	for (;;) {
+		if (threadIdx.x == 0) next_item(next, nitems, nact, t.spre, t.active, &cur_inst, &cur_local);
+		__syncthreads();
+		const int inst = cur_inst, local = cur_local;
+		if (inst < 0) return;
+		copy_to_shared(&si, insts + inst);
+		copy_to_shared(&so, t.io + inst);
+		__syncthreads();
+		CompPtrs fe;
+#pragma unroll
+		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
+		spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, perm, so.pbase,
+		                           off + si.bin_s, binmax ? binmax + (size_t) si.bin_s * kMaxDims : nullptr, fe,
+		                           local / DIMS, local % DIMS);
+		__syncthreads();
+	}
+}
+
+// Persistent interpolation over the active instances' (tile, component)
+// items (plain staging of each tile's region); with step set, the serving
+// epilogue (advection + spring force) is applied.
+template <typename D, int DIMS, int PREC>
+__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
+batch_interp_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
+                    const int* __restrict__ perm, const int* __restrict__ off, int step, double dt, double k,
+                    int* status)
+{
+	__shared__ int cur_inst, cur_local;
+	__shared__ BatchInst si;
+	__shared__ BatchIO so;
+	__shared__ StepEpilogue epi;
+	const int nitems = __ldg(&t.hdr->items_i), nact = __ldg(&t.hdr->num_active);
+	for (;;) {
+		if (threadIdx.x == 0) next_item(next, nitems, nact, t.ipre, t.active, &cur_inst, &cur_local);
+		__syncthreads();
+		const int inst = cur_inst, local = cur_local;
+		if (inst < 0) return;
+		copy_to_shared(&si, insts + inst);
+		copy_to_shared(&so, t.io + inst);
+		__syncthreads();
+		if (step && threadIdx.x == 0) epi = StepEpilogue{so.xn, so.fs, so.xref, dt, k};
+		__syncthreads();
+		ConstCompPtrs ue;
+#pragma unroll
+		for (int c = 0; c < kMaxDims; ++c) ue.p[c] = so.ue[c];
+		interp_tile<D, DIMS, PREC>(si.g, si.ti, so.n, so.x, perm, so.pbase, off + si.bin_i, ue, so.ul, nullptr, 0,
+		                           status, step ? &epi : nullptr, local / DIMS, local % DIMS);
+		__syncthreads();
+	}
+}
+
+} // namespace
+
+struct Batch;
+using BatchRunFn = ibk_status (*)(Batch&, int op, cudaStream_t);
+using BatchPrepFn = ibk_status (*)(Batch&);
+
+struct BatchOps {
+	BatchRunFn run;
+	BatchPrepFn prepare;     // kernel attributes and persistent grid sizes
+};
+
+struct Batch {
+	int device = 0, dims = 3, count = 0, M = 4, precision = 0;
+	int delta_kind = 0, delta_order = 0;
+	const BatchOps* ops = nullptr;
+	std::vector<GridGeom> geo;
+	std::vector<ibk_grid_info> info;
+	std::vector<int> tag;
+	ibk_batch_config config{};
+	// configuration-derived
+	std::vector<BatchInst> inst_h;
+	int bins_s = 0, bins_i = 0;
+	std::vector<int> nitem_s, nitem_i;  // work items per instance
+	long long items_s = 0, items_i = 0; // of all instances
+	size_t smem_s = 0, smem_i = 0;
+	int grid_s = 0, grid_i = 0, grid_bin = 1;
+	BatchInst* d_inst = nullptr;
+	size_t bins_cap = 0;
+	// bindings
+	int capacity = 0;
+	std::vector<BatchIO> io_h;
+	unsigned char* d_table = nullptr; // header, io, pstart, active, spre, ipre
+	size_t table_bytes = 0, off_io = 0, off_pstart = 0, off_active = 0, off_spre = 0, off_ipre = 0;
+	unsigned char* h_ring[kRing] = {};
+	cudaEvent_t ring_ev[kRing] = {};
+	int ring_next = 0;
+	bool bound = false;
+	// scratch
+	int *d_counts = nullptr, *d_off = nullptr, *d_chunk = nullptr, *d_perm = nullptr, *d_next = nullptr;
+	int* d_status = nullptr;
+	int2* d_kr = nullptr;
+	unsigned* d_binmax = nullptr;
+	// step parameters and graphs
+	double dt = 0.0, k = 0.0;
+	cudaStream_t cap_stream = nullptr;
+	cudaGraphExec_t exec[4] = {};
+	long long launches = 0;
+	int num_sms = 0;
+};
+
+namespace {
+
+ibk_status cuda_check(cudaError_t e, const char* what)
+{
+	if (e == cudaSuccess) return IBK_OK;
+	cudaGetLastError();
+	return set_error(e == cudaErrorMemoryAllocation ? IBK_ERR_OUT_OF_MEMORY : IBK_ERR_CUDA,
+	                 std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+void drop_graphs(Batch& b)
+{
+	for (cudaGraphExec_t& e : b.exec)
+		if (e) { cudaGraphExecDestroy(e); e = nullptr; }
+}
+
+inline int blocks_for(long long n, int threads) { return (int) ((n + threads - 1) / threads); }
+
+BatchTable table_view(const Batch& b)
+{
+	BatchTable t;
+	t.hdr = reinterpret_cast<const BatchHeader*>(b.d_table);
+	t.io = reinterpret_cast<const BatchIO*>(b.d_table + b.off_io);
+	t.pstart = reinterpret_cast<const int*>(b.d_table + b.off_pstart);
+	t.active = reinterpret_cast<const int*>(b.d_table + b.off_active);
+	t.spre = reinterpret_cast<const int*>(b.d_table + b.off_spre);
+	t.ipre = reinterpret_cast<const int*>(b.d_table + b.off_ipre);
+	t.count = b.count;
+	return t;
+}
+
+// Binning of the bound points by the spread (spread = 1) or interpolation
+// tiles, then the scan and the scatter of the batch permutation.
+template <int M, int DIMS>
+ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved, int forces)
+{
+	const BatchTable t = table_view(b);
+	const int nbins = spread ? b.bins_s : b.bins_i;
+	if (forces) {
+		ibk_status st = cuda_check(cudaMemsetAsync(b.d_binmax, 0, sizeof(unsigned) * kMaxDims * (size_t) nbins, s),
+		                           "cudaMemsetAsync");
+		if (st != IBK_OK) return st;
+	}
+	batch_bin_count_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, forces,
+	                                                                    b.d_counts, b.d_kr,
+	                                                                    forces ? b.d_binmax : nullptr);
+	const int nchunks = (nbins + kScanChunk - 1) / kScanChunk;
+	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, nbins);
+	bin_scan_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, b.d_off, nbins, nchunks);
+	batch_bin_scatter_kernel<<<b.grid_bin, kBinThreads, 0, s>>>(t, b.d_kr, b.d_off, b.d_perm);
+	b.launches += 4;
+	return check_launch("batch binning");
+}
+
+template <int KIND, int ORDER, int DIMS, int PREC>
+ibk_status batch_run_impl(Batch& b, int op, cudaStream_t s)
+{
+	using D = Delta<KIND, ORDER>;
+	const BatchTable t = table_view(b);
+	ibk_status st;
+	if ((st = cuda_check(cudaMemsetAsync(b.d_next, 0, sizeof(int) * 2, s), "cudaMemsetAsync")) != IBK_OK) return st;
+	const bool step = op == IBK_OP_STEP;
+	if (op == IBK_OP_INTERPOLATE || step) {
+		if ((st = batch_bin<D::M, DIMS>(b, s, 0, 0, 0)) != IBK_OK) return st;
+		batch_interp_kernel<D, DIMS, PREC><<<b.grid_i, kTileThreads, b.smem_i, s>>>(
+			b.d_inst, t, b.d_next + 1, b.d_perm, b.d_off, step ? 1 : 0, b.dt, b.k, b.d_status);
+		b.launches += 1;
+		if ((st = check_launch("batch_interp_kernel")) != IBK_OK) return st;
+	}
+	if (op == IBK_OP_SPREAD || step) {
+		const int forces = PREC == IBK_PRECISION_FP32C ? (step ? 2 : 1) : 0;
+		if ((st = batch_bin<D::M, DIMS>(b, s, 1, step ? 1 : 0, forces)) != IBK_OK) return st;
+		batch_spread_kernel<D, DIMS, PREC><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
+			b.d_inst, t, b.d_next, b.d_perm, b.d_off, PREC == IBK_PRECISION_FP32C ? b.d_binmax : nullptr,
+			step ? 1 : 0);
+		b.launches += 1;
+		if ((st = check_launch("batch_spread_kernel")) != IBK_OK) return st;
+	}
+	return IBK_OK;
+}
+
+// Kernel attributes and persistent grid sizes for the current configuration.
+template <int KIND, int ORDER, int DIMS, int PREC>
+ibk_status batch_prepare_impl(Batch& b)
+{
+	using D = Delta<KIND, ORDER>;
+	auto ks = batch_spread_kernel<D, DIMS, PREC>;
+	auto ki = batch_interp_kernel<D, DIMS, PREC>;
+	ibk_status st;
+	if ((st = cuda_check(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b.smem_s),
+	                     "cudaFuncSetAttribute")) != IBK_OK) return st;
+	if ((st = cuda_check(cudaFuncSetAttribute(ki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b.smem_i),
+	                     "cudaFuncSetAttribute")) != IBK_OK) return st;
+	int occ_s = 0, occ_i = 0;
+	if ((st = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, ks, kTileThreads, b.smem_s),
+	                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor")) != IBK_OK) return st;
+	if ((st = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, ki, kTileThreads, b.smem_i),
+	                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor")) != IBK_OK) return st;
+	if (occ_s < 1 || occ_i < 1) return set_error(IBK_ERR_UNSUPPORTED, "batch tiles need more shared memory than an SM has");
+	if (b.config.spread_ctas_per_sm > 0) occ_s = std::min(occ_s, b.config.spread_ctas_per_sm);
+	if (b.config.interp_ctas_per_sm > 0) occ_i = std::min(occ_i, b.config.interp_ctas_per_sm);
+	b.grid_s = (int) std::max(1LL, std::min(b.items_s, (long long) occ_s * b.num_sms));
+	b.grid_i = (int) std::max(1LL, std::min(b.items_i, (long long) occ_i * b.num_sms));
+	b.grid_bin = std::max(1, std::min(blocks_for(b.capacity, kBinThreads), 8 * b.num_sms));
+	return IBK_OK;
+}
+
+template <int KIND, int ORDER, int DIMS, int PREC>
+constexpr BatchOps make_batch_ops()
+{
+	return BatchOps{&batch_run_impl<KIND, ORDER, DIMS, PREC>, &batch_prepare_impl<KIND, ORDER, DIMS, PREC>};
+}
+
+struct BatchEntry { int kind, order, dims, prec; BatchOps ops; };
+
+#define IBK_BENTRY(K, O, DIM, PR) BatchEntry{K, O, DIM, PR, make_batch_ops<K, O, DIM, PR>()}
+#define IBK_BATCH_ENTRIES(DIM, PR)                                            \
+	IBK_BENTRY(kBspline, 1, DIM, PR), IBK_BENTRY(kBspline, 2, DIM, PR),     \
+	IBK_BENTRY(kBspline, 3, DIM, PR), IBK_BENTRY(kBspline, 4, DIM, PR),     \
+	IBK_BENTRY(kBspline, 5, DIM, PR), IBK_BENTRY(kPeskin, 0, DIM, PR),      \
+	IBK_BENTRY(kRoma, 0, DIM, PR), IBK_BENTRY(kCosine, 0, DIM, PR),         \
+	IBK_BENTRY(kHat, 0, DIM, PR)
+
+const BatchEntry kBatchTable[] = {
+	IBK_BATCH_ENTRIES(2, IBK_PRECISION_FP64),
+	IBK_BATCH_ENTRIES(3, IBK_PRECISION_FP64),
+	IBK_BATCH_ENTRIES(2, IBK_PRECISION_FP32C),
+	IBK_BATCH_ENTRIES(3, IBK_PRECISION_FP32C),
+};
+
+const BatchOps* find_batch_ops(int kind, int order, int dims, int precision)
+{
+	if (kind != kBspline) order = 0;
+	for (const BatchEntry& e : kBatchTable)
+		if (e.kind == kind && e.order == order && e.dims == dims && e.prec == precision) return &e.ops;
+	return nullptr;
+}
+
+template <typename T>
+ibk_status grow(T** ptr, size_t& cap, size_t want, const char* what)
+{
+	if (*ptr && cap >= want) return IBK_OK;
+	if (*ptr) cudaFree(*ptr);
+	*ptr = nullptr;
+	cap = 0;
+	ibk_status st = cuda_check(cudaMalloc(reinterpret_cast<void**>(ptr), std::max<size_t>(want, 1) * sizeof(T)), what);
+	if (st == IBK_OK) cap = want;
+	return st;
+}
+
+// Halo extents of the staged interpolation region, as interp_tile lays it out.
+size_t region_bytes(int M, const TileGeom& tg, int dims)
+{
+	const int hl = 1 + ((M - 1) >> 1), hh = 1 + M / 2;
+	size_t v = 1;
+	for (int d = 0; d < dims; ++d) {
+		int e = tg.T[d] + hl + hh;
+		if (d == 0) e = (e + 1) & ~1;
+		v *= (size_t) e;
+	}
+	return sizeof(double) * v + 128;
+}
+
+// The table of a binding: header, io, pstart, active list and item prefixes.
+void build_table(const Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
+{
+	std::memset(out, 0, b.table_bytes);
+	BatchHeader* h = reinterpret_cast<BatchHeader*>(out);
+	int* pstart = reinterpret_cast<int*>(out + b.off_pstart);
+	int* active = reinterpret_cast<int*>(out + b.off_active);
+	int* spre = reinterpret_cast<int*>(out + b.off_spre);
+	int* ipre = reinterpret_cast<int*>(out + b.off_ipre);
+	std::memcpy(out + b.off_io, io.data(), sizeof(BatchIO) * io.size());
+	int total = 0, nact = 0, ns = 0, ni = 0;
+	for (int i = 0; i < b.count; ++i) {
+		pstart[i] = total;
+		total += io[i].n;
+		if (io[i].n == 0) continue;
+		active[nact] = i;
+		spre[nact] = ns;
+		ipre[nact] = ni;
+		ns += b.nitem_s[i];
+		ni += b.nitem_i[i];
+		++nact;
+	}
+	pstart[b.count] = total;
+	spre[nact] = ns;
+	ipre[nact] = ni;
+	h->total_points = total;
+	h->num_active = nact;
+	h->items_s = ns;
+	h->items_i = ni;
+}
+
+// Tiles, bins, work items and shared-memory sizes of a configuration.
+ibk_status configure(Batch& b, const ibk_batch_config& cfg)
+{
+	std::vector<BatchInst> inst(b.count);
+	std::vector<int> nitem_s(b.count), nitem_i(b.count);
+	long long bins_s = 0, bins_i = 0, items_s = 0, items_i = 0;
+	size_t tv_max = 1, region_max = 0;
+	for (int i = 0; i < b.count; ++i) {
+		BatchInst& bi = inst[i];
+		bi.g = b.geo[i];
+		bi.ts = make_tiles(bi.g, b.tag[i], b.M, cfg.spread_tile);
+		bi.ti = make_tiles(bi.g, b.tag[i], b.M, cfg.interp_tile);
+		bi.bin_s = (int) bins_s;
+		bi.bin_i = (int) bins_i;
+		bins_s += bi.ts.num_bins;
+		bins_i += bi.ti.num_bins;
+		nitem_s[i] = bi.ts.num_tiles * b.dims;
+		nitem_i[i] = bi.ti.num_tiles * b.dims;
+		items_s += nitem_s[i];
+		items_i += nitem_i[i];
+		if (bins_s >= (1LL << 30) || bins_i >= (1LL << 30) || items_s >= (1LL << 30) || items_i >= (1LL << 30))
+			return set_error(IBK_ERR_INVALID_ARGUMENT, "batch has too many tiles");
+		size_t tv = 1;
+		for (int d = 0; d < b.dims; ++d) tv *= (size_t) bi.ts.T[d];
+		tv_max = std::max(tv_max, tv);
+		region_max = std::max(region_max, region_bytes(b.M, bi.ti, b.dims));
+	}
+	const size_t per_face = b.precision == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
+	const size_t smem_s = per_face * tv_max;
+	if (smem_s > 200 * 1024 || region_max > 200 * 1024)
+		return set_error(IBK_ERR_UNSUPPORTED, "batch tile shape needs more than 200 KB of shared memory");
+	ibk_status st;
+	const size_t nb = (size_t) std::max(bins_s, bins_i);
+	if (!b.d_counts || b.bins_cap < nb) {
+		// bin arrays sized for the larger bin space (counts start zeroed and
+		// every scan leaves them zeroed)
+		void** bufs[] = {reinterpret_cast<void**>(&b.d_counts), reinterpret_cast<void**>(&b.d_off),
+		                 reinterpret_cast<void**>(&b.d_chunk), reinterpret_cast<void**>(&b.d_binmax)};
+		const size_t bytes[] = {sizeof(int) * nb, sizeof(int) * (nb + 1), sizeof(int) * (nb / kScanChunk + 2),
+		                        sizeof(unsigned) * kMaxDims * nb};
+		b.bins_cap = 0;
+		for (int j = 0; j < 4; ++j) {
+			if (*bufs[j]) cudaFree(*bufs[j]);
+			*bufs[j] = nullptr;
+		}
+		for (int j = 0; j < 4; ++j)
+			if ((st = cuda_check(cudaMalloc(bufs[j], bytes[j]), "cudaMalloc")) != IBK_OK) return st;
+		if ((st = cuda_check(cudaMemset(b.d_counts, 0, bytes[0]), "cudaMemset")) != IBK_OK) return st;
+		b.bins_cap = nb;
+	}
+	size_t cap = 0;
+	BatchInst* d_inst = nullptr;
+	if ((st = grow(&d_inst, cap, (size_t) b.count, "cudaMalloc")) != IBK_OK) return st;
+	st = cuda_check(cudaMemcpy(d_inst, inst.data(), sizeof(BatchInst) * b.count, cudaMemcpyHostToDevice), "cudaMemcpy");
+	if (st != IBK_OK) { cudaFree(d_inst); return st; }
+	// finish the work on the old configuration before replacing it
+	if ((st = cuda_check(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) != IBK_OK) { cudaFree(d_inst); return st; }
+	if (b.d_inst) cudaFree(b.d_inst);
+	b.d_inst = d_inst;
+	b.inst_h = std::move(inst);
+	b.nitem_s = std::move(nitem_s);
+	b.nitem_i = std::move(nitem_i);
+	b.bins_s = (int) bins_s;
+	b.bins_i = (int) bins_i;
+	b.items_s = items_s;
+	b.items_i = items_i;
+	b.smem_s = smem_s;
+	b.smem_i = region_max;
+	b.config = cfg;
+	drop_graphs(b);
+	if (b.bound) {
+		// the bound table's item prefixes follow the tiles: rebuild it
+		std::vector<unsigned char> tab(b.table_bytes);
+		build_table(b, b.io_h, tab.data());
+		if ((st = cuda_check(cudaMemcpy(b.d_table, tab.data(), b.table_bytes, cudaMemcpyHostToDevice), "cudaMemcpy")) != IBK_OK)
+			return st;
+	}
+	return b.ops->prepare(b);
+}
+
+void destroy(Batch* b)
+{
+	drop_graphs(*b);
+	for (int r = 0; r < kRing; ++r) {
+		if (b->ring_ev[r]) { cudaEventSynchronize(b->ring_ev[r]); cudaEventDestroy(b->ring_ev[r]); }
+		if (b->h_ring[r]) cudaFreeHost(b->h_ring[r]);
+	}
+	void* bufs[] = {b->d_inst, b->d_table, b->d_counts, b->d_off, b->d_chunk, b->d_perm,
+	                b->d_next, b->d_status, b->d_kr, b->d_binmax};
+	for (void* p : bufs)
+		if (p) cudaFree(p);
+	if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
+	delete b;
+}
+
+// Arrays an operation reads or writes for every instance with points.
+ibk_status check_bound(const Batch& b, int op)
+{
+	if (!b.bound) return set_error(IBK_ERR_INVALID_ARGUMENT, "batch has no bound arrays");
+	for (int i = 0; i < b.count; ++i) {
+		const BatchIO& o = b.io_h[i];
+		if (o.n == 0) continue;
+		bool ok = o.x != nullptr;
+		if (op == IBK_OP_SPREAD || op == IBK_OP_STEP)
+			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe[c] != nullptr;
+		if (op == IBK_OP_SPREAD) ok = ok && o.fl != nullptr;
+		if (op == IBK_OP_INTERPOLATE || op == IBK_OP_STEP)
+			for (int c = 0; c < b.dims; ++c) ok = ok && o.ue[c] != nullptr;
+		if (op == IBK_OP_INTERPOLATE) ok = ok && o.ul != nullptr;
+		if (op == IBK_OP_STEP) ok = ok && o.xn && o.xref && o.fs;
+		if (!ok)
+			return set_error(IBK_ERR_INVALID_ARGUMENT,
+			                 "instance " + std::to_string(i) + " lacks an array this operation needs");
+	}
+	return IBK_OK;
+}
+
+} // namespace
+} // namespace ibk
+
+using namespace ibk;
+
+extern "C" {
+
+ibk_status ibk_batch_create(int count, const ibk_instance_desc* instances, ibk_delta delta, int precision,
+                            int max_points, ibk_batch* out)
+{
+	if (!out || !instances || count <= 0 || max_points < 0)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null pointer, no instances or negative capacity");
+	*out = nullptr;
+	const int dims = instances[0].domain.dims;
+	for (int i = 0; i < count; ++i) {
+		ibk_status cs = check_domain(&instances[i].domain, instances[i].tag, instances[i].refinement);
+		if (cs != IBK_OK) return cs;
+		if (instances[i].domain.dims != dims) return set_error(IBK_ERR_INVALID_ARGUMENT, "instances differ in dims");
+	}
+	const BatchOps* ops = find_batch_ops(delta.kind, delta.order, dims, precision);
+	if (!ops) return set_error(IBK_ERR_UNSUPPORTED, "delta / dims / precision combination not built");
+	Batch* b = new (std::nothrow) Batch();
+	if (!b) return set_error(IBK_ERR_OUT_OF_MEMORY, "host allocation failed");
+	b->ops = ops;
+	b->dims = dims;
+	b->count = count;
+	b->precision = precision;
+	b->delta_kind = delta.kind;
+	b->delta_order = delta.kind == kBspline ? delta.order : 0;
+	b->M = meshwidths_of(delta.kind, b->delta_order);
+	b->capacity = max_points;
+	cudaGetDevice(&b->device);
+	cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, b->device);
+	b->geo.resize(count);
+	b->info.resize(count);
+	b->tag.resize(count);
+	for (int i = 0; i < count; ++i) {
+		ibk_status gs = make_geometry(&instances[i].domain, instances[i].tag, instances[i].refinement, b->M,
+		                              b->geo[i], b->info[i]);
+		if (gs != IBK_OK) { destroy(b); return gs; }
+		b->tag[i] = instances[i].tag;
+		for (int d = 0; d < dims; ++d)
+			if (b->geo[i].comp[0].cells[d] < b->M) {
+				destroy(b);
+				return set_error(IBK_ERR_UNSUPPORTED, "instance " + std::to_string(i) +
+				                 " has an axis with fewer cells than the stencil is wide (use a plan)");
+			}
+	}
+	ibk_status st = IBK_OK;
+	auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
+	b->off_io = al(sizeof(BatchHeader));
+	b->off_pstart = al(b->off_io + sizeof(BatchIO) * (size_t) count);
+	b->off_active = al(b->off_pstart + sizeof(int) * ((size_t) count + 1));
+	b->off_spre = al(b->off_active + sizeof(int) * (size_t) count);
+	b->off_ipre = al(b->off_spre + sizeof(int) * ((size_t) count + 1));
+	b->table_bytes = b->off_ipre + sizeof(int) * ((size_t) count + 1);
+	size_t cap = 0;
+	if (st == IBK_OK) st = grow(&b->d_table, cap, b->table_bytes, "cudaMalloc");
+	for (int r = 0; r < kRing && st == IBK_OK; ++r) {
+		st = cuda_check(cudaHostAlloc(reinterpret_cast<void**>(&b->h_ring[r]), b->table_bytes, cudaHostAllocDefault),
+		                "cudaHostAlloc");
+		if (st == IBK_OK) st = cuda_check(cudaEventCreateWithFlags(&b->ring_ev[r], cudaEventDisableTiming), "cudaEventCreate");
+	}
+	const size_t pts = (size_t) std::max(max_points, 1);
+	cap = 0;
+	if (st == IBK_OK) st = grow(&b->d_kr, cap, pts, "cudaMalloc");
+	cap = 0;
+	if (st == IBK_OK) st = grow(&b->d_perm, cap, pts, "cudaMalloc");
+	cap = 0;
+	if (st == IBK_OK) st = grow(&b->d_next, cap, 4, "cudaMalloc");
+	cap = 0;
+	if (st == IBK_OK) st = grow(&b->d_status, cap, 4, "cudaMalloc");
+	if (st == IBK_OK) st = cuda_check(cudaMemset(b->d_status, 0, sizeof(int) * 4), "cudaMemset");
+	if (st == IBK_OK) {
+		// an empty binding: every instance idle
+		std::vector<unsigned char> zero(b->table_bytes, 0);
+		st = cuda_check(cudaMemcpy(b->d_table, zero.data(), b->table_bytes, cudaMemcpyHostToDevice), "cudaMemcpy");
+	}
+	if (st == IBK_OK) st = cuda_check(cudaStreamCreateWithFlags(&b->cap_stream, cudaStreamNonBlocking), "cudaStreamCreate");
+	ibk_batch_config cfg{};
+	for (int d = 0; d < 3; ++d) { cfg.spread_tile[d] = 16; cfg.interp_tile[d] = 16; }
+	if (st == IBK_OK) st = configure(*b, cfg);
+	if (st != IBK_OK) { destroy(b); return st; }
+	*out = reinterpret_cast<ibk_batch>(b);
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_destroy(ibk_batch handle)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (b) destroy(b);
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_info(ibk_batch handle, int instance, ibk_grid_info* info)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || !info || instance < 0 || instance >= b->count)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or info, or instance out of range");
+	*info = b->info[instance];
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_bind(ibk_batch handle, const ibk_instance_io* io, void* stream)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || !io) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or io");
+	std::vector<BatchIO> tab(b->count);
+	long long total = 0;
+	for (int i = 0; i < b->count; ++i) {
+		const ibk_instance_io& s = io[i];
+		if (s.n < 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "negative point count");
+		BatchIO& t = tab[i];
+		t.n = s.n;
+		t.pbase = (int) total;
+		t.x = s.x;
+		t.fl = s.fl;
+		for (int c = 0; c < kMaxDims; ++c) { t.fe[c] = s.fe[c]; t.ue[c] = s.ue[c]; }
+		t.ul = s.ul;
+		t.xn = s.xn;
+		t.xref = s.xref;
+		t.fs = s.fs;
+		total += s.n;
+		if (total > b->capacity)
+			return set_error(IBK_ERR_CAPACITY, "bound points exceed the batch capacity of " +
+			                 std::to_string(b->capacity));
+	}
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	const int r = b->ring_next;
+	b->ring_next = (r + 1) % kRing;
+	ibk_status st = cuda_check(cudaEventSynchronize(b->ring_ev[r]), "cudaEventSynchronize");
+	if (st != IBK_OK) return st;
+	build_table(*b, tab, b->h_ring[r]);
+	if ((st = cuda_check(cudaMemcpyAsync(b->d_table, b->h_ring[r], b->table_bytes, cudaMemcpyHostToDevice, s),
+	                     "cudaMemcpyAsync")) != IBK_OK) return st;
+	if ((st = cuda_check(cudaEventRecord(b->ring_ev[r], s), "cudaEventRecord")) != IBK_OK) return st;
+	b->io_h = std::move(tab);
+	b->bound = true;
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_set_step(ibk_batch handle, double dt, double k)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch");
+	if (dt != b->dt || k != b->k) {
+		if (b->exec[IBK_OP_STEP]) { cudaGraphExecDestroy(b->exec[IBK_OP_STEP]); b->exec[IBK_OP_STEP] = nullptr; }
+		b->dt = dt;
+		b->k = k;
+	}
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_run(ibk_batch handle, int op, void* stream)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_STEP) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
+	ibk_status st = check_bound(*b, op);
+	if (st != IBK_OK) return st;
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	if (b->exec[op]) {
+		b->launches += (op == IBK_OP_STEP ? 10 : 5);
+		return cuda_check(cudaGraphLaunch(b->exec[op], s), "cudaGraphLaunch");
+	}
+	return b->ops->run(*b, op, s);
+}
+
+ibk_status ibk_batch_capture(ibk_batch handle, int op)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_STEP) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
+	if (b->exec[op]) { cudaGraphExecDestroy(b->exec[op]); b->exec[op] = nullptr; }
+	ibk_status st = cuda_check(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal),
+	                           "cudaStreamBeginCapture");
+	if (st != IBK_OK) return st;
+	const long long before = b->launches;
+	ibk_status rs = b->ops->run(*b, op, b->cap_stream);
+	b->launches = before;
+	cudaGraph_t graph = nullptr;
+	st = cuda_check(cudaStreamEndCapture(b->cap_stream, &graph), "cudaStreamEndCapture");
+	if (rs != IBK_OK) { if (graph) cudaGraphDestroy(graph); return rs; }
+	if (st != IBK_OK) return st;
+	st = cuda_check(cudaGraphInstantiate(&b->exec[op], graph, 0), "cudaGraphInstantiate");
+	cudaGraphDestroy(graph);
+	return st;
+}
+
+ibk_status ibk_batch_configure(ibk_batch handle, const ibk_batch_config* config)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || !config) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or config");
+	for (int d = 0; d < 3; ++d)
+		if (config->spread_tile[d] < 2 || config->interp_tile[d] < 2 || config->spread_tile[d] > 256 ||
+		    config->interp_tile[d] > 256)
+			return set_error(IBK_ERR_INVALID_ARGUMENT, "tile extents must lie in [2, 256]");
+	if (config->spread_ctas_per_sm < 0 || config->interp_ctas_per_sm < 0)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "negative CTAs per SM");
+	const ibk_batch_config old = b->config;
+	ibk_status st = configure(*b, *config);
+	if (st != IBK_OK) configure(*b, old);
+	return st;
+}
+
+ibk_status ibk_batch_get_config(ibk_batch handle, ibk_batch_config* config)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || !config) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or config");
+	*config = b->config;
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_tune(ibk_batch handle, int op, void* stream, ibk_batch_config* best)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_STEP) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
+	ibk_status st = check_bound(*b, op);
+	if (st != IBK_OK) return st;
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	cudaEvent_t e0, e1;
+	cudaEventCreate(&e0);
+	cudaEventCreate(&e1);
+	// time one configuration: one warm-up run, then the mean of three
+	auto time_cfg = [&](const ibk_batch_config& cfg, float& ms) -> ibk_status {
+		ibk_status cs = configure(*b, cfg);
+		if (cs != IBK_OK) return cs;
+		if ((cs = b->ops->run(*b, op, s)) != IBK_OK) return cs;
+		cudaEventRecord(e0, s);
+		for (int r = 0; r < 3 && cs == IBK_OK; ++r) cs = b->ops->run(*b, op, s);
+		cudaEventRecord(e1, s);
+		if (cs != IBK_OK) return cs;
+		if ((cs = cuda_check(cudaEventSynchronize(e1), "cudaEventSynchronize")) != IBK_OK) return cs;
+		cudaEventElapsedTime(&ms, e0, e1);
+		ms /= 3.0f;
+		return IBK_OK;
+	};
+	static const int spread_shapes[][3] = {{16, 16, 16}, {32, 16, 16}, {16, 16, 8}, {32, 16, 8}, {32, 32, 8}, {8, 8, 8}};
+	static const int interp_shapes[][3] = {{16, 16, 16}, {16, 16, 8}, {32, 16, 8}, {8, 8, 8}, {24, 16, 16}};
+	ibk_batch_config cur = b->config;
+	float best_ms = 0.0f;
+	if ((st = time_cfg(cur, best_ms)) == IBK_OK) {
+		const bool tune_s = op != IBK_OP_INTERPOLATE, tune_i = op != IBK_OP_SPREAD;
+		for (int pass = 0; pass < 2 && st == IBK_OK; ++pass) {
+			const bool spread_pass = pass == 0;
+			if ((spread_pass && !tune_s) || (!spread_pass && !tune_i)) continue;
+			const int nshape = spread_pass ? 6 : 5;
+			for (int k = 0; k < nshape; ++k) {
+				ibk_batch_config c = cur;
+				int* ext = spread_pass ? c.spread_tile : c.interp_tile;
+				const int* want = spread_pass ? spread_shapes[k] : interp_shapes[k];
+				for (int d = 0; d < 3; ++d) ext[d] = want[d];
+				float ms = 0.0f;
+				ibk_status cs = time_cfg(c, ms);
+				if (cs == IBK_ERR_UNSUPPORTED) continue;     // shape does not fit in shared memory
+				if (cs != IBK_OK) { st = cs; break; }
+				if (ms < best_ms) { best_ms = ms; cur = c; }
+			}
+			// persistent CTAs per SM for the chosen shape
+			for (int occ = 1; occ <= 4 && st == IBK_OK; ++occ) {
+				ibk_batch_config c = cur;
+				(spread_pass ? c.spread_ctas_per_sm : c.interp_ctas_per_sm) = occ;
+				float ms = 0.0f;
+				ibk_status cs = time_cfg(c, ms);
+				if (cs != IBK_OK) { st = cs; break; }
+				if (ms < best_ms) { best_ms = ms; cur = c; }
+			}
+		}
+	}
+	cudaEventDestroy(e0);
+	cudaEventDestroy(e1);
+	ibk_status fs = configure(*b, cur);
+	if (st == IBK_OK) st = fs;
+	if (st == IBK_OK && best) *best = cur;
+	return st;
+}
+
+ibk_status ibk_batch_launch_count(ibk_batch handle, long long* launches)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b || !launches) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or output");
+	*launches = b->launches;
+	return IBK_OK;
+}
+
+ibk_status ibk_batch_check(ibk_batch handle)
+{
+	Batch* b = reinterpret_cast<Batch*>(handle);
+	if (!b) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch");
+	int st[4] = {0, 0, 0, 0};
+	ibk_status s = cuda_check(cudaMemcpy(st, b->d_status, sizeof(st), cudaMemcpyDeviceToHost), "cudaMemcpy");
+	if (s != IBK_OK) return s;
+	if (st[0] == 0) return IBK_OK;
+	cudaMemset(b->d_status, 0, sizeof(int) * 4);
+	return set_error(IBK_ERR_DEVICE_CHECK, "device check tripped (code " + std::to_string(st[0]) + ")");
+}
+
+} // extern "C"

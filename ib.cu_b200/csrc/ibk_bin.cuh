@@ -53,60 +53,69 @@ __device__ __forceinline__ AxisReach<M> axis_reach(const GridGeom& g, const Tile
 	return r;
 }
 
-// With f != nullptr (spread) the kernel also writes this block's max|F| per
-// component to fpart[block * 3 + c]; bin_chunk_sum_kernel folds the partials.
+// Bin of point p: home tile * 3^dims + reach class.
 template <int M, int DIMS>
-__global__ void __launch_bounds__(256)
-bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                 int* __restrict__ count, int2* __restrict__ key_rank,
-                 const double* __restrict__ f, float* __restrict__ fpart)
+__device__ __forceinline__ int bin_key(const GridGeom& g, const TileGeom& tg, const double* __restrict__ x,
+                                       int n, int p)
 {
-	const int p = blockIdx.x * blockDim.x + threadIdx.x;
-	const bool active = p < n;
-	if (f != nullptr) {
-		__shared__ float wmax[8][kMaxDims];
+	int tile = 0, cls = 0, ts = 1, cs = 1;
 #pragma unroll
-		for (int c = 0; c < DIMS; ++c) {
-			float a = active ? fabsf((float) __ldg(f + (size_t) c * n + p)) : 0.0f;
-#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) a = fmaxf(a, __shfl_xor_sync(0xffffffffu, a, o));
-			if ((threadIdx.x & 31) == 0) wmax[threadIdx.x >> 5][c] = a;
-		}
-		__syncthreads();
-		if (threadIdx.x < DIMS) {
-			float a = 0.0f;
-			for (int w = 0; w < (int) (blockDim.x >> 5); ++w) a = fmaxf(a, wmax[w][threadIdx.x]);
-			fpart[blockIdx.x * kMaxDims + threadIdx.x] = a;
-		}
+	for (int d = 0; d < DIMS; ++d) {
+		AxisReach<M> r = axis_reach<M, DIMS>(g, tg, d, __ldg(x + (size_t) d * n + p));
+		const int t = r.home / tg.T[d];
+		const int tlo = t * tg.T[d];
+		const int thi = min(tlo + tg.T[d], tg.cells[d]);
+		int c = 1;
+		if (tg.ntiles[d] > 1) c = r.node_lo < tlo ? 0 : (r.node_hi >= thi ? 2 : 1);
+		tile += t * ts;
+		ts *= tg.ntiles[d];
+		cls += c * cs;
+		cs *= 3;
 	}
-	int key = 0;
-	if (active) {
-		int tile = 0, cls = 0, ts = 1, cs = 1;
-#pragma unroll
-		for (int d = 0; d < DIMS; ++d) {
-			AxisReach<M> r = axis_reach<M, DIMS>(g, tg, d, __ldg(x + (size_t) d * n + p));
-			const int t = r.home / tg.T[d];
-			const int tlo = t * tg.T[d];
-			const int thi = min(tlo + tg.T[d], tg.cells[d]);
-			int c = 1;
-			if (tg.ntiles[d] > 1) c = r.node_lo < tlo ? 0 : (r.node_hi >= thi ? 2 : 1);
-			tile += t * ts;
-			ts *= tg.ntiles[d];
-			cls += c * cs;
-			cs *= 3;
-		}
-		key = tile * tg.nclass + cls;
-	}
-	const unsigned mask = __ballot_sync(0xffffffffu, active);
-	if (!active) return;
+	return tile * tg.nclass + cls;
+}
+
+// Warp-aggregated rank of a point in its bin (one atomic per group of lanes
+// sharing a key); with f != nullptr also raises binmax[key * 3 + c] to the
+// FP32 |f[c * n + p]| of the group.  Every lane of `mask` must call it, all
+// with f null or all with f set.
+template <int DIMS>
+__device__ __forceinline__ void bin_rank(unsigned mask, int key, int* __restrict__ count, int2* __restrict__ kr_out,
+                                         const double* __restrict__ f, int n, int p, unsigned* __restrict__ binmax)
+{
 	const int lane = threadIdx.x & 31;
 	const unsigned peers = __match_any_sync(mask, key);
 	const int leader = __ffs(peers) - 1;
 	int base = 0;
 	if (lane == leader) base = atomicAdd(count + key, __popc(peers));
 	base = __shfl_sync(peers, base, leader);
-	const int rank = base + __popc(peers & ((1u << lane) - 1u));
-	key_rank[p] = make_int2(key, rank);
+	*kr_out = make_int2(key, base + __popc(peers & ((1u << lane) - 1u)));
+	if (f != nullptr) {
+#pragma unroll
+		for (int c = 0; c < DIMS; ++c) {
+			const unsigned v = __float_as_uint(fabsf((float) __ldg(f + (size_t) c * n + p)));
+			const unsigned m = __reduce_max_sync(peers, v);
+			if (lane == leader && m != 0u) atomicMax(binmax + (size_t) key * kMaxDims + c, m);
+		}
+	}
+}
+
+// With f != nullptr (spread) the kernel also raises binmax[key * 3 + c] to
+// the FP32 |F| of every point of the bin, per component; binmax starts at
+// zero and, as all values are non-negative floats, compares as unsigned bit
+// patterns.  The maximum does not depend on the order of the atomics.
+template <int M, int DIMS>
+__global__ void __launch_bounds__(256)
+bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                 int* __restrict__ count, int2* __restrict__ key_rank,
+                 const double* __restrict__ f, unsigned* __restrict__ binmax)
+{
+	const int p = blockIdx.x * blockDim.x + threadIdx.x;
+	const bool active = p < n;
+	const int key = active ? bin_key<M, DIMS>(g, tg, x, n, p) : 0;
+	const unsigned mask = __ballot_sync(0xffffffffu, active);
+	if (!active) return;
+	bin_rank<DIMS>(mask, key, count, key_rank + p, f, n, p, binmax);
 }
 
 // Exclusive scan of the bin counts in two launches.  Each CTA owns a chunk
@@ -144,31 +153,9 @@ __device__ __forceinline__ int block_exclusive_scan(int v, int& total)
 	return r;
 }
 
-// Also folds the per-block max|F| partials of bin_count_kernel (nparts
-// blocks; none when fpart is null) into fmax[0..2] with one atomic per CTA.
 static __global__ void __launch_bounds__(kScanThreads)
-bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int num_bins,
-                     const float* __restrict__ fpart, int nparts, float* __restrict__ fmax)
+bin_chunk_sum_kernel(const int* __restrict__ count, int* __restrict__ chunk, int num_bins)
 {
-	if (fpart != nullptr) {
-		__shared__ float red[32][kMaxDims];
-		float a[kMaxDims] = {0.f, 0.f, 0.f};
-		for (int b = blockIdx.x * kScanThreads + threadIdx.x; b < nparts; b += gridDim.x * kScanThreads)
-#pragma unroll
-			for (int c = 0; c < kMaxDims; ++c) a[c] = fmaxf(a[c], fpart[b * kMaxDims + c]);
-#pragma unroll
-		for (int c = 0; c < kMaxDims; ++c) {
-#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) a[c] = fmaxf(a[c], __shfl_xor_sync(0xffffffffu, a[c], o));
-			if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5][c] = a[c];
-		}
-		__syncthreads();
-		if (threadIdx.x < kMaxDims) {
-			float m = 0.f;
-			for (int w = 0; w < kScanThreads / 32; ++w) m = fmaxf(m, red[w][threadIdx.x]);
-			atomicMax(reinterpret_cast<int*>(fmax) + threadIdx.x, __float_as_int(m));
-		}
-	}
 	const int i0 = blockIdx.x * kScanChunk + threadIdx.x * 4;
 	int v = 0;
 	if (i0 + 3 < num_bins) {

@@ -76,7 +76,7 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 }
 
 // Scratch slots of a plan.
-enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotFmax = 5 };
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotBinMax = 5 };
 
 // Tile decomposition of a plan's grid for stencil width M.
 // pref_extent: preferred tile extent per axis (nullptr: 16 cells).
@@ -87,6 +87,16 @@ const OpTable* find_ops(int kind, int order, int dims, int precision);
 
 // Grow scratch slot `slot` of the plan to at least `bytes`.
 ibk_status ensure_scratch(Plan& plan, int slot, size_t bytes, cudaStream_t stream, bool zero = false);
+
+// Stencil width M of a delta (1 + order for bspline<order>).
+int meshwidths_of(int kind, int order);
+
+// Validation of a domain / tag / refinement triple (status + message).
+ibk_status check_domain(const ibk_domain* domain, int tag, int refinement);
+
+// Geometry of every component grid of a validated domain.
+ibk_status make_geometry(const ibk_domain* domain, int tag, int refinement, int meshwidths, GridGeom& g,
+                         ibk_grid_info& info);
 
 ibk_status set_error(ibk_status s, const std::string& msg);
 ibk_status check_launch(const char* what);

@@ -171,7 +171,7 @@ ibk_status run(const GridGeom& g, int tag, int n, const double* x, ConstCompPtrs
 	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
 	bin_count_kernel<M, DIMS><<<nb, 256, 0, stream>>>(g, tg, n, x, count, kr, nullptr, nullptr);
 	if ((s = check_launch("bin_count_kernel")) != IBK_OK) return s;
-	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, stream>>>(count, chunk, tg.num_bins, nullptr, 0, nullptr);
+	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, stream>>>(count, chunk, tg.num_bins);
 	if ((s = check_launch("bin_chunk_sum_kernel")) != IBK_OK) return s;
 	bin_scan_kernel<<<nchunks, kScanThreads, 0, stream>>>(count, chunk, off, tg.num_bins, nchunks);
 	if ((s = check_launch("bin_scan_kernel")) != IBK_OK) return s;

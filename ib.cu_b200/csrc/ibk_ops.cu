@@ -40,7 +40,7 @@ ibk_status interp_direct(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* 
 // Counting sort of the points by (tile, reach class): perm + bin offsets.
 template <int M, int DIMS>
 ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, int** perm_out, int** off_out,
-                      const double* f = nullptr, float** fmax_out = nullptr)
+                      const double* f = nullptr, unsigned** binmax_out = nullptr)
 {
 	ibk_status s;
 	const int need = a.n > plan.reserved_points ? a.n : plan.reserved_points;
@@ -54,25 +54,24 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, int** per
 	int* perm = static_cast<int*>(plan.scratch[kSlotPerm].ptr);
 	const GridGeom& g = *a.g;
 	const int nb = blocks_for(a.n, 256);
-	float* fmax = nullptr;
-	float* fpart = nullptr;
+	unsigned* binmax = nullptr;
 	if (f) {
-		// fmax[0..2] followed by one partial per bin_count block
-		if ((s = ensure_scratch(plan, kSlotFmax, sizeof(float) * kMaxDims * ((size_t) nb + 1), a.stream)) != IBK_OK) return s;
-		fmax = static_cast<float*>(plan.scratch[kSlotFmax].ptr);
-		fpart = fmax + kMaxDims;
-		cudaError_t e = cudaMemsetAsync(fmax, 0, sizeof(float) * kMaxDims, a.stream);
+		// per-bin, per-component max|F| (FP32 bit patterns), zeroed each call
+		const size_t bytes = sizeof(unsigned) * kMaxDims * (size_t) tg.num_bins;
+		if ((s = ensure_scratch(plan, kSlotBinMax, bytes, a.stream)) != IBK_OK) return s;
+		binmax = static_cast<unsigned*>(plan.scratch[kSlotBinMax].ptr);
+		cudaError_t e = cudaMemsetAsync(binmax, 0, bytes, a.stream);
 		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
-		*fmax_out = fmax;
+		*binmax_out = binmax;
 	}
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
-		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, f, fpart);
+		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, f, binmax);
 	})) != IBK_OK) return s;
 	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
 	if ((s = ensure_scratch(plan, kSlotChunk, sizeof(int) * ((size_t) nchunks + 1), a.stream)) != IBK_OK) return s;
 	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
 	if ((s = launch(plan, "bin_chunk_sum_kernel", a.stream, [&] {
-		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins, fpart, nb, fmax);
+		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scan_kernel", a.stream, [&] {
 		bin_scan_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, off, tg.num_bins, nchunks);
@@ -103,8 +102,9 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	const TileGeom& tg = plan.spread_tiles;
 	if (!plan.tiled) return spread_direct<D, DIMS>(plan, a, fl, fe);
 	int *perm = nullptr, *off = nullptr;
-	float* fmax = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off, fl, &fmax);
+	unsigned* binmax = nullptr;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off,
+	                                      PREC == IBK_PRECISION_FP32C ? fl : nullptr, &binmax);
 	if (s != IBK_OK) return s;
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	// FP64: one double per face; FP32C: an FP64 total and a 32-bit working word
@@ -113,7 +113,7 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	auto kern = spread_tile_kernel<D, DIMS, PREC>;
 	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
 	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, fmax, fe);
+		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, binmax, fe);
 	});
 }
 
@@ -230,9 +230,10 @@ const Entry kTable[] = {
 
 } // namespace
 
-// Tile extent per axis: 16 cells where the last tile keeps at least M cells
-// (a stencil can then reach at most one neighbour per side), otherwise the
-// nearest size in [8, 20] that does; axes of at most 16 cells are one tile.
+// Tile extent per axis: the preferred extent (16 cells by default) where the
+// last tile keeps at least M cells (a stencil can then reach at most one
+// neighbour per side), otherwise the nearest size that does; an axis no
+// longer than the preferred extent is one tile.
 TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
 {
 	TileGeom tg{};
@@ -249,11 +250,15 @@ TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
 			static const int prefs[] = {16, 14, 18, 12, 20, 10, 8, 9, 11, 13, 15, 17, 19};
 			T = 0;
 			if (want != 16) {
-				// a larger preferred extent first, then the regular ladder
-				for (int t = want; t >= 22 && T == 0; t -= 2) {
-					const int r = cells % t;
-					if (r == 0 || r >= minlast) T = t;
-				}
+				// the preferred extent, then its nearest neighbours (larger
+				// first), then the regular ladder
+				for (int dist = 0; dist <= 6 && T == 0; ++dist)
+					for (int sgn = 1; sgn >= -1 && T == 0; sgn -= 2) {
+						const int t = want + sgn * dist;
+						if (t < minlast || t < 4 || t >= cells) continue;
+						const int r = cells % t;
+						if (r == 0 || r >= minlast) T = t;
+					}
 			}
 			for (int i = 0; i < (int) (sizeof(prefs) / sizeof(prefs[0])) && T == 0; ++i) {
 				const int r = cells % prefs[i];

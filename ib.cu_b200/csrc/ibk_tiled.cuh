@@ -82,15 +82,18 @@ struct RangeTable {
 	int start[kMaxRanges];
 	int pref[kMaxRanges + 1];
 	int count;
+	unsigned fmax_bits;     // spread: max over the candidate bins of binmax[bin][comp]
 };
 
 template <int DIMS>
 __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& tg, const int* tc,
-                                             const int* __restrict__ off, RangeTable& rt, bool neighbours)
+                                             const int* __restrict__ off, RangeTable& rt, bool neighbours,
+                                             const unsigned* __restrict__ binmax = nullptr, int comp = 0)
 {
 	const int nent = neighbours ? (DIMS == 3 ? 125 : 25) : 1;
 	const int tid = threadIdx.x;
 	int len = 0, st = 0;
+	unsigned fm = 0;
 	if (tid < nent) {
 		int tile = 0, cls = 0, ts = 1, cs = 1;
 		bool ok = true;
@@ -120,11 +123,13 @@ __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& 
 			const int bin = tile * tg.nclass + cls;
 			st = off[bin];
 			len = off[bin + 1] - st;
+			if (binmax != nullptr && len > 0) fm = binmax[(size_t) bin * kMaxDims + comp];
 		}
 		rt.start[tid] = st;
 	}
 	// block-wide exclusive scan of len over the first 128 threads
 	__shared__ int warp_tot[4];
+	__shared__ unsigned warp_fm[4];
 	const int lane = tid & 31, warp = tid >> 5;
 	int incl = (tid < 128) ? len : 0;
 	if (tid < 128) {
@@ -133,7 +138,11 @@ __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& 
 			int v = __shfl_up_sync(0xffffffffu, incl, o);
 			if (lane >= o) incl += v;
 		}
-		if (lane == 31) warp_tot[warp] = incl;
+		const unsigned wm = __reduce_max_sync(0xffffffffu, fm);
+		if (lane == 31) {
+			warp_tot[warp] = incl;
+			warp_fm[warp] = wm;
+		}
 	}
 	__syncthreads();
 	if (tid < 128) {
@@ -143,6 +152,7 @@ __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& 
 		if (tid == nent - 1) {
 			rt.pref[nent] = base + incl;
 			rt.count = nent;
+			rt.fmax_bits = max(max(warp_fm[0], warp_fm[1]), max(warp_fm[2], warp_fm[3]));
 		}
 	}
 	__syncthreads();
@@ -179,39 +189,118 @@ template <typename D, int DIMS>
 struct SpreadSmem<D, DIMS, IBK_PRECISION_FP32C> { using acc_t = int; };
 
 // Fixed point of the FP32C spread.  Each FP32 product is scaled so that the
-// largest possible term (max|w| * res * max|F|) is at most 2^21, rounded to
-// an integer with the float magic number 1.5 * 2^23 (x + magic carries rint(x)
-// in its low mantissa bits for |x| < 2^22: an FADD and an integer subtract,
-// no conversion instruction), and added to the face's 32-bit working word
-// with one integer shared atomic.  At most kFixChunk candidates are summed
-// between folds (kFixChunk * 2^21 < 2^31, so a working word cannot overflow);
-// each fold adds the working words exactly into an FP64 total per face
-// (integers below 2^53 are exact in FP64).  The sum is therefore exact and
-// order-independent; the only rounding is each product's quantisation to
-// 2^-22 of the largest possible term.
+// largest possible term of the tile (max|w| * res * max|F| over the tile's
+// candidate points) is below 2^22, rounded to an integer with the float magic
+// number 1.5 * 2^23 (x + magic carries rint(x) in its low mantissa bits for
+// |x| <= 2^22: an FADD and an integer subtract, no conversion instruction),
+// and added to the face's 32-bit working word with one integer shared atomic.
+// At most kFixChunk candidates are summed between folds (kFixChunk * 2^22 <
+// 2^31, so a working word cannot overflow); each fold adds the working words
+// exactly into an FP64 total per face (integers below 2^53 are exact in
+// FP64).  The sum is therefore exact and independent of the order in which
+// points are visited (the binning order is not deterministic; the result
+// is); the only rounding is each product's quantisation to 2^-23 of the
+// tile's largest possible term, and the final scaling is exact.
 constexpr float kMagic = 12582912.0f;           // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
-constexpr int kFixChunk = 1000;                 // candidates between folds
-constexpr int kFixTermLog2 = 21;                // largest term * scale <= 2^21
+constexpr int kFixChunk = 511;                  // candidates between folds
+constexpr int kFixTermLog2 = 22;                // largest term * scale < 2^22
 
 __device__ __forceinline__ void fix_add(int* word, float s)
 {
 	atomicAdd(word, __float_as_int(s + kMagic) - kMagicBits);   // rint(s)
 }
 
+// One candidate point p of a spread tile [lo, hi): its in-tile stencil
+// contributions added to the tile's accumulators (F is read only when the
+// stencil touches the tile).  FP32C: the FP32 product res * F is scaled by
+// the tile's fixed-point scale.
 template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads)
-spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                   const double* __restrict__ fl, const int* __restrict__ perm,
-                   const int* __restrict__ off, const float* __restrict__ fmax, CompPtrs fe)
+__device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGeom& cg, int n,
+                                                 const double* __restrict__ x, const double* __restrict__ fc,
+                                                 int p, float scale, const int* lo, const int* hi, int T0, int T1,
+                                                 typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
 {
-	// grid: (tile, component)
+	constexpr int M = D::M, sh = (M - 1) >> 1;
+	int loc[DIMS][M];
+	unsigned mask[DIMS];
+	double dl[DIMS];
+	bool any = true;
+#pragma unroll
+	for (int d = 0; d < DIMS; ++d) {
+		AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
+		dl[d] = a.delta;
+		unsigned mk = 0;
+#pragma unroll
+		for (int m = 0; m < M; ++m) {
+			// spread drops nodes outside [0, points) (errors_negative);
+			// this tile owns [lo, hi)
+			const int j = node_index(g, cg, d, a.base + m - sh);
+			loc[d][m] = j - lo[d];
+			mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
+		}
+		mask[d] = mk;
+		any = any && mk;
+	}
+	if (!any) return;
+	if constexpr (PREC == IBK_PRECISION_FP64) {
+		const double f = __dmul_rn(g.res, __ldg(fc + p));
+		double w[DIMS][M];
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d)
+#pragma unroll
+			for (int m = 0; m < M; ++m)
+				w[d][m] = (mask[d] >> m & 1u) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
+#pragma unroll
+		for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
+#pragma unroll
+		for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+			const int m1 = r % M, m2 = r / M;
+			const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+			if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
+			const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
+			const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
+#pragma unroll
+			for (int m0 = 0; m0 < M; ++m0)
+				if ((mask[0] >> m0) & rm)
+					atomicAdd(acc + row + loc[0][m0], __dmul_rn(w[0][m0], w12));
+		}
+	} else {
+		const float f = (float) (g.res * __ldg(fc + p)) * scale;
+		float w[DIMS][M];
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
+#pragma unroll
+		for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
+#pragma unroll
+		for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+			const int m1 = r % M, m2 = r / M;
+			const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+			if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
+			const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+			const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
+#pragma unroll
+			for (int m0 = 0; m0 < M; ++m0)
+				if ((mask[0] >> m0) & rm)
+					fix_add(acc + row + loc[0][m0], w[0][m0] * w12);
+		}
+	}
+}
+
+// One (tile, component) of the spread; every thread of the CTA calls it.
+// perm holds point indices offset by pbase (a batch numbers the points of
+// all its instances consecutively); off and binmax are this grid's bins.
+template <typename D, int DIMS, int PREC>
+__device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
+                                            const double* __restrict__ fl, const int* __restrict__ perm, int pbase,
+                                            const int* __restrict__ off, const unsigned* __restrict__ binmax,
+                                            const CompPtrs& fe, int tile, int c)
+{
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ RangeTable rt;
 
-	const int c = blockIdx.y;
 	const CompGeom& cg = g.comp[c];
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
 	const int TV = T0 * T1 * T2;
@@ -220,100 +309,53 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	acc_t* acc = PREC == IBK_PRECISION_FP64 ? reinterpret_cast<acc_t*>(smem_raw)
 	                                        : reinterpret_cast<acc_t*>(total + TV);
 	int tc[3] = {0, 0, 0};
-	tile_coords(tg, blockIdx.x, tc);
+	tile_coords(tg, tile, tc);
 	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
 		lo[d] = tc[d] * tg.T[d];
 		hi[d] = min(lo[d] + tg.T[d], cg.points[d]);
 	}
+	build_ranges<DIMS>(g, tg, tc, off, rt, true, binmax, c);
+	const double* __restrict__ fc = fl + (size_t) c * n;
+	const int e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = DIMS == 3 ? hi[2] - lo[2] : 1;
+	double* __restrict__ out = fe.p[c];
+	const int ncand = rt.pref[rt.count];
+	if (ncand == 0) {
+		// no point reaches the tile: its faces are zero
+		for (int i = threadIdx.x; i < e1 * e2 * T0; i += kTileThreads) {
+			const int l0 = i % T0;
+			const int r = i / T0;
+			if (l0 >= e0) continue;
+			const int l1 = r % e1, l2 = r / e1;
+			out[(size_t) (lo[0] + l0) + (size_t) cg.points[0] *
+			    ((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0))] = 0.0;
+		}
+		return;
+	}
 	for (int i = threadIdx.x; i < TV; i += kTileThreads) acc[i] = (acc_t) 0;
 	if constexpr (PREC == IBK_PRECISION_FP32C)
 		for (int i = threadIdx.x; i < TV; i += kTileThreads) total[i] = 0.0;
-	build_ranges<DIMS>(g, tg, tc, off, rt, true);
-	const double* __restrict__ fc = fl + (size_t) c * n;
+	__syncthreads();
 
-	// FP32C: the largest possible single term, max|F| * max|w| * res, is
-	// scaled to at most 2^21
-	float scale = 1.0f;
-	if constexpr (PREC == IBK_PRECISION_FP32C) {
-		const float bound = __ldg(fmax + c) * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
+	double inv_scale = 1.0;     // FP32C: back to force density (exact power of two)
+	if constexpr (PREC == IBK_PRECISION_FP64) {
+		for (int it = threadIdx.x; it < ncand; it += kTileThreads)
+			spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, 0.0f,
+			                                lo, hi, T0, T1, acc);
+	} else {
+		// the tile's largest possible term, max|F| * max|w| * res (max|F| over
+		// its candidate bins, rounded to FP32, hence the 1.001), is scaled to
+		// below 2^22; at most kFixChunk candidates between folds
+		const float bound = __uint_as_float(rt.fmax_bits) * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
 		int e;
 		frexpf(bound, &e);                      // bound < 2^e
-		scale = ldexpf(1.0f, min(kFixTermLog2 - e, 126));
-	}
-
-	const int ncand = rt.pref[rt.count];
-	const int chunk = PREC == IBK_PRECISION_FP32C ? kFixChunk : max(ncand, 1);
-	for (int base = 0; base < ncand; base += chunk) {
-		const int stop = min(ncand, base + chunk);
-		for (int it = base + threadIdx.x; it < stop; it += kTileThreads) {
-			const int p = __ldg(perm + range_lookup(rt, it));
-			int loc[DIMS][M];
-			unsigned mask[DIMS];
-			double dl[DIMS];
-			bool any = true;
-#pragma unroll
-			for (int d = 0; d < DIMS; ++d) {
-				AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
-				dl[d] = a.delta;
-				unsigned mk = 0;
-#pragma unroll
-				for (int m = 0; m < M; ++m) {
-					// spread drops nodes outside [0, points) (errors_negative);
-					// this tile owns [lo, hi)
-					const int j = node_index(g, cg, d, a.base + m - sh);
-					loc[d][m] = j - lo[d];
-					mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
-				}
-				mask[d] = mk;
-				any = any && mk;
-			}
-			if (!any) continue;
-			if constexpr (PREC == IBK_PRECISION_FP64) {
-				const double f = __dmul_rn(g.res, __ldg(fc + p));
-				double w[DIMS][M];
-#pragma unroll
-				for (int d = 0; d < DIMS; ++d)
-#pragma unroll
-					for (int m = 0; m < M; ++m)
-						w[d][m] = (mask[d] >> m & 1u) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
-#pragma unroll
-				for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
-#pragma unroll
-				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-					const int m1 = r % M, m2 = r / M;
-					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
-					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
-					const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
-					const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
-#pragma unroll
-					for (int m0 = 0; m0 < M; ++m0)
-						if ((mask[0] >> m0) & rm)
-							atomicAdd(acc + row + loc[0][m0], __dmul_rn(w[0][m0], w12));
-				}
-			} else {
-				const float f = (float) (g.res * __ldg(fc + p)) * scale;
-				float w[DIMS][M];
-#pragma unroll
-				for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
-#pragma unroll
-				for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
-#pragma unroll
-				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-					const int m1 = r % M, m2 = r / M;
-					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
-					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
-					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-					const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
-#pragma unroll
-					for (int m0 = 0; m0 < M; ++m0)
-						if ((mask[0] >> m0) & rm)
-							fix_add(acc + row + loc[0][m0], w[0][m0] * w12);
-				}
-			}
-		}
-		if constexpr (PREC == IBK_PRECISION_FP32C) {
+		const float scale = ldexpf(1.0f, min(kFixTermLog2 - e, 126));
+		for (int base = 0; base < ncand; base += kFixChunk) {
+			const int stop = min(ncand, base + kFixChunk);
+			for (int it = base + threadIdx.x; it < stop; it += kTileThreads)
+				spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, scale,
+				                                lo, hi, T0, T1, acc);
 			// fold the working words into the exact FP64 totals
 			__syncthreads();
 			for (int i = threadIdx.x; i < TV; i += kTileThreads) {
@@ -322,13 +364,11 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			}
 			__syncthreads();
 		}
+		inv_scale = 1.0 / (double) scale;
 	}
 	__syncthreads();
 
 	// every face of the tile, written once
-	const int e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = DIMS == 3 ? hi[2] - lo[2] : 1;
-	const double inv = 1.0 / (double) scale;
-	double* __restrict__ out = fe.p[c];
 	for (int i = threadIdx.x; i < e1 * e2 * T0; i += kTileThreads) {
 		const int l0 = i % T0;
 		const int r = i / T0;
@@ -338,8 +378,18 @@ spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
 		const int li = (l2 * T1 + l1) * T0 + l0;
 		if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = acc[li];
-		else out[gi] = total[li] * inv;
+		else out[gi] = total[li] * inv_scale;
 	}
+}
+
+template <typename D, int DIMS, int PREC>
+__global__ void __launch_bounds__(kTileThreads)
+spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                   const double* __restrict__ fl, const int* __restrict__ perm,
+                   const int* __restrict__ off, const unsigned* __restrict__ binmax, CompPtrs fe)
+{
+	// grid: (tile, component)
+	spread_tile<D, DIMS, PREC>(g, tg, n, x, fl, perm, 0, off, binmax, fe, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------ interp ---
@@ -368,14 +418,27 @@ __host__ __device__ inline int region_extent(int T, int d)
 	return d == 0 ? (e + 1) & ~1 : e;
 }
 
+// Epilogue of the serving step, applied to each interpolated velocity U of
+// component c at point p: forward Euler advection and a linear spring to the
+// point's reference position,
+//   xn = x + dt * U,   fl = -k * (xn - xref)    (FP64, no contraction).
+struct StepEpilogue {
+	double* xn;             // 3n, advected positions
+	double* fl;             // 3n, spring forces at xn
+	const double* xref;     // 3n, reference positions
+	double dt, k;
+};
+
+// One (tile, component) of the interpolation; every thread of the CTA calls
+// it.  maps/use_tma select TMA staging (single-grid launches only); epi, when
+// not null, adds the serving-step epilogue; ul may then be null.
 template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
-interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                   const int* __restrict__ perm, const int* __restrict__ off,
-                   ConstCompPtrs ue, double* __restrict__ ul,
-                   const __grid_constant__ TmaMaps maps, int use_tma, int* status)
+__device__ __forceinline__ void interp_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
+                                            const int* __restrict__ perm, int pbase, const int* __restrict__ off,
+                                            const ConstCompPtrs& ue, double* __restrict__ ul,
+                                            const CUtensorMap* maps, int use_tma, int* status,
+                                            const StepEpilogue* epi, int t, int c)
 {
-	// grid: (tile, component)
 	using P = Pattern<D::M, DIMS, D::every_other>;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	constexpr int HL = Halo<M>::lo;
@@ -385,8 +448,6 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	double* reg = reinterpret_cast<double*>(interp_smem + ((128u - (smem_addr(interp_smem) & 127u)) & 127u));
 	__shared__ __align__(8) uint64_t bar;
 
-	const int t = blockIdx.x;
-	const int c = blockIdx.y;
 	const int start = __ldg(off + t * tg.nclass);
 	const int end = __ldg(off + (t + 1) * tg.nclass);
 	if (start == end) return;
@@ -415,7 +476,7 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	int p_next = 0;
 	double z_next[DIMS];
 	if (it < end) {
-		p_next = __ldg(perm + it);
+		p_next = __ldg(perm + it) - pbase;
 #pragma unroll
 		for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
 	}
@@ -427,8 +488,8 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 		__syncthreads();
 		if (threadIdx.x == 0) {
 			mbar_arrive_expect_tx(&bar, (unsigned) (sizeof(double) * E[0] * E[1] * E[2]));
-			if constexpr (DIMS == 3) tma_load_3d(reg, &maps.map[c], rlo[0], rlo[1], rlo[2], &bar);
-			else tma_load_2d(reg, &maps.map[c], rlo[0], rlo[1], &bar);
+			if constexpr (DIMS == 3) tma_load_3d(reg, maps + c, rlo[0], rlo[1], rlo[2], &bar);
+			else tma_load_2d(reg, maps + c, rlo[0], rlo[1], &bar);
 		}
 		// one thread polls the mbarrier; the others park at the CTA barrier
 		// (no issue slots spent spinning)
@@ -472,28 +533,60 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 			__syncthreads();
 		}
 	} else {
-		// plain row copies that wrap periodic and clamp solid halos
+		// plain row copies that wrap periodic and clamp solid halos: a warp
+		// per row, lanes along x, kRowsInFlight rows' loads issued before
+		// their stores
+		constexpr int kRowsInFlight = 4;
+		constexpr int kWarps = kTileThreads / 32;
 		const int rows = E[1] * E[2];
 		const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
-		for (int r = warp; r < rows; r += kTileThreads / 32) {
-			const int l1 = r % E[1], l2 = r / E[1];
-			size_t rb = (size_t) fold(g, cg, 1, rlo[1] + l1);
-			if (DIMS == 3) rb += (size_t) cg.points[1] * (size_t) fold(g, cg, 2, rlo[2] + l2);
-			rb *= (size_t) cg.points[0];
-			double* dst = reg + (size_t) r * E[0];
-			for (int l0 = lane; l0 < E[0]; l0 += 32)
-				dst[l0] = __ldg(u + rb + fold(g, cg, 0, rlo[0] + l0));
+		for (int r0 = warp; r0 < rows; r0 += kWarps * kRowsInFlight) {
+			double v[kRowsInFlight][2];
+#pragma unroll
+			for (int q = 0; q < kRowsInFlight; ++q) {
+				const int r = r0 + q * kWarps;
+				if (r >= rows) break;
+				const int l1 = r % E[1], l2 = r / E[1];
+				size_t rb = (size_t) fold(g, cg, 1, rlo[1] + l1);
+				if (DIMS == 3) rb += (size_t) cg.points[1] * (size_t) fold(g, cg, 2, rlo[2] + l2);
+				rb *= (size_t) cg.points[0];
+#pragma unroll
+				for (int h = 0; h < 2; ++h) {
+					const int l0 = lane + 32 * h;
+					if (l0 < E[0]) v[q][h] = __ldg(u + rb + fold(g, cg, 0, rlo[0] + l0));
+				}
+			}
+#pragma unroll
+			for (int q = 0; q < kRowsInFlight; ++q) {
+				const int r = r0 + q * kWarps;
+				if (r >= rows) break;
+#pragma unroll
+				for (int h = 0; h < 2; ++h) {
+					const int l0 = lane + 32 * h;
+					if (l0 < E[0]) reg[(size_t) r * E[0] + l0] = v[q][h];
+				}
+			}
+		}
+		// wider regions (x extent above 64) finish row by row
+		if (E[0] > 64) {
+			for (int r = warp; r < rows; r += kWarps) {
+				const int l1 = r % E[1], l2 = r / E[1];
+				size_t rb = (size_t) fold(g, cg, 1, rlo[1] + l1);
+				if (DIMS == 3) rb += (size_t) cg.points[1] * (size_t) fold(g, cg, 2, rlo[2] + l2);
+				rb *= (size_t) cg.points[0];
+				for (int l0 = 64 + lane; l0 < E[0]; l0 += 32)
+					reg[(size_t) r * E[0] + l0] = __ldg(u + rb + fold(g, cg, 0, rlo[0] + l0));
+			}
 		}
 		__syncthreads();
 	}
-	double* __restrict__ out = ul + (size_t) c * n;
 	for (; it < end; it += kTileThreads) {
 		const int p = p_next;
 		double z[DIMS];
 #pragma unroll
 		for (int d = 0; d < DIMS; ++d) z[d] = z_next[d];
 		if (it + kTileThreads < end) {          // prefetch the next point
-			p_next = __ldg(perm + it + kTileThreads);
+			p_next = __ldg(perm + it + kTileThreads) - pbase;
 #pragma unroll
 			for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
 		}
@@ -594,8 +687,29 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 				v = __dadd_rn(v, __dmul_rn(wt, __ldg(u + k)));
 			}
 		}
-		out[p] = v;
+		const size_t i = (size_t) c * n + p;
+		if (ul != nullptr) ul[i] = v;
+		if (epi != nullptr) {
+			double zc = z[0];
+#pragma unroll
+			for (int d = 1; d < DIMS; ++d) zc = d == c ? z[d] : zc;
+			const double xn = __dadd_rn(zc, __dmul_rn(epi->dt, v));
+			epi->xn[i] = xn;
+			epi->fl[i] = __dmul_rn(-epi->k, __dsub_rn(xn, __ldg(epi->xref + i)));
+		}
 	}
+}
+
+template <typename D, int DIMS, int PREC>
+__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
+interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                   const int* __restrict__ perm, const int* __restrict__ off,
+                   ConstCompPtrs ue, double* __restrict__ ul,
+                   const __grid_constant__ TmaMaps maps, int use_tma, int* status)
+{
+	// grid: (tile, component)
+	interp_tile<D, DIMS, PREC>(g, tg, n, x, perm, 0, off, ue, ul, maps.map, use_tma, status, nullptr,
+	                           blockIdx.x, blockIdx.y);
 }
 
 } // namespace ibk

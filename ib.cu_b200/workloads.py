@@ -236,6 +236,28 @@ def ensemble_instance(rng: np.random.Generator, name: str = "instance") -> Workl
     return w
 
 
+def small_instance(rng: np.random.Generator, side: int, ncell: int, walls: bool = False,
+                   name: str = "small") -> Workload:
+    """A test-sized instance: side^3 cells of h = 0.25 um (a walled channel
+    along y when walls is set), ncell platelets or small RBCs (386 / 864
+    points) placed at random (inside the walls, overlaps allowed)."""
+    L = side * H_UM
+    parts, cells = [], []
+    for _ in range(ncell):
+        kind, npts = [("plt", 386), ("rbc", 864)][int(rng.integers(0, 2))]
+        ref = rbc_surface(npts) if kind == "rbc" else platelet_surface(npts)
+        centre = rng.uniform(0, L, size=3)
+        if walls:
+            centre[1] = rng.uniform(0.45 * L, 0.55 * L)
+            ref = ref * min(1.0, 0.3 * L / RBC_RADIUS_UM)
+        parts.append((ref @ random_rotation(rng).T + centre) * UM)
+        cells.append((kind, npts))
+    w = Workload(f"{name}-{side}^3", [L * UM] * 3, [0, 1 if walls else 0, 0], side, cells)
+    w.x = _assemble(parts)
+    w.f = _forces(rng, w.n)
+    return w
+
+
 def ensemble(seed: int = 0, count: int = 256):
     rng = np.random.default_rng(seed)
     return [ensemble_instance(rng, f"member{i}") for i in range(count)]

@@ -63,8 +63,10 @@ typedef enum {
 /* Arithmetic of the operators.  FP64: the reference's arithmetic (keys,
  * origins and weights bit-exact; interpolation sums in the reference's order;
  * spread differs from the reference only by summation order).  FP32C: the
- * same FP64 index step, FP32 weights and products, compensated (TwoSum)
- * accumulation; FP64 inputs and outputs. */
+ * same FP64 index step and FP32 weights; spread sums the FP32 products
+ * exactly in fixed point (order-independent, so results do not depend on
+ * scheduling), interpolation applies the FP32 weights to the FP64 values
+ * with FP64 accumulation; FP64 inputs and outputs. */
 typedef enum { IBK_PRECISION_FP64 = 0, IBK_PRECISION_FP32C = 1 } ibk_precision;
 
 /* fd::domain of fd::dimension{length, boundary} (include/fd/domain.h:15-33,
@@ -163,6 +165,163 @@ ibk_status ibk_plan_check(ibk_plan plan);
 ibk_status ibk_interpolate_noalloc(const ibk_domain* domain, int tag, int refinement,
                                    ibk_delta delta, int precision, int n, const double* x,
                                    const double* const* ue, double* ul, void* stream);
+
+/* ---- Batches: many independent grids per launch --------------------------
+ * No counterpart in the reference, which builds one operator object per grid
+ * and launches its kernels grid by grid.  A batch holds `count` instances
+ * (each its own domain, tag and refinement; one delta, precision and dims for
+ * all) and runs spread, interpolate, or the coupled step below over all of
+ * them with one persistent kernel per operator: CTAs take (instance, tile,
+ * component) work items from a device-side counter, so uneven instances
+ * balance across the SMs.  Instance i behaves exactly like a plan of its own
+ * (same arrays, layouts, overwrite semantics; FP32C spread results are
+ * bit-identical to a single plan's, FP64 ones equal up to summation order).
+ * An instance whose bound point count is 0 is left untouched, as n <= 0 is
+ * for a plan. */
+typedef struct ibk_batch_s* ibk_batch;
+
+typedef struct {
+	ibk_domain domain;
+	int tag;                /* ibk_tag */
+	int refinement;
+} ibk_instance_desc;
+
+/* Device arrays of one instance for the next runs (reference layouts, as
+ * ibk_spread / ibk_interpolate take them).  Pointers an operation does not
+ * use may be NULL. */
+typedef struct {
+	int n;                  /* points (0: instance idle) */
+	const double* x;        /* dims*n positions */
+	const double* fl;       /* dims*n forces: IBK_OP_SPREAD input */
+	double* fe[3];          /* force density per component: spread output */
+	const double* ue[3];    /* velocity per component: interpolate input */
+	double* ul;             /* dims*n velocities: interpolate output */
+	double* xn;             /* dims*n: IBK_OP_STEP advected positions */
+	const double* xref;     /* dims*n: IBK_OP_STEP spring rest positions */
+	double* fs;             /* dims*n: IBK_OP_STEP spring forces */
+} ibk_instance_io;
+
+typedef enum {
+	IBK_OP_SPREAD = 1,      /* fe <- spread(x, fl) */
+	IBK_OP_INTERPOLATE = 2, /* ul <- interpolate(x, ue) */
+	/* One coupled immersed-boundary step: U = interpolate(x, ue) (written to
+	 * ul when ul is not NULL); xn = x + dt*U (forward Euler); fs = -k*(xn -
+	 * xref) (linear spring to the rest shape); fe <- spread(xn, fs). */
+	IBK_OP_STEP = 3
+} ibk_batch_op;
+
+/* Launch shape of a batch: preferred tile extents in cells per axis (shrunk
+ * per instance so the last tile keeps at least M cells) and persistent CTAs
+ * per SM (0: as many as fit). */
+typedef struct {
+	int spread_tile[3];
+	int interp_tile[3];
+	int spread_ctas_per_sm;
+	int interp_ctas_per_sm;
+} ibk_batch_config;
+
+/* max_points bounds the sum of the bound point counts; all scratch is
+ * allocated here and by ibk_batch_configure, never by a run. */
+ibk_status ibk_batch_create(int count, const ibk_instance_desc* instances, ibk_delta delta,
+                            int precision, int max_points, ibk_batch* out);
+ibk_status ibk_batch_destroy(ibk_batch batch);
+ibk_status ibk_batch_info(ibk_batch batch, int instance, ibk_grid_info* info);
+
+/* Binds the arrays of every instance (io[count]).  Stream-ordered: the table
+ * is copied to the device on `stream` from a ring of pinned host buffers, so
+ * a run queued after it on the same stream sees it; the host blocks only
+ * when four binds are still in flight. */
+ibk_status ibk_batch_bind(ibk_batch batch, const ibk_instance_io* io, void* stream);
+
+/* dt and k of IBK_OP_STEP (internal units); drops a captured step graph. */
+ibk_status ibk_batch_set_step(ibk_batch batch, double dt, double k);
+
+/* Runs op over every instance with the bound arrays.  After
+ * ibk_batch_capture(op) it replays the captured CUDA graph instead. */
+ibk_status ibk_batch_run(ibk_batch batch, int op, void* stream);
+
+/* Records op as one CUDA graph (on an internal stream) for later runs.  The
+ * graph reads the arrays bound at run time, so binds stay outside it. */
+ibk_status ibk_batch_capture(ibk_batch batch, int op);
+
+ibk_status ibk_batch_configure(ibk_batch batch, const ibk_batch_config* config);
+ibk_status ibk_batch_get_config(ibk_batch batch, ibk_batch_config* config);
+
+/* Autotuner: times op (synchronising) over candidate tile shapes and CTAs per
+ * SM on the bound arrays, keeps the fastest configuration and returns it. */
+ibk_status ibk_batch_tune(ibk_batch batch, int op, void* stream, ibk_batch_config* best);
+
+ibk_status ibk_batch_launch_count(ibk_batch batch, long long* launches);
+/* As ibk_plan_check, for the batch's device status word. */
+ibk_status ibk_batch_check(ibk_batch batch);
+
+/* ---- Serving: continuous batching of coupled steps -------------------------
+ * No counterpart in the reference.  A server holds the device-resident state
+ * of many small simulations ("members": positions, spring rest shape, grid
+ * velocity and grid force density) and takes IBK_OP_STEP requests for them as
+ * they arrive.  Requests are packed into batched persistent launches on
+ * `slots` CUDA streams: while one batch is on the GPU, requests that arrive
+ * are launched on the next free slot, so their work overlaps on the device.
+ * A member is stepped by at most one launch at a time (its requests run in
+ * arrival order).  Admission allocates a member's state only while the total
+ * stays within hbm_budget bytes and the device has the memory free.  With
+ * FP32C a member's results do not depend on which other members share its
+ * launches. */
+typedef struct ibk_server_s* ibk_server;
+
+typedef struct {
+	ibk_delta delta;
+	int precision;              /* ibk_precision */
+	int slots;                  /* launches in flight at most (>= 1) */
+	double dt, k;               /* IBK_OP_STEP parameters, internal units */
+	long long hbm_budget;       /* bytes of member state admitted at most */
+	int max_points;             /* points of all members together, at most */
+} ibk_server_config;
+
+typedef struct {
+	long long requests;         /* completed requests */
+	long long launches;         /* batched launches (graph replays) */
+	long long points;           /* points stepped */
+	double p50_ms, p99_ms, mean_ms, max_ms;   /* arrival -> completion seen */
+	double wall_s;              /* first arrival -> last completion */
+	long long admitted_bytes;
+} ibk_server_stats;
+
+ibk_status ibk_server_create(int members, const ibk_instance_desc* desc, const ibk_server_config* config,
+                             ibk_server* out);
+ibk_status ibk_server_destroy(ibk_server server);
+
+/* Copies a member's initial positions (n points, host, x[d*n + p]; also its
+ * spring rest shape) and grid velocity (host, one array per component) to
+ * the device and zeroes its force grid.  IBK_ERR_CAPACITY when the member
+ * would exceed hbm_budget or the device's free memory. */
+ibk_status ibk_server_admit(ibk_server server, int member, int n, const double* x,
+                            const double* const* ue);
+/* Waits for the member's steps in flight, then releases its state. */
+ibk_status ibk_server_retire(ibk_server server, int member);
+
+/* Queues one step request; t_arrival in seconds on the server's clock
+ * (ibk_server_clock), or < 0 for now. */
+ibk_status ibk_server_submit(ibk_server server, int member, double t_arrival);
+/* Non-blocking: completes finished launches and launches queued requests on
+ * free slots.  *pending (optional) receives the requests not yet complete. */
+ibk_status ibk_server_progress(ibk_server server, int* pending);
+/* Progresses until every queued request is complete. */
+ibk_status ibk_server_drain(ibk_server server);
+double ibk_server_clock(ibk_server server);
+
+/* Synchronising copy of a member's state to the host: positions (dims*n) and
+ * force grid per component (either may be NULL). */
+ibk_status ibk_server_read(ibk_server server, int member, double* x, double* const* fe);
+
+ibk_status ibk_server_get_stats(ibk_server server, ibk_server_stats* stats);
+ibk_status ibk_server_reset_stats(ibk_server server);
+
+/* Open-loop load: `requests` step requests with Poisson arrivals at
+ * rate_per_s, each for a member drawn uniformly from the admitted ones
+ * (seeded); served as they arrive; returns the statistics of this run. */
+ibk_status ibk_server_run_poisson(ibk_server server, double rate_per_s, int requests,
+                                  unsigned long long seed, ibk_server_stats* stats);
 
 /* Human-readable text of the last error on the calling host thread. */
 const char* ibk_last_error(void);

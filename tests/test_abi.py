@@ -44,3 +44,9 @@ def test_host_only_calls(ibk):
     assert lib.ibk_plan_destroy(None) == 0
     # n <= 0 returns before touching the plan's device state
     assert lib.ibk_spread(None, 0, None, None, None, None) == 1  # null plan is rejected first
+    # batches: argument checks happen before any device work
+    h = ctypes.c_void_p()
+    assert lib.ibk_batch_create(0, None, ibk._Delta(), 0, 0, ctypes.byref(h)) == 1
+    assert lib.ibk_batch_destroy(None) == 0
+    assert lib.ibk_batch_run(None, ibk.OP_SPREAD, None) == 1
+    assert lib.ibk_batch_bind(None, None, None) == 1
