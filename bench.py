@@ -2,11 +2,23 @@
 """Benchmark of the IB coupling operators (spread + interpolate) on B200.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
-                    [--workload large-channel|channel|single-rbc] [--precision fp32c|fp64]
+                    [--workload large-channel|medium-channel|channel|single-rbc]
+                    [--precision fp32c|fp64] [--no-cpu] [--no-extras]
+                    [--leg all|batched|serving]
 
 One step = ibk_spread + ibk_interpolate over every Lagrangian point of the
 workload (spread overwrites all grid faces, interpolate writes every point
-velocity).  Metric: points per second through spread+interp.
+velocity).  Metric: points per second through spread+interp, in the chosen
+FP32C form, with the plain FP64 path, its accuracy, p50/p99 step times, the
+end-to-end rate through host buffers and the CPU baseline in the same line.
+
+The same line also carries two legs (skipped with --no-extras, or run alone
+with --leg): "batched" -- 256 independent instances (cube grids 32^3..128^3,
+1-50 cells each) in one persistent graph-captured launch per operator, FP32C
+against the FP64 batch and against a loop of single plans; "serving" -- the
+256 instances as device-resident members stepped (interpolate, advect, spring
+force, spread) under Poisson request arrivals from 1k to 50k steps/s, with
+p50/p99 latency per offered rate.
 
 Default workload: the large channel, 128 x 64 x 128 um, MAC grid 512 x 256 x
 512 (h = 0.25 um), 3300 RBCs x 2210 points + 6000 platelets x 605 points =
@@ -116,6 +128,16 @@ class ClockSampler:
 
 
 # ------------------------------------------------------------ workloads
+def max_over_ranks(ms, world, device):
+    """The job's time: the largest per-rank device time (all_reduce MAX)."""
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([float(ms)], dtype=torch.float64, device=device)
+    if world > 1:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
 def make_workload(name, seed=0):
     load_package()
     from ib_cu_b200 import workloads as W
@@ -234,6 +256,16 @@ def run_ours(args):
     ibk.lib()
     from ib_cu_b200 import workloads as W
 
+    if args.leg in ("batched", "serving"):
+        # one leg alone (profiling runs): its own JSON object
+        if args.leg == "batched":
+            res = run_batched(ibk, W, dev, seed=0, steps=max(5, args.steps), rank=rank, world=world)
+        else:
+            res = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
+        if rank == 0:
+            print(json.dumps({"leg": args.leg, args.leg: res}), flush=True)
+        return
+
     w = make_workload(args.workload, seed=rank)
     precision = {"fp64": ibk.FP64, "fp32c": ibk.FP32C}[args.precision]
     dom = ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)])
@@ -293,10 +325,7 @@ def run_ours(args):
                 elapsed += e0.elapsed_time(e1)
         barrier()
     launches = plan.launch_count() - launches0
-    t = torch.tensor([elapsed], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    ms_total = float(t.item())
+    ms_total = max_over_ranks(elapsed, world, dev)
     ms_step = ms_total / args.steps
     value = world * n / (ms_step / 1000.0)
     clocks = clk.summary()
@@ -345,10 +374,7 @@ def run_ours(args):
         a1.record(stream)
         torch.cuda.synchronize()
         e2e_ms += a0.elapsed_time(a1)
-    te = torch.tensor([e2e_ms], dtype=torch.float64, device=dev)
-    if world > 1:
-        dist.all_reduce(te, op=dist.ReduceOp.MAX)
-    e2e_value = world * n / (float(te.item()) / args.steps / 1000.0)
+    e2e_value = world * n / (max_over_ranks(e2e_ms, world, dev) / args.steps / 1000.0)
 
     # ---- step-time distribution (each step bracketed by its own events)
     per_step = []
@@ -411,10 +437,10 @@ def run_ours(args):
         del fe64, ul64, plan64
 
     extras = {}
-    if not args.no_extras:
+    if not args.no_extras and args.leg == "all":
         del fe, ul
         torch.cuda.empty_cache()
-        extras["batched"] = run_batched(ibk, W, dev, seed=rank, steps=max(5, args.steps // 2))
+        extras["batched"] = run_batched(ibk, W, dev, seed=0, steps=max(5, args.steps // 2), rank=rank, world=world)
         extras["serving"] = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
 
     cpu = None
@@ -493,26 +519,36 @@ def time_batch(batch, ops, steps, stream):
     return e0.elapsed_time(e1) / steps
 
 
-def run_batched(ibk, W, dev, seed, steps):
+def run_batched(ibk, W, dev, seed, steps, rank=0, world=1):
     """256 independent instances (cube grids of 32^3..128^3, 1-50 cells), one
     persistent graph-captured launch per operator; FP32C vs FP64 batches and
-    a loop of single plans for comparison."""
+    a loop of single plans for comparison.  With several ranks the 256
+    instances are partitioned over them (longest first; no exchange), each
+    rank runs its share, and the times are the slowest rank's."""
     import torch
+    from ib_cu_b200 import sharding
     stream = torch.cuda.current_stream()
-    insts_w = W.ensemble(seed=seed, count=256)
+    everything = W.ensemble(seed=seed, count=256)
+    # periodic cubes of side s cells: 3 s^3 faces (h = 0.25 um = 0.025 units)
+    cube_faces = [3 * int(round(w.lengths[0] / 0.025)) ** 3 for w in everything]
+    shards = sharding.partition([sharding.instance_cost(w.n, f) for w, f in zip(everything, cube_faces)], world)
+    insts_w = [everything[i] for i in shards[rank]]
     ops = (ibk.OP_SPREAD, ibk.OP_INTERPOLATE)
-    out = {"instances": len(insts_w)}
+    out = {"instances": len(everything), "instances_this_rank": len(insts_w),
+           "scaling": "strong", "parallelism": f"instances partitioned over {world} rank(s)"}
     batch, io, total = ensemble_arrays(ibk, W, insts_w, ibk.FP32C, dev, 2000 + seed)
-    faces = sum(sum(batch.sizes(i)) for i in range(len(insts_w)))
-    t_default = time_batch(batch, ops, steps, stream)
+    faces = sum(cube_faces)
+    assert world > 1 or faces == sum(sum(batch.sizes(i)) for i in range(len(insts_w)))
+    t_default = max_over_ranks(time_batch(batch, ops, steps, stream), world, dev)
     cfg_s = batch.tune(ibk.OP_SPREAD, stream)
     cfg = batch.tune(ibk.OP_INTERPOLATE, stream)
     for op in ops:
         batch.capture(op)
     l0 = batch.launch_count()
-    ms = time_batch(batch, ops, steps, stream)
+    ms = max_over_ranks(time_batch(batch, ops, steps, stream), world, dev)
     launches = (batch.launch_count() - l0) // (steps + 3)
-    out.update({"points": total, "faces": faces, "value": total / (ms / 1000.0), "unit": "points/s",
+    all_points = sum(w.n for w in everything)
+    out.update({"points": all_points, "faces": faces, "value": all_points / (ms / 1000.0), "unit": "points/s",
                 "ms_per_step": ms, "faces_per_s": faces / (ms / 1000.0), "ms_default_config": t_default,
                 "tuned_config": cfg, "launches_per_step": launches,
                 "roofline_bytes_per_step": 2 * algorithmic_bytes(total, faces)})
@@ -525,7 +561,7 @@ def run_batched(ibk, W, dev, seed, steps):
     b64.bind([dict(e, fe=fe64[i], ul=ul64[i]) for i, e in enumerate(io)])
     for op in ops:
         b64.capture(op)
-    ms64 = time_batch(b64, ops, max(3, steps // 2), stream)
+    ms64 = max_over_ranks(time_batch(b64, ops, max(3, steps // 2), stream), world, dev)
     err_s = err_u = 0.0
     for i, e in enumerate(io):
         for c in range(3):
@@ -536,7 +572,7 @@ def run_batched(ibk, W, dev, seed, steps):
             ref = ul64[i][c * n_i:(c + 1) * n_i]
             err_u = max(err_u, float((e["ul"][c * n_i:(c + 1) * n_i] - ref).abs().max())
                         / max(float(ref.abs().max()), 1e-300))
-    out["plain_fp64"] = {"value": total / (ms64 / 1000.0), "ms_per_step": ms64, "speedup": ms64 / ms,
+    out["plain_fp64"] = {"value": all_points / (ms64 / 1000.0), "ms_per_step": ms64, "speedup": ms64 / ms,
                          "accuracy_vs_fp64": {"spread_max": err_s, "interp_max": err_u}}
     del b64, fe64, ul64
     # a loop of single FP32C plans (one per instance), for the batching gain
@@ -559,7 +595,7 @@ def run_batched(ibk, W, dev, seed, steps):
         loop()
     e1.record(stream)
     torch.cuda.synchronize()
-    ms_loop = e0.elapsed_time(e1) / max(2, steps // 4)
+    ms_loop = max_over_ranks(e0.elapsed_time(e1) / max(2, steps // 4), world, dev)
     out["plan_loop"] = {"ms_per_step": ms_loop, "batch_speedup": ms_loop / ms}
     del plans, batch, io
     torch.cuda.empty_cache()
@@ -611,6 +647,8 @@ def main():
     ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
     ap.add_argument("--cpu-seconds", type=float, default=20.0)
+    ap.add_argument("--leg", choices=["all", "batched", "serving"], default="all",
+                    help="batched / serving: run that leg alone (its own JSON line)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched (256 instances) and serving legs")
     args = ap.parse_args()

@@ -50,3 +50,37 @@ def test_host_only_calls(ibk):
     assert lib.ibk_batch_destroy(None) == 0
     assert lib.ibk_batch_run(None, ibk.OP_SPREAD, None) == 1
     assert lib.ibk_batch_bind(None, None, None) == 1
+
+
+def test_cpp_adapter_compiles(tmp_path):
+    """include/ibk.hpp (the reference-shaped C++ surface) compiles against
+    the C ABI: operator objects, the allocating overloads and batches."""
+    import shutil
+    import subprocess
+    cxx = shutil.which("g++")
+    if cxx is None:
+        import pytest
+        pytest.skip("no host C++ compiler")
+    src = tmp_path / "use_adapter.cc"
+    src.write_text(r'''
+#include "ibk.hpp"
+int use(const double* x, const double* fl, const double* u0, const double* u1, const double* u2, int n)
+{
+    ibk::domain dom{ibk::dimension{3.2, ibk::periodic}, ibk::dimension{1.6, ibk::dirichlet},
+                    ibk::dimension{3.2, ibk::periodic}};
+    ibk::spread spread{ibk::mac{64}, dom, ibk::bspline<3>{}, IBK_PRECISION_FP32C};
+    ibk::interpolate interp{ibk::mac{64}, dom, ibk::bspline<3>{}};
+    auto fe = spread(n, x, fl);
+    auto ul = interp(n, x, {u0, u1, u2});
+    spread(n, x, fl, {fe[0].values(), fe[1].values(), fe[2].values()});
+    std::vector<std::pair<ibk::mac, ibk::domain>> insts{{ibk::mac{32}, dom}, {ibk::mac{64}, dom}};
+    ibk::batch b{insts, ibk_delta{IBK_DELTA_BSPLINE, 3}, IBK_PRECISION_FP32C, 2 * n};
+    b.set_step(1e-3, 1e-3);
+    return (int) ul.size();
+}
+''')
+    inc = os.path.join(ROOT, "include")
+    cuda_inc = "/usr/local/cuda/include"
+    r = subprocess.run([cxx, "-std=c++17", "-c", str(src), "-I" + inc, "-I" + cuda_inc,
+                        "-o", str(tmp_path / "use_adapter.o")], capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
