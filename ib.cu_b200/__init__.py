@@ -40,7 +40,7 @@ FP64, FP32C = 0, 1
 
 # Every symbol include/ibk.h declares (checked by the CPU test suite).
 ABI_SYMBOLS = (
-    "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
+    "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve", "ibk_plan_set_tiles",
     "ibk_spread", "ibk_interpolate", "ibk_sort_keys",
     "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
     "ibk_plan_launch_count", "ibk_plan_check", "ibk_interpolate_noalloc",
@@ -144,6 +144,8 @@ def lib() -> ctypes.CDLL:
         L.ibk_plan_destroy.argtypes = [_vp]
         L.ibk_plan_info.argtypes = [_vp, ctypes.POINTER(GridInfo)]
         L.ibk_plan_reserve.argtypes = [_vp, ctypes.c_int]
+        L.ibk_plan_set_tiles.argtypes = [_vp, ctypes.POINTER(ctypes.c_int * 3), ctypes.POINTER(ctypes.c_int * 3)]
+        L.ibk_plan_set_tiles.restype = ctypes.c_int
         L.ibk_spread.argtypes = [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp), _vp]
         L.ibk_interpolate.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_vp), _vp, _vp]
         L.ibk_sort_keys.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
@@ -331,6 +333,12 @@ class Plan:
 
     def reserve(self, max_points: int):
         check(lib().ibk_plan_reserve(self._h, int(max_points)))
+
+    def set_tiles(self, spread_tile=None, interp_tile=None):
+        """Preferred tile extents (cells per axis) of the spread / interpolation kernels."""
+        def arr(t):
+            return None if t is None else ctypes.byref((ctypes.c_int * 3)(*[int(v) for v in t]))
+        check(lib().ibk_plan_set_tiles(self._h, arr(spread_tile), arr(interp_tile)))
 
     def _comp_ptrs(self, arrs):
         P = (_vp * 3)()

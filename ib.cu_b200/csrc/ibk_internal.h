@@ -47,7 +47,7 @@ struct Plan {
 	TileGeom spread_tiles{};   // spread tiles (owner-computes accumulators)
 	bool tiled = true;         // false: an axis has fewer cells than the stencil width
 	ibk_grid_info info{};
-	int delta_kind = 0, delta_order = 0, precision = 0;
+	int delta_kind = 0, delta_order = 0, precision = 0, tag = 0;
 	int device = 0;
 	int reserved_points = 0;
 	OpTable ops{};

@@ -110,10 +110,17 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	// FP64: one double per face; FP32C: an FP64 total and a 32-bit working word
 	const size_t per_face = PREC == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
 	const size_t smem = per_face * (size_t) tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
-	auto kern = spread_tile_kernel<D, DIMS, PREC>;
+	// threads per CTA: 256 per 4096 faces of the tile (FP32C), 256 (FP64)
+	const int tv = tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
+	int nt = 256;
+	auto kern = spread_tile_kernel<D, DIMS, PREC, 256>;
+	if constexpr (PREC == IBK_PRECISION_FP32C) {
+		if (tv > 8192) { nt = 1024; kern = spread_tile_kernel<D, DIMS, PREC, 1024>; }
+		else if (tv > 4096) { nt = 512; kern = spread_tile_kernel<D, DIMS, PREC, 512>; }
+	}
 	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
 	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, binmax, fe);
+		kern<<<dim3(tg.num_tiles, DIMS), nt, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, binmax, fe);
 	});
 }
 

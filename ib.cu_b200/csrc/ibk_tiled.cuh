@@ -211,15 +211,39 @@ __device__ __forceinline__ void fix_add(int* word, float s)
 	atomicAdd(word, __float_as_int(s + kMagic) - kMagicBits);   // rint(s)
 }
 
+// fix_add of the product a * b, rounded once (rint of the exact product).
+__device__ __forceinline__ void fix_add_product(int* word, float a, float b)
+{
+	atomicAdd(word, __float_as_int(__fmaf_rn(a, b, kMagic)) - kMagicBits);
+}
+
+// The fixed-point increments of a0 * b and a1 * b (each rounded once, as in
+// fix_add_product), from one packed two-lane FP32 FMA.
+__device__ __forceinline__ int2 fix_terms2(float a0, float a1, float b)
+{
+	float r0, r1;
+	asm("{\n\t.reg .b64 pa, pb, pc, pd;\n\t"
+	    "mov.b64 pa, {%2, %3};\n\t"
+	    "mov.b64 pb, {%4, %4};\n\t"
+	    "mov.b64 pc, {%5, %5};\n\t"
+	    "fma.rn.f32x2 pd, pa, pb, pc;\n\t"
+	    "mov.b64 {%0, %1}, pd;\n\t}"
+	    : "=f"(r0), "=f"(r1) : "f"(a0), "f"(a1), "f"(b), "f"(kMagic));
+	return make_int2(__float_as_int(r0) - kMagicBits, __float_as_int(r1) - kMagicBits);
+}
+
 // One candidate point p of a spread tile [lo, hi): its in-tile stencil
 // contributions added to the tile's accumulators (F is read only when the
 // stencil touches the tile).  FP32C: the FP32 product res * F is scaled by
 // the tile's fixed-point scale.
+// contig: the tile spans no periodic axis whole, so the in-tile nodes of a
+// stencil are consecutive along every axis and their accumulators sit at
+// fixed offsets from the first one.
 template <typename D, int DIMS, int PREC>
 __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGeom& cg, int n,
                                                  const double* __restrict__ x, const double* __restrict__ fc,
                                                  int p, float scale, const int* lo, const int* hi, int T0, int T1,
-                                                 typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
+                                                 bool contig, typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
 {
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	int loc[DIMS][M];
@@ -272,17 +296,67 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 		for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
 #pragma unroll
 		for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
+		if (contig) {
+			// node (m0, m1, m2) at first + (m2 * T1 + m1) * T0 + m0, where
+			// first is the (possibly outside) position of node (0, 0, 0)
+			int lb[DIMS];
 #pragma unroll
-		for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-			const int m1 = r % M, m2 = r / M;
-			const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
-			if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
-			const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-			const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
+			for (int d = 0; d < DIMS; ++d) {
+				int v = 0;
+				bool found = false;
 #pragma unroll
-			for (int m0 = 0; m0 < M; ++m0)
-				if ((mask[0] >> m0) & rm)
-					fix_add(acc + row + loc[0][m0], w[0][m0] * w12);
+				for (int m = 0; m < M; ++m)
+					if (!found && ((mask[d] >> m) & 1u)) { v = loc[d][m] - m; found = true; }
+				lb[d] = v;
+			}
+			const int first = DIMS == 3 ? (lb[2] * T1 + lb[1]) * T0 + lb[0] : lb[1] * T0 + lb[0];
+			int* base = acc + first;
+			constexpr unsigned kFull = (1u << M) - 1u;
+			const bool full = mask[0] == kFull && mask[1] == kFull && (DIMS < 3 || mask[2] == kFull);
+			if (full) {
+				// the whole stencil inside the tile: no per-node tests
+#pragma unroll
+				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+					const int m1 = r % M, m2 = r / M;
+					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+					int* rowp = base + ((DIMS == 3 ? m2 * T1 : 0) + m1) * T0;
+#pragma unroll
+					for (int m0 = 0; m0 + 1 < M; m0 += 2) {
+						const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
+						atomicAdd(rowp + m0, t.x);
+						atomicAdd(rowp + m0 + 1, t.y);
+					}
+					if (M & 1) fix_add_product(rowp + (M - 1), w[0][M - 1], w12);
+				}
+			} else {
+#pragma unroll
+				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+					const int m1 = r % M, m2 = r / M;
+					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
+					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+					int* rowp = base + ((DIMS == 3 ? m2 * T1 : 0) + m1) * T0;
+#pragma unroll
+					for (int m0 = 0; m0 + 1 < M; m0 += 2) {
+						const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
+						if ((mask[0] >> m0) & 1u) atomicAdd(rowp + m0, t.x);
+						if ((mask[0] >> (m0 + 1)) & 1u) atomicAdd(rowp + m0 + 1, t.y);
+					}
+					if ((M & 1) && ((mask[0] >> (M - 1)) & 1u)) fix_add_product(rowp + (M - 1), w[0][M - 1], w12);
+				}
+			}
+		} else {
+#pragma unroll
+			for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
+				const int m1 = r % M, m2 = r / M;
+				const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
+				if (!rm) continue;
+				const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+				const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
+#pragma unroll
+				for (int m0 = 0; m0 < M; ++m0)
+					if ((mask[0] >> m0) & rm) fix_add_product(acc + row + loc[0][m0], w[0][m0], w12);
+			}
 		}
 	}
 }
@@ -290,7 +364,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 // One (tile, component) of the spread; every thread of the CTA calls it.
 // perm holds point indices offset by pbase (a batch numbers the points of
 // all its instances consecutively); off and binmax are this grid's bins.
-template <typename D, int DIMS, int PREC>
+template <typename D, int DIMS, int PREC, int NT = kTileThreads>
 __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
                                             const double* __restrict__ fl, const int* __restrict__ perm, int pbase,
                                             const int* __restrict__ off, const unsigned* __restrict__ binmax,
@@ -311,10 +385,12 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, tile, tc);
 	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
+	bool contig = true;
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
 		lo[d] = tc[d] * tg.T[d];
 		hi[d] = min(lo[d] + tg.T[d], cg.points[d]);
+		contig = contig && (g.solid[d] || tg.ntiles[d] > 1);
 	}
 	build_ranges<DIMS>(g, tg, tc, off, rt, true, binmax, c);
 	const double* __restrict__ fc = fl + (size_t) c * n;
@@ -323,7 +399,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	const int ncand = rt.pref[rt.count];
 	if (ncand == 0) {
 		// no point reaches the tile: its faces are zero
-		for (int i = threadIdx.x; i < e1 * e2 * T0; i += kTileThreads) {
+		for (int i = threadIdx.x; i < e1 * e2 * T0; i += NT) {
 			const int l0 = i % T0;
 			const int r = i / T0;
 			if (l0 >= e0) continue;
@@ -333,16 +409,16 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		}
 		return;
 	}
-	for (int i = threadIdx.x; i < TV; i += kTileThreads) acc[i] = (acc_t) 0;
+	for (int i = threadIdx.x; i < TV; i += NT) acc[i] = (acc_t) 0;
 	if constexpr (PREC == IBK_PRECISION_FP32C)
-		for (int i = threadIdx.x; i < TV; i += kTileThreads) total[i] = 0.0;
+		for (int i = threadIdx.x; i < TV; i += NT) total[i] = 0.0;
 	__syncthreads();
 
 	double inv_scale = 1.0;     // FP32C: back to force density (exact power of two)
 	if constexpr (PREC == IBK_PRECISION_FP64) {
-		for (int it = threadIdx.x; it < ncand; it += kTileThreads)
+		for (int it = threadIdx.x; it < ncand; it += NT)
 			spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, 0.0f,
-			                                lo, hi, T0, T1, acc);
+			                                lo, hi, T0, T1, contig, acc);
 	} else {
 		// the tile's largest possible term, max|F| * max|w| * res (max|F| over
 		// its candidate bins, rounded to FP32, hence the 1.001), is scaled to
@@ -353,12 +429,12 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		const float scale = ldexpf(1.0f, min(kFixTermLog2 - e, 126));
 		for (int base = 0; base < ncand; base += kFixChunk) {
 			const int stop = min(ncand, base + kFixChunk);
-			for (int it = base + threadIdx.x; it < stop; it += kTileThreads)
+			for (int it = base + threadIdx.x; it < stop; it += NT)
 				spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, scale,
-				                                lo, hi, T0, T1, acc);
+				                                lo, hi, T0, T1, contig, acc);
 			// fold the working words into the exact FP64 totals
 			__syncthreads();
-			for (int i = threadIdx.x; i < TV; i += kTileThreads) {
+			for (int i = threadIdx.x; i < TV; i += NT) {
 				total[i] += (double) acc[i];
 				acc[i] = 0;
 			}
@@ -369,7 +445,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	__syncthreads();
 
 	// every face of the tile, written once
-	for (int i = threadIdx.x; i < e1 * e2 * T0; i += kTileThreads) {
+	for (int i = threadIdx.x; i < e1 * e2 * T0; i += NT) {
 		const int l0 = i % T0;
 		const int r = i / T0;
 		if (l0 >= e0) continue;
@@ -382,14 +458,17 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	}
 }
 
-template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads)
+// NT threads per CTA; FP32C CTAs are capped at 64 registers per thread so
+// that 1024 threads of them fit on an SM, FP64 ones (256 threads) at 85 so
+// that three fit.
+template <typename D, int DIMS, int PREC, int NT>
+__global__ void __launch_bounds__(NT, PREC == IBK_PRECISION_FP32C ? 1024 / NT : 3)
 spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const double* __restrict__ fl, const int* __restrict__ perm,
                    const int* __restrict__ off, const unsigned* __restrict__ binmax, CompPtrs fe)
 {
 	// grid: (tile, component)
-	spread_tile<D, DIMS, PREC>(g, tg, n, x, fl, perm, 0, off, binmax, fe, blockIdx.x, blockIdx.y);
+	spread_tile<D, DIMS, PREC, NT>(g, tg, n, x, fl, perm, 0, off, binmax, fe, blockIdx.x, blockIdx.y);
 }
 
 // ------------------------------------------------------------ interp ---

@@ -106,6 +106,13 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement,
 ibk_status ibk_plan_destroy(ibk_plan plan);
 ibk_status ibk_plan_info(ibk_plan plan, ibk_grid_info* info);
 
+/* Preferred tile extents in cells per axis for the spread (owner-computes
+ * accumulator tiles) and interpolation (staged halo regions) kernels; either
+ * may be NULL to keep the current shape.  Each axis is shrunk so its last
+ * tile keeps at least M cells.  Defaults: 16^3 for both.  Results do not depend on the shape
+ * except through the FP32C fixed-point scale, which is per tile. */
+ibk_status ibk_plan_set_tiles(ibk_plan plan, const int* spread_tile, const int* interp_tile);
+
 /* Pre-size the plan's device scratch for up to max_points points, so that
  * later calls allocate nothing (required before CUDA-graph capture). */
 ibk_status ibk_plan_reserve(ibk_plan plan, int max_points);
