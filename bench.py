@@ -48,6 +48,13 @@ sys.path.insert(0, ROOT)
 METRIC = "spread+interp points/s"
 L2_BYTES = 126 * 1024 * 1024
 
+# DRAM bytes moved by one launch of the dominant kernel per algorithmic byte,
+# from one ncu capture (dram__bytes_read.sum + dram__bytes_write.sum) of the
+# FP32C spread on the 256 x 128 x 256 channel (1,364,270 points): 311.98 MB
+# against 266.29 MB.  Points and faces both scale by 8.01 to the 512 x 256 x
+# 512 channel, so a launch's traffic is this ratio times its algorithmic bytes.
+TRAFFIC_PER_ALGORITHMIC_BYTE = {("spread_tile_kernel", "fp32c"): 311.98e6 / 266.29e6}
+
 
 def load_package():
     import importlib.util
@@ -345,6 +352,10 @@ def run_ours(args):
     avg_ms = tot / max(nl, 1)
     op_bytes = algorithmic_bytes(n, G)
     achieved = op_bytes / (avg_ms / 1000.0) / 1e9 if avg_ms > 0 else 0.0
+    ratio = TRAFFIC_PER_ALGORITHMIC_BYTE.get((name, args.precision))
+    traffic = ratio * op_bytes if ratio is not None else None
+    traffic_source = ("ncu dram bytes of the FP32C spread on the 256x128x256 channel, scaled by units "
+                      "processed (x8.01)" if ratio is not None else None)
     kernels = {k: {"launches": v[0], "avg_ms": v[1] / max(v[0], 1),
                    "share": v[1] / max(sum(s[1] for s in stats.values()), 1e-12)}
                for k, v in stats.items()}
@@ -462,7 +473,8 @@ def run_ours(args):
         "config": dict(workload_config(w, args.precision), parallelism=f"replicas{world}"),
         "faces_per_s": world * G / (ms_step / 1000.0),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                     "frac": achieved / peak, "traffic": None, "kernel": name,
+                     "frac": achieved / peak, "traffic": traffic, "traffic_source": traffic_source,
+                     "kernel": name,
                      "algorithmic_bytes_per_launch": op_bytes, "avg_launch_ms": avg_ms,
                      "peak_source": peak_kind},
         "kernels": kernels,
