@@ -614,7 +614,7 @@ def run_batched(ibk, W, dev, seed, steps, rank=0, world=1):
     return out
 
 
-def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=2):
+def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=4):
     """Serving sweep: 256 ensemble members resident on the device, Poisson
     step requests (interpolate, advect dt = 1 us, spring k = 1 pN/um,
     spread) at each offered rate, continuous batching on `slots` streams."""

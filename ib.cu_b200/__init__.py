@@ -50,6 +50,8 @@ ABI_SYMBOLS = (
     "ibk_server_create", "ibk_server_destroy", "ibk_server_admit", "ibk_server_retire",
     "ibk_server_submit", "ibk_server_progress", "ibk_server_drain", "ibk_server_clock",
     "ibk_server_read", "ibk_server_get_stats", "ibk_server_reset_stats", "ibk_server_run_poisson",
+    "ibk_server_save", "ibk_server_admit_from",
+    "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
 OP_SPREAD, OP_INTERPOLATE, OP_STEP = 1, 2, 3
@@ -103,6 +105,11 @@ class BatchConfig(ctypes.Structure):
         return {"spread_tile": list(self.spread_tile), "interp_tile": list(self.interp_tile),
                 "spread_ctas_per_sm": self.spread_ctas_per_sm,
                 "interp_ctas_per_sm": self.interp_ctas_per_sm}
+
+
+class IoHeader(ctypes.Structure):
+    _fields_ = [("magic", ctypes.c_int), ("matrix", ctypes.c_int), ("rows", ctypes.c_int),
+                ("cols", ctypes.c_int), ("count", ctypes.c_int)]
 
 
 class ServerConfig(ctypes.Structure):
@@ -187,8 +194,17 @@ def lib() -> ctypes.CDLL:
         L.ibk_server_reset_stats.argtypes = [_vp]
         L.ibk_server_run_poisson.argtypes = [_vp, ctypes.c_double, ctypes.c_int, ctypes.c_ulonglong,
                                              ctypes.POINTER(ServerStats)]
+        L.ibk_server_save.argtypes = [_vp, ctypes.c_int, ctypes.c_char_p]
+        L.ibk_server_admit_from.argtypes = [_vp, ctypes.c_int, ctypes.c_char_p]
+        L.ibk_io_write_dense.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                         ctypes.c_int, _vp]
+        L.ibk_io_write_scalar.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_double]
+        L.ibk_io_read_dense.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(IoHeader), _vp,
+                                        ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
+        L.ibk_io_read_scalar.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
+                                         ctypes.POINTER(ctypes.c_longlong)]
         for name in ABI_SYMBOLS:
-            if name.startswith(("ibk_batch_", "ibk_server_")) and name != "ibk_server_clock":
+            if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_")) and name != "ibk_server_clock":
                 getattr(L, name).restype = ctypes.c_int
         L.ibk_last_error.restype = ctypes.c_char_p
         L.ibk_status_string.restype = ctypes.c_char_p
@@ -626,7 +642,56 @@ class Server:
     def reset_stats(self):
         check(lib().ibk_server_reset_stats(self._h))
 
+    def save(self, member: int, path: str):
+        """Checkpoint of one member in the linalg::io binary format."""
+        check(lib().ibk_server_save(self._h, int(member), os.fsencode(path)))
+
+    def admit_from(self, member: int, path: str):
+        check(lib().ibk_server_admit_from(self._h, int(member), os.fsencode(path)))
+
     def run_poisson(self, rate: float, requests: int, seed: int = 0) -> dict:
         st = ServerStats()
         check(lib().ibk_server_run_poisson(self._h, float(rate), int(requests), int(seed), ctypes.byref(st)))
         return st.as_dict()
+
+
+# ------------------------------------------------------- linalg::io files
+def io_write(path, objects):
+    """Write numpy arrays / floats to one file in the reference's binary
+    format: 1-D arrays as vectors, 2-D arrays (n x m) as column-major
+    matrices, Python floats as raw FP64 scalars."""
+    import numpy as np
+    for k, obj in enumerate(objects):
+        append = 1 if k else 0
+        if isinstance(obj, float):
+            check(lib().ibk_io_write_scalar(os.fsencode(path), append, obj))
+            continue
+        a = np.asarray(obj, dtype=np.float64)
+        if a.ndim == 1:
+            v = np.ascontiguousarray(a)
+            check(lib().ibk_io_write_dense(os.fsencode(path), append, 0, a.shape[0], 1, v.ctypes.data))
+        elif a.ndim == 2:
+            v = np.ascontiguousarray(a.T)          # column-major values
+            check(lib().ibk_io_write_dense(os.fsencode(path), append, 1, a.shape[0], a.shape[1],
+                                           v.ctypes.data))
+        else:
+            raise ValueError("only vectors and matrices")
+
+
+def io_read(path, count=None):
+    """Read consecutive dense containers: vectors as 1-D arrays, matrices as
+    (rows, cols) arrays (values column-major in the file)."""
+    import numpy as np
+    out, off = [], 0
+    size = os.path.getsize(path)
+    while off < size and (count is None or len(out) < count):
+        h = IoHeader()
+        check(lib().ibk_io_read_dense(os.fsencode(path), off, ctypes.byref(h), None, 0, None))
+        buf = np.empty(max(h.count, 1), dtype=np.float64)
+        nxt = ctypes.c_longlong()
+        check(lib().ibk_io_read_dense(os.fsencode(path), off, ctypes.byref(h), buf.ctypes.data, buf.size,
+                                      ctypes.byref(nxt)))
+        buf = buf[:h.count]
+        out.append(buf.reshape(h.cols, h.rows).T.copy() if h.matrix else buf)
+        off = nxt.value
+    return out

@@ -402,6 +402,70 @@ ibk_status ibk_server_read(ibk_server handle, int member, double* x, double* con
 	return st;
 }
 
+ibk_status ibk_server_save(ibk_server handle, int member, const char* path)
+{
+	Server* s = reinterpret_cast<Server*>(handle);
+	if (!s || !path || member < 0 || member >= (int) s->members.size() || !s->members[member].admitted)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null server or path, or member not admitted");
+	ibk_status st = wait_member(*s, member);
+	if (st != IBK_OK) return st;
+	Member& m = s->members[member];
+	if ((st = cuda_ok(cudaDeviceSynchronize(), "cudaDeviceSynchronize")) != IBK_OK) return st;
+	const size_t pn = (size_t) s->dims * (size_t) m.n;
+	std::vector<double> buf(pn);
+	const double* pts[2] = {m.x[m.cur], m.xref};
+	for (int k = 0; k < 2 && st == IBK_OK; ++k) {
+		if (pn) st = cuda_ok(cudaMemcpy(buf.data(), pts[k], sizeof(double) * pn, cudaMemcpyDeviceToHost), "cudaMemcpy");
+		if (st == IBK_OK) st = ibk_io_write_dense(path, k, 1, m.n, s->dims, buf.data());
+	}
+	for (int pass = 0; pass < 2 && st == IBK_OK; ++pass)
+		for (int c = 0; c < s->dims && st == IBK_OK; ++c) {
+			std::vector<double> g((size_t) m.sizes[c]);
+			st = cuda_ok(cudaMemcpy(g.data(), pass == 0 ? m.ue[c] : m.fe[c], sizeof(double) * g.size(),
+			                        cudaMemcpyDeviceToHost), "cudaMemcpy");
+			if (st == IBK_OK) st = ibk_io_write_dense(path, 1, 0, (int) g.size(), 1, g.data());
+		}
+	return st;
+}
+
+ibk_status ibk_server_admit_from(ibk_server handle, int member, const char* path)
+{
+	Server* s = reinterpret_cast<Server*>(handle);
+	if (!s || !path || member < 0 || member >= (int) s->members.size())
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null server or path, or bad member");
+	long long off = 0;
+	ibk_io_header h{};
+	std::vector<double> x, xref;
+	std::vector<std::vector<double>> grids(2 * s->dims);
+	ibk_status st = IBK_OK;
+	for (int k = 0; k < 2 && st == IBK_OK; ++k) {
+		std::vector<double>& dst = k == 0 ? x : xref;
+		if ((st = ibk_io_read_dense(path, off, &h, nullptr, 0, nullptr)) != IBK_OK) break;
+		if (!h.matrix || h.cols != s->dims) { st = set_error(IBK_ERR_INVALID_ARGUMENT, "checkpoint positions are not n x dims"); break; }
+		dst.resize((size_t) h.count);
+		st = ibk_io_read_dense(path, off, &h, dst.data(), h.count, &off);
+	}
+	if (st == IBK_OK && xref.size() != x.size()) st = set_error(IBK_ERR_INVALID_ARGUMENT, "checkpoint shapes differ");
+	for (int j = 0; j < 2 * s->dims && st == IBK_OK; ++j) {
+		const int c = j % s->dims;
+		if ((st = ibk_io_read_dense(path, off, &h, nullptr, 0, nullptr)) != IBK_OK) break;
+		if (h.count != s->info[member].size[c]) { st = set_error(IBK_ERR_INVALID_ARGUMENT, "checkpoint grid size differs from the member's grid"); break; }
+		grids[j].resize((size_t) h.count);
+		st = ibk_io_read_dense(path, off, &h, grids[j].data(), h.count, &off);
+	}
+	if (st != IBK_OK) return st;
+	const int n = (int) (x.size() / (size_t) s->dims);
+	const double* ue[kMaxDims] = {nullptr, nullptr, nullptr};
+	for (int c = 0; c < s->dims; ++c) ue[c] = grids[c].data();
+	if ((st = ibk_server_admit(handle, member, n, x.data(), ue)) != IBK_OK) return st;
+	Member& m = s->members[member];
+	if (n > 0) st = cuda_ok(cudaMemcpy(m.xref, xref.data(), sizeof(double) * xref.size(), cudaMemcpyHostToDevice), "cudaMemcpy");
+	for (int c = 0; c < s->dims && st == IBK_OK; ++c)
+		st = cuda_ok(cudaMemcpy(m.fe[c], grids[s->dims + c].data(), sizeof(double) * grids[s->dims + c].size(),
+		                        cudaMemcpyHostToDevice), "cudaMemcpy");
+	return st;
+}
+
 ibk_status ibk_server_get_stats(ibk_server handle, ibk_server_stats* stats)
 {
 	Server* s = reinterpret_cast<Server*>(handle);

@@ -330,6 +330,35 @@ ibk_status ibk_server_reset_stats(ibk_server server);
 ibk_status ibk_server_run_poisson(ibk_server server, double rate_per_s, int requests,
                                   unsigned long long seed, ibk_server_stats* stats);
 
+/* Checkpoint of one member in the linalg::io binary format (below): its
+ * positions and spring rest shape (matrices n x dims), grid velocity and grid
+ * force density (one vector per component), in that order.  Synchronising.
+ * ibk_server_admit_from admits a member from such a file. */
+ibk_status ibk_server_save(ibk_server server, int member, const char* path);
+ibk_status ibk_server_admit_from(ibk_server server, int member, const char* path);
+
+/* ---- linalg::io binary containers (include/linalg/io.h:66-94, 425-533) ----
+ * Each dense vector / matrix is a 32-bit magic number ('v','e' or 'm','a' |
+ * 'd' dense | 'd' FP64 or 's' FP32), three 32-bit ints (rows, cols, values)
+ * and the values column-major; scalars are raw bytes; objects follow each
+ * other in one file.  Host arrays.  Writes are FP64; reads accept FP32 or
+ * FP64 values and return FP64.  Sparse containers are not read. */
+typedef struct {
+	int magic;
+	int matrix;             /* 1: matrix, 0: vector */
+	int rows, cols;
+	int count;              /* rows * cols */
+} ibk_io_header;
+
+ibk_status ibk_io_write_dense(const char* path, int append, int matrix, int rows, int cols,
+                              const double* values);
+ibk_status ibk_io_write_scalar(const char* path, int append, double value);
+/* Reads the object at byte `offset`; values may be NULL to read the header
+ * only; *next_offset (optional) receives the offset of the next object. */
+ibk_status ibk_io_read_dense(const char* path, long long offset, ibk_io_header* header, double* values,
+                             long long capacity, long long* next_offset);
+ibk_status ibk_io_read_scalar(const char* path, long long offset, double* value, long long* next_offset);
+
 /* Human-readable text of the last error on the calling host thread. */
 const char* ibk_last_error(void);
 const char* ibk_status_string(ibk_status status);

@@ -132,3 +132,31 @@ def test_poisson_load_serves_every_request(ibk, cuda):
     assert st["requests"] == 200
     assert 0 < st["p50_ms"] <= st["p99_ms"] <= st["max_ms"]
     assert st["launches"] >= 1 and st["wall_s"] > 0
+
+
+def test_checkpoint_restores_a_member(ibk, cuda, tmp_path):
+    """A member saved in the linalg::io format and admitted into another
+    server continues bit for bit like the original."""
+    ws = _members()[:2]
+    plans, ues = zip(*[_velocities(ibk, w, 500 + i) for i, w in enumerate(ws)])
+    a = _server(ibk, ws, ues, slots=2)
+    for _ in range(3):
+        a.submit(0)
+        a.submit(1)
+    a.drain()
+    path = str(tmp_path / "member0.bin")
+    a.save(0, path)
+    objs = ibk.io_read(path)
+    assert [o.shape for o in objs[:2]] == [(ws[0].n, 3), (ws[0].n, 3)]
+    assert len(objs) == 2 + 2 * 3
+    insts = [ibk.Instance(ibk.Mac(w.refinement), _domain(ibk, w)) for w in ws]
+    b = ibk.Server(insts, ibk.Bspline(3), ibk.FP32C, slots=1, dt=DT, k=K, max_points=sum(w.n for w in ws))
+    b.admit_from(0, path)
+    for srv in (a, b):
+        srv.submit(0)
+        srv.drain()
+    xa, fa = a.read(0, ws[0].n, plans[0].sizes())
+    xb, fb = b.read(0, ws[0].n, plans[0].sizes())
+    assert np.array_equal(xa, xb)
+    for u, v in zip(fa, fb):
+        assert np.array_equal(u, v)
