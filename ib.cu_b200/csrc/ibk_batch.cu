@@ -66,6 +66,8 @@ struct BatchTable {
 	const int* active;      // [num_active]: instances bound with points
 	const int* spre;        // [num_active + 1]: prefix of their spread items
 	const int* ipre;        // [num_active + 1]: prefix of their interpolation items
+	const CUtensorMap* maps; // [count * 3]: velocity grids of the active instances
+	const int* use_tma;     // [count]: 1 when the maps are valid for TMA staging
 	int count;
 };
 
@@ -192,8 +194,9 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 }
 
 // Persistent interpolation over the active instances' (tile, component)
-// items (plain staging of each tile's region); with step set, the serving
-// epilogue (advection + spring force) is applied.
+// items (each tile's region staged by one TMA copy where the instance's grids
+// allow it, else by plain loads); with step set, the serving epilogue
+// (advection + spring force) is applied.
 template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
 batch_interp_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
@@ -218,8 +221,11 @@ batch_interp_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		ConstCompPtrs ue;
 #pragma unroll
 		for (int c = 0; c < kMaxDims; ++c) ue.p[c] = so.ue[c];
-		interp_tile<D, DIMS, PREC>(si.g, si.ti, so.n, so.x, perm, so.pbase, off + si.bin_i, ue, so.ul, nullptr, 0,
-		                           status, step ? &epi : nullptr, local / DIMS, local % DIMS);
+		const bool ok = interp_tile<D, DIMS, PREC>(si.g, si.ti, so.n, so.x, perm, so.pbase, off + si.bin_i, ue,
+		                                           so.ul, t.maps + (size_t) inst * kMaxDims,
+		                                           __ldg(t.use_tma + inst), true, status,
+		                                           step ? &epi : nullptr, local / DIMS, local % DIMS);
+		if (!ok) return;            // a staging copy never completed: stop this CTA
 		__syncthreads();
 	}
 }
@@ -257,6 +263,12 @@ struct Batch {
 	std::vector<BatchIO> io_h;
 	unsigned char* d_table = nullptr; // header, io, pstart, active, spre, ipre
 	size_t table_bytes = 0, off_io = 0, off_pstart = 0, off_active = 0, off_spre = 0, off_ipre = 0;
+	size_t off_maps = 0, off_tma = 0;
+	// tensor maps of the velocity grids, encoded on the host per instance and
+	// component, reused while the bound pointer and the tile shape stay
+	std::vector<CUtensorMap> map_cache;
+	std::vector<const double*> map_ptr;     // grid the cached map describes
+	std::vector<char> map_ok;
 	unsigned char* h_ring[kRing] = {};
 	cudaEvent_t ring_ev[kRing] = {};
 	int ring_next = 0;
@@ -301,6 +313,8 @@ BatchTable table_view(const Batch& b)
 	t.active = reinterpret_cast<const int*>(b.d_table + b.off_active);
 	t.spre = reinterpret_cast<const int*>(b.d_table + b.off_spre);
 	t.ipre = reinterpret_cast<const int*>(b.d_table + b.off_ipre);
+	t.maps = reinterpret_cast<const CUtensorMap*>(b.d_table + b.off_maps);
+	t.use_tma = reinterpret_cast<const int*>(b.d_table + b.off_tma);
 	t.count = b.count;
 	return t;
 }
@@ -437,8 +451,34 @@ size_t region_bytes(int M, const TileGeom& tg, int dims)
 	return sizeof(double) * v + 128;
 }
 
-// The table of a binding: header, io, pstart, active list and item prefixes.
-void build_table(const Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
+// Tensor maps of instance i's velocity grids for its interpolation regions,
+// from the cache when the grid pointers are unchanged; false when any grid
+// or box breaks a TMA rule (the instance is then staged by plain loads).
+bool instance_maps(Batch& b, int i, const BatchIO& o)
+{
+	const BatchInst& bi = b.inst_h[i];
+	const int hl = 1 + ((b.M - 1) >> 1), hh = 1 + b.M / 2;
+	if ((bi.ti.T[0] & 1) || (hl & 1)) return false;     // region x origin must stay even
+	int box[3] = {1, 1, 1};
+	for (int d = 0; d < b.dims; ++d) {
+		box[d] = bi.ti.T[d] + hl + hh;
+		if (d == 0) box[d] = (box[d] + 1) & ~1;
+	}
+	bool ok = true;
+	for (int c = 0; c < b.dims; ++c) {
+		const size_t k = (size_t) i * kMaxDims + c;
+		if (b.map_ptr[k] != o.ue[c]) {
+			b.map_ok[k] = o.ue[c] && grid_tensor_map(&b.map_cache[k], o.ue[c], bi.g.comp[c], b.dims, box);
+			b.map_ptr[k] = o.ue[c];
+		}
+		ok = ok && b.map_ok[k];
+	}
+	return ok;
+}
+
+// The table of a binding: header, io, pstart, active list, item prefixes and
+// the active instances' tensor maps.
+void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 {
 	std::memset(out, 0, b.table_bytes);
 	BatchHeader* h = reinterpret_cast<BatchHeader*>(out);
@@ -447,11 +487,17 @@ void build_table(const Batch& b, const std::vector<BatchIO>& io, unsigned char* 
 	int* spre = reinterpret_cast<int*>(out + b.off_spre);
 	int* ipre = reinterpret_cast<int*>(out + b.off_ipre);
 	std::memcpy(out + b.off_io, io.data(), sizeof(BatchIO) * io.size());
+	CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(out + b.off_maps);
+	int* use_tma = reinterpret_cast<int*>(out + b.off_tma);
 	int total = 0, nact = 0, ns = 0, ni = 0;
 	for (int i = 0; i < b.count; ++i) {
 		pstart[i] = total;
 		total += io[i].n;
 		if (io[i].n == 0) continue;
+		if (instance_maps(b, i, io[i])) {
+			use_tma[i] = 1;
+			for (int c = 0; c < b.dims; ++c) maps[(size_t) i * kMaxDims + c] = b.map_cache[(size_t) i * kMaxDims + c];
+		}
 		active[nact] = i;
 		spre[nact] = ns;
 		ipre[nact] = ni;
@@ -537,6 +583,7 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 	b.smem_s = smem_s;
 	b.smem_i = region_max;
 	b.config = cfg;
+	std::fill(b.map_ptr.begin(), b.map_ptr.end(), nullptr);   // boxes follow the tiles
 	drop_graphs(b);
 	if (b.bound) {
 		// the bound table's item prefixes follow the tiles: rebuild it
@@ -640,7 +687,12 @@ ibk_status ibk_batch_create(int count, const ibk_instance_desc* instances, ibk_d
 	b->off_active = al(b->off_pstart + sizeof(int) * ((size_t) count + 1));
 	b->off_spre = al(b->off_active + sizeof(int) * (size_t) count);
 	b->off_ipre = al(b->off_spre + sizeof(int) * ((size_t) count + 1));
-	b->table_bytes = b->off_ipre + sizeof(int) * ((size_t) count + 1);
+	b->off_maps = al(b->off_ipre + sizeof(int) * ((size_t) count + 1));
+	b->off_tma = al(b->off_maps + sizeof(CUtensorMap) * kMaxDims * (size_t) count);
+	b->table_bytes = b->off_tma + sizeof(int) * (size_t) count;
+	b->map_cache.resize((size_t) count * kMaxDims);
+	b->map_ptr.assign((size_t) count * kMaxDims, nullptr);
+	b->map_ok.assign((size_t) count * kMaxDims, 0);
 	size_t cap = 0;
 	if (st == IBK_OK) st = grow(&b->d_table, cap, b->table_bytes, "cudaMalloc");
 	for (int r = 0; r < kRing && st == IBK_OK; ++r) {

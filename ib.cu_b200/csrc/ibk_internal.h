@@ -1,5 +1,6 @@
 // Host-side internals shared by the library's translation units.
 #pragma once
+#include <cuda.h>
 #include <cuda_runtime.h>
 #include <string>
 #include <vector>
@@ -97,6 +98,11 @@ ibk_status check_domain(const ibk_domain* domain, int tag, int refinement);
 // Geometry of every component grid of a validated domain.
 ibk_status make_geometry(const ibk_domain* domain, int tag, int refinement, int meshwidths, GridGeom& g,
                          ibk_grid_info& info);
+
+// Tensor map of one FP64 component grid for TMA boxes of `box` elements per
+// axis; false when a TMA rule is violated (16-byte base and strides, box rows
+// a multiple of 16 bytes, at most 256 elements per box axis).
+bool grid_tensor_map(CUtensorMap* map, const double* base, const CompGeom& cg, int dims, const int* box);
 
 ibk_status set_error(ibk_status s, const std::string& msg);
 ibk_status check_launch(const char* what);

@@ -146,6 +146,8 @@ EncodeTiledFn encode_fn()
 	return fn;
 }
 
+} // namespace
+
 // Tensor map of one FP64 component grid with box `box` (elements per axis).
 // False when the grid or box violates a TMA rule (16-byte base and strides,
 // box rows a multiple of 16 bytes, at most 256 elements per box axis).
@@ -170,6 +172,8 @@ bool grid_tensor_map(CUtensorMap* map, const double* base, const CompGeom& cg, i
 	                CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
 	return r == CUDA_SUCCESS;
 }
+
+namespace {
 
 template <int KIND, int ORDER, int DIMS, int PREC>
 ibk_status interp_impl(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul)

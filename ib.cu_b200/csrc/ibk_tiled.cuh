@@ -509,13 +509,16 @@ struct StepEpilogue {
 };
 
 // One (tile, component) of the interpolation; every thread of the CTA calls
-// it.  maps/use_tma select TMA staging (single-grid launches only); epi, when
-// not null, adds the serving-step epilogue; ul may then be null.
+// it.  maps/use_tma select TMA staging (maps_global: the maps live in global
+// memory, written by a copy before the launch); epi, when not null, adds the
+// serving-step epilogue; ul may then be null.  Returns false only when a
+// bounded wait for the staging copy gave up (the status word records it and
+// the CTA must stop).
 template <typename D, int DIMS, int PREC>
-__device__ __forceinline__ void interp_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
+__device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
                                             const int* __restrict__ perm, int pbase, const int* __restrict__ off,
                                             const ConstCompPtrs& ue, double* __restrict__ ul,
-                                            const CUtensorMap* maps, int use_tma, int* status,
+                                            const CUtensorMap* maps, int use_tma, bool maps_global, int* status,
                                             const StepEpilogue* epi, int t, int c)
 {
 	using P = Pattern<D::M, DIMS, D::every_other>;
@@ -529,7 +532,7 @@ __device__ __forceinline__ void interp_tile(const GridGeom& g, const TileGeom& t
 
 	const int start = __ldg(off + t * tg.nclass);
 	const int end = __ldg(off + (t + 1) * tg.nclass);
-	if (start == end) return;
+	if (start == end) return true;
 	const CompGeom& cg = g.comp[c];
 	const double* __restrict__ u = ue.p[c];
 	int tc[3] = {0, 0, 0};
@@ -566,6 +569,7 @@ __device__ __forceinline__ void interp_tile(const GridGeom& g, const TileGeom& t
 		if (threadIdx.x == 0) mbar_init(&bar, 1);
 		__syncthreads();
 		if (threadIdx.x == 0) {
+			if (maps_global) tensormap_acquire(maps + c);
 			mbar_arrive_expect_tx(&bar, (unsigned) (sizeof(double) * E[0] * E[1] * E[2]));
 			if constexpr (DIMS == 3) tma_load_3d(reg, maps + c, rlo[0], rlo[1], rlo[2], &bar);
 			else tma_load_2d(reg, maps + c, rlo[0], rlo[1], &bar);
@@ -575,7 +579,8 @@ __device__ __forceinline__ void interp_tile(const GridGeom& g, const TileGeom& t
 		__shared__ int tma_ok;
 		if (threadIdx.x == 0) tma_ok = mbar_wait_bounded(&bar, 0, status) ? 1 : 0;
 		__syncthreads();
-		if (!tma_ok) return;
+		if (!tma_ok) return false;
+		if (threadIdx.x == 0) mbar_inval(&bar);   // every thread is past the wait
 		if (!interior) {
 			// out-of-range slabs: wrap periodic, clamp solid (interpolate.h:16-22)
 #pragma unroll 1
@@ -777,6 +782,7 @@ __device__ __forceinline__ void interp_tile(const GridGeom& g, const TileGeom& t
 			epi->fl[i] = __dmul_rn(-epi->k, __dsub_rn(xn, __ldg(epi->xref + i)));
 		}
 	}
+	return true;
 }
 
 template <typename D, int DIMS, int PREC>
@@ -787,7 +793,7 @@ interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const __grid_constant__ TmaMaps maps, int use_tma, int* status)
 {
 	// grid: (tile, component)
-	interp_tile<D, DIMS, PREC>(g, tg, n, x, perm, 0, off, ue, ul, maps.map, use_tma, status, nullptr,
+	interp_tile<D, DIMS, PREC>(g, tg, n, x, perm, 0, off, ue, ul, maps.map, use_tma, false, status, nullptr,
 	                           blockIdx.x, blockIdx.y);
 }
 

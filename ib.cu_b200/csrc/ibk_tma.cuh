@@ -31,6 +31,21 @@ __device__ __forceinline__ void mbar_init(uint64_t* bar, unsigned count)
 	asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
 }
 
+// Ends the barrier object so its memory can be initialised again (a
+// persistent CTA reuses one barrier for every tile it stages).
+__device__ __forceinline__ void mbar_inval(uint64_t* bar)
+{
+	asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_addr(bar)) : "memory");
+}
+
+// A tensor map in global memory written before the launch (by a copy from
+// the host) is made visible to the tensor-copy proxy before its first use.
+__device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map)
+{
+	asm volatile("fence.proxy.tensormap::generic.acquire.gpu [%0], 128;"
+	             :: "l"(reinterpret_cast<uint64_t>(map)) : "memory");
+}
+
 __device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, unsigned bytes)
 {
 	asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;"
