@@ -41,7 +41,7 @@ FP64, FP32C = 0, 1
 # Every symbol include/ibk.h declares (checked by the CPU test suite).
 ABI_SYMBOLS = (
     "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve", "ibk_plan_set_tiles",
-    "ibk_spread", "ibk_interpolate", "ibk_sort_keys",
+    "ibk_spread", "ibk_interpolate", "ibk_sort_keys", "ibk_force_moments", "ibk_grid_totals",
     "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
     "ibk_plan_launch_count", "ibk_plan_check", "ibk_interpolate_noalloc",
     "ibk_batch_create", "ibk_batch_destroy", "ibk_batch_info", "ibk_batch_bind",
@@ -156,6 +156,10 @@ def lib() -> ctypes.CDLL:
         L.ibk_spread.argtypes = [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp), _vp]
         L.ibk_interpolate.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_vp), _vp, _vp]
         L.ibk_sort_keys.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
+        L.ibk_force_moments.argtypes = [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]
+        L.ibk_force_moments.restype = ctypes.c_int
+        L.ibk_grid_totals.argtypes = [_vp, ctypes.POINTER(_vp), _vp, _vp]
+        L.ibk_grid_totals.restype = ctypes.c_int
         L.ibk_plan_set_profiling.argtypes = [_vp, ctypes.c_int]
         L.ibk_plan_kernel_stats.argtypes = [_vp, ctypes.POINTER(KernelStat), ctypes.c_int,
                                             ctypes.POINTER(ctypes.c_int)]
@@ -210,7 +214,7 @@ def lib() -> ctypes.CDLL:
         L.ibk_status_string.restype = ctypes.c_char_p
         L.ibk_status_string.argtypes = [ctypes.c_int]
         for name in ("ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve",
-                     "ibk_spread", "ibk_interpolate", "ibk_sort_keys", "ibk_plan_set_profiling",
+                     "ibk_spread", "ibk_interpolate", "ibk_sort_keys", "ibk_force_moments", "ibk_grid_totals", "ibk_plan_set_profiling",
                      "ibk_plan_kernel_stats", "ibk_plan_reset_stats", "ibk_plan_launch_count",
                      "ibk_plan_check"):
             getattr(L, name).restype = ctypes.c_int
@@ -392,6 +396,20 @@ class Plan:
         v = ctypes.c_longlong()
         check(lib().ibk_plan_launch_count(self._h, ctypes.byref(v)))
         return int(v.value)
+
+    def force_moments(self, n, x, fl, stream=None):
+        """FP64 total force and torque of the point forces (deterministic): 6 values."""
+        import torch
+        out = torch.empty(6, dtype=torch.float64, device=x.device)
+        check(lib().ibk_force_moments(self._h, int(n), _ptr(x), _ptr(fl), _ptr(out), _stream_handle(stream)))
+        return out.cpu().numpy()
+
+    def grid_totals(self, fe, stream=None):
+        """FP64 h^dims * sum over faces of each spread component (deterministic)."""
+        import torch
+        out = torch.empty(self.dims, dtype=torch.float64, device=fe[0].device)
+        check(lib().ibk_grid_totals(self._h, self._comp_ptrs(fe), _ptr(out), _stream_handle(stream)))
+        return out.cpu().numpy()
 
     def sort_keys(self, comp, n, x, keys, stream=None):
         check(lib().ibk_sort_keys(self._h, int(comp), int(n), _ptr(x), _ptr(keys),

@@ -77,7 +77,7 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 }
 
 // Scratch slots of a plan.
-enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotBinMax = 5 };
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotBinMax = 5, kSlotSums = 6 };
 
 // Tile decomposition of a plan's grid for stencil width M.
 // pref_extent: preferred tile extent per axis (nullptr: 16 cells).

@@ -135,6 +135,16 @@ ibk_status ibk_interpolate(ibk_plan plan, int n, const double* x,
 ibk_status ibk_sort_keys(ibk_plan plan, int component, int n, const double* x,
                          int* keys, void* stream);
 
+/* Conservation sums in FP64 with a fixed summation order (the same result on
+ * every run).  ibk_force_moments: out[0..3) = sum_p F_p, out[3..6) = sum_p
+ * x_p cross F_p (2-D: out[5] only).  ibk_grid_totals: out[c] = h^dims *
+ * sum_j fe[c][j], the grid side of the force balance (equal to sum_p F_p,c in
+ * periodic domains, where spreading conserves force).  out: device arrays of
+ * 6 and dims doubles, written in stream order. */
+ibk_status ibk_force_moments(ibk_plan plan, int n, const double* x, const double* fl, double* out,
+                             void* stream);
+ibk_status ibk_grid_totals(ibk_plan plan, double* const* fe, double* out, void* stream);
+
 /* Instrumentation (no reference counterpart; the reference times with
  * cuda::timer, include/cuda/timer.h:9-19).  While profiling is enabled every
  * kernel launch of the plan is bracketed by CUDA events on its stream;

@@ -1,0 +1,147 @@
+"""Size-independent properties at full size, on the GPU through the C ABI.
+
+The oracle finishes only small cases, so the benchmark-sized workloads are
+checked through properties the immersed-boundary operators have at any size:
+
+* the chosen FP32C form against the plain FP64 path on the 512 x 256 x 512
+  channel (10,923,000 points): normwise |err| <= 1e-5 * max|ref| per
+  component, for spread and interpolation; FP32C spread is deterministic
+  (exact fixed-point sums), so two runs agree bit for bit;
+* force conservation in a periodic domain: h^3 * sum over faces of each
+  spread component equals the sum of the point forces (FP64 path: 1e-12,
+  FP32C: 1e-5, relative to sum |F|), both sums taken by the library's FP64
+  conservation kernels;
+* adjointness in a periodic domain: h^3 <spread(F), u> = <F, interp(u)>
+  (FP64 path, 1e-12 relative to sum |F_p U_p|);
+* translation by one cell along a periodic axis permutes the spread grid
+  (FP64 path, 1e-12 relative to max |fe|).
+"""
+import numpy as np
+import pytest
+
+pytestmark = pytest.mark.gpu
+
+FP32C_TOL = 1e-5
+
+
+def _dev(a, device):
+    import torch
+    return torch.from_numpy(np.ascontiguousarray(a)).to(device)
+
+
+def _plan(ibk, w, precision):
+    dom = ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)])
+    return ibk.Plan(ibk.Mac(w.refinement), dom, ibk.Bspline(3), precision)
+
+
+def _periodic_instance():
+    from ib_cu_b200 import workloads as W
+    rng = np.random.default_rng(77)
+    return W.small_instance(rng, 96, 30, False, "periodic96")
+
+
+def test_large_channel_fp32c_against_fp64_and_deterministic(ibk, cuda):
+    import torch
+    from ib_cu_b200 import workloads as W
+    w = W.large_channel()
+    p32, p64 = _plan(ibk, w, ibk.FP32C), _plan(ibk, w, ibk.FP64)
+    x, f = _dev(w.x, cuda), _dev(w.f, cuda)
+    sizes = p32.sizes()
+    gen = torch.Generator(device=cuda)
+    gen.manual_seed(5)
+    ue = [torch.randn(s, generator=gen, dtype=torch.float64, device=cuda) for s in sizes]
+    fe32 = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    fe64 = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    p32.spread(w.n, x, f, fe32)
+    p64.spread(w.n, x, f, fe64)
+    for a, b in zip(fe32, fe64):
+        assert float((a - b).abs().max()) <= FP32C_TOL * float(b.abs().max())
+    again = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    p32.spread(w.n, x, f, again)
+    for a, b in zip(fe32, again):
+        assert torch.equal(a, b)
+    del fe64, again
+    u32 = torch.empty(3 * w.n, dtype=torch.float64, device=cuda)
+    u64 = torch.empty(3 * w.n, dtype=torch.float64, device=cuda)
+    p32.interpolate(w.n, x, ue, u32)
+    p64.interpolate(w.n, x, ue, u64)
+    for c in range(3):
+        a, b = u32[c * w.n:(c + 1) * w.n], u64[c * w.n:(c + 1) * w.n]
+        assert float((a - b).abs().max()) <= FP32C_TOL * float(b.abs().max())
+    p32.check()
+    p64.check()
+
+
+@pytest.mark.parametrize("precision,tol", [(0, 1e-12), (1, FP32C_TOL)])
+def test_periodic_force_conservation(ibk, cuda, precision, tol):
+    import torch
+    w = _periodic_instance()
+    plan = _plan(ibk, w, precision)
+    x, f = _dev(w.x, cuda), _dev(w.f, cuda)
+    fe = [torch.empty(s, dtype=torch.float64, device=cuda) for s in plan.sizes()]
+    plan.spread(w.n, x, f, fe)
+    grid = plan.grid_totals(fe)
+    points = plan.force_moments(w.n, x, f)
+    total_abs = np.abs(w.f.reshape(3, -1)).sum(axis=1)
+    for c in range(3):
+        assert abs(grid[c] - points[c]) <= tol * total_abs[c]
+    # the sums are deterministic
+    assert np.array_equal(plan.grid_totals(fe), grid)
+    assert np.array_equal(plan.force_moments(w.n, x, f), points)
+    # and match a host FP64 sum
+    assert np.allclose(points[:3], w.f.reshape(3, -1).sum(axis=1), rtol=0, atol=1e-12 * total_abs.max())
+
+
+def test_force_moments_known_answer(ibk, cuda):
+    """Two points: total force and torque about the origin, exactly."""
+    from ib_cu_b200 import workloads as W
+    w = W.single_rbc(seed=3)
+    plan = _plan(ibk, w, ibk.FP64)
+    x = np.array([1.0, 0.0, 0.0, 2.0, 0.5, 0.0])            # (1,0,0.5) and (0,2,0) as x[d*n+p]
+    fl = np.array([0.0, 1.0, 0.0, 0.0, 3.0, 0.0])           # (0,0,3) and (1,0,0)
+    m = plan.force_moments(2, _dev(x, cuda), _dev(fl, cuda))
+    # F = (1, 0, 3); tau = (1,0,0.5)x(0,0,3) + (0,2,0)x(1,0,0) = (0,-3,0) + (0,0,-2)
+    assert np.array_equal(m, np.array([1.0, 0.0, 3.0, 0.0, -3.0, -2.0]))
+
+
+def test_periodic_adjointness_fp64(ibk, cuda):
+    import torch
+    w = _periodic_instance()
+    plan = _plan(ibk, w, ibk.FP64)
+    x, f = _dev(w.x, cuda), _dev(w.f, cuda)
+    sizes = plan.sizes()
+    gen = torch.Generator(device=cuda)
+    gen.manual_seed(9)
+    u = [torch.randn(s, generator=gen, dtype=torch.float64, device=cuda) for s in sizes]
+    fe = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    plan.spread(w.n, x, f, fe)
+    U = torch.empty(3 * w.n, dtype=torch.float64, device=cuda)
+    plan.interpolate(w.n, x, u, U)
+    h3 = 1.0 / plan.info.resolution ** 3
+    lhs = h3 * sum(float((a * b).sum()) for a, b in zip(fe, u))
+    rhs = float((f * U).sum())
+    scale = float((f * U).abs().sum())
+    assert abs(lhs - rhs) <= 1e-12 * scale
+
+
+def test_translation_by_one_cell_permutes_fp64(ibk, cuda):
+    import torch
+    w = _periodic_instance()
+    plan = _plan(ibk, w, ibk.FP64)
+    h = w.lengths[0] / w.refinement
+    xs = w.x.copy().reshape(3, -1)
+    x0 = _dev(xs.reshape(-1), cuda)
+    xs[0] += h
+    x1 = _dev(xs.reshape(-1), cuda)
+    f = _dev(w.f, cuda)
+    sizes = plan.sizes()
+    fe0 = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    fe1 = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    plan.spread(w.n, x0, f, fe0)
+    plan.spread(w.n, x1, f, fe1)
+    for c in range(3):
+        p = plan.info.comp_points(c)
+        a = fe0[c].reshape(p[2], p[1], p[0])
+        b = fe1[c].reshape(p[2], p[1], p[0])
+        shifted = torch.roll(a, shifts=1, dims=2)
+        assert float((shifted - b).abs().max()) <= 1e-12 * float(a.abs().max())
