@@ -20,7 +20,9 @@
 //   indices.  Every point of the tile then gathers its M^dims nodes from
 //   shared memory.
 //     FP64:  exact weights, sums in the reference's pattern order (bit-exact).
-//     FP32C: FP32 weights applied to the FP64 values, FP64 accumulation.
+//     FP32C: the staged values rounded to FP32 in shared memory (half the
+//            shared-memory traffic of the gathers), FP32 weights, FP32 row
+//            sums of M products, FP64 sum of the rows.
 #pragma once
 #include "ibk_device.cuh"
 #include "ibk_bin.cuh"
@@ -664,6 +666,28 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 		}
 		__syncthreads();
 	}
+	if constexpr (PREC == IBK_PRECISION_FP32C) {
+		// the staged FP64 values rounded to FP32 in place, in chunks: a chunk's
+		// FP32 words land on FP64 elements that are read by then
+		constexpr int kChunk = kTileThreads * 8;
+		const int vol = E[0] * E[1] * E[2];
+		float* regf = reinterpret_cast<float*>(reg);
+		for (int b0 = 0; b0 < vol; b0 += kChunk) {
+			double v8[8];
+#pragma unroll
+			for (int q = 0; q < 8; ++q) {
+				const int i = b0 + q * kTileThreads + threadIdx.x;
+				v8[q] = i < vol ? reg[i] : 0.0;
+			}
+			__syncthreads();
+#pragma unroll
+			for (int q = 0; q < 8; ++q) {
+				const int i = b0 + q * kTileThreads + threadIdx.x;
+				if (i < vol) regf[i] = (float) v8[q];
+			}
+			__syncthreads();
+		}
+	}
 	for (; it < end; it += kTileThreads) {
 		const int p = p_next;
 		double z[DIMS];
@@ -718,25 +742,22 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 					v = __dadd_rn(v, __dmul_rn(wt, reg[k]));   // interpolate.h:71-72
 				}
 			} else {
-				// FP32 delta weights applied to the FP64 values, FP64 accumulation
+				// FP32 weights and FP32 staged values; FP32 row sums, FP64 total
 				float w32[DIMS][M];
-				double w[DIMS][M];
 #pragma unroll
-				for (int d = 0; d < DIMS; ++d) {
-					weights32<D>((float) dl[d], w32[d]);
-#pragma unroll
-					for (int m = 0; m < M; ++m) w[d][m] = (double) w32[d][m];
-				}
+				for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w32[d]);
+				const float* regf = reinterpret_cast<const float*>(reg);
 				v = 0.0;
 				constexpr int R = DIMS == 3 ? M * M : M;
 #pragma unroll
 				for (int r = 0; r < R; ++r) {
 					const int m1 = r % M, m2 = r / M;
-					const double* row = reg + base + (DIMS == 3 ? (m2 * E[1] + m1) * E[0] : m1 * E[0]);
-					double rs = 0.0;
+					const float* row = regf + base + (DIMS == 3 ? (m2 * E[1] + m1) * E[0] : m1 * E[0]);
+					float rs = 0.0f;
 #pragma unroll
-					for (int m0 = 0; m0 < M; ++m0) rs = fma(w[0][m0], row[m0], rs);
-					v = fma(DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1], rs, v);
+					for (int m0 = 0; m0 < M; ++m0) rs = fmaf(w32[0][m0], row[m0], rs);
+					const double w12 = DIMS == 3 ? (double) w32[1][m1] * (double) w32[2][m2] : (double) w32[1][m1];
+					v = fma(w12, (double) rs, v);
 				}
 			}
 		} else {
