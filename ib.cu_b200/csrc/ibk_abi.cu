@@ -325,8 +325,9 @@ ibk_status ibk_plan_set_tiles(ibk_plan handle, const int* spread_tile, const int
 		ts = make_tiles(plan->g, plan->tag, M, spread_tile);
 		long long tv = 1;
 		for (int d = 0; d < dims; ++d) tv *= ts.T[d];
+		const long long words = spread_strides(ts.T[0], ts.T[1], ts.T[2], dims).words;
 		const long long per_face = plan->precision == IBK_PRECISION_FP32C ? 12 : 8;
-		if (tv * per_face > 200 * 1024 || tv > 4 * 8192)
+		if (words * per_face > 200 * 1024 || tv > 4 * 8192)
 			return set_error(IBK_ERR_UNSUPPORTED, "spread tile needs more than 200 KB of shared memory");
 	}
 	if (interp_tile) {

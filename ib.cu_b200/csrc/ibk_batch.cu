@@ -536,9 +536,7 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		items_i += nitem_i[i];
 		if (bins_s >= (1LL << 30) || bins_i >= (1LL << 30) || items_s >= (1LL << 30) || items_i >= (1LL << 30))
 			return set_error(IBK_ERR_INVALID_ARGUMENT, "batch has too many tiles");
-		size_t tv = 1;
-		for (int d = 0; d < b.dims; ++d) tv *= (size_t) bi.ts.T[d];
-		tv_max = std::max(tv_max, tv);
+		tv_max = std::max(tv_max, (size_t) spread_strides(bi.ts.T[0], bi.ts.T[1], bi.ts.T[2], b.dims).words);
 		region_max = std::max(region_max, region_bytes(b.M, bi.ti, b.dims));
 	}
 	const size_t per_face = b.precision == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);

@@ -17,7 +17,7 @@
 namespace ibk {
 namespace {
 
-constexpr int kVector = 0x65760000, kMatrix = 0x616d0000, kDense = 0x6400, kSparse = 0x7300;
+constexpr int kVector = 0x65760000, kMatrix = 0x616d0000, kDense = 0x6400;   // sparse: 0x7300
 constexpr int kF64 = 0x64, kF32 = 0x73;
 
 struct File {

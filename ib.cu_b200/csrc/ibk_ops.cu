@@ -109,7 +109,7 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	// FP64: one double per face; FP32C: an FP64 total and a 32-bit working word
 	const size_t per_face = PREC == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
-	const size_t smem = per_face * (size_t) tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
+	const size_t smem = per_face * (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], DIMS).words;
 	// threads per CTA: 256 per 4096 faces of the tile (FP32C), 256 (FP64)
 	const int tv = tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
 	int nt = 256;

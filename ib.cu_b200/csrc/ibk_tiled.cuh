@@ -244,7 +244,7 @@ __device__ __forceinline__ int2 fix_terms2(float a0, float a1, float b)
 template <typename D, int DIMS, int PREC>
 __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGeom& cg, int n,
                                                  const double* __restrict__ x, const double* __restrict__ fc,
-                                                 int p, float scale, const int* lo, const int* hi, int T0, int T1,
+                                                 int p, float scale, const int* lo, const int* hi, int S1, int S2,
                                                  bool contig, typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
 {
 	constexpr int M = D::M, sh = (M - 1) >> 1;
@@ -285,7 +285,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 			const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
 			if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
 			const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
-			const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
+			const int row = (DIMS == 3 ? loc[2][m2] * S2 : 0) + loc[1][m1] * S1;
 #pragma unroll
 			for (int m0 = 0; m0 < M; ++m0)
 				if ((mask[0] >> m0) & rm)
@@ -299,7 +299,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 #pragma unroll
 		for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
 		if (contig) {
-			// node (m0, m1, m2) at first + (m2 * T1 + m1) * T0 + m0, where
+			// node (m0, m1, m2) at first + m2 * S2 + m1 * S1 + m0, where
 			// first is the (possibly outside) position of node (0, 0, 0)
 			int lb[DIMS];
 #pragma unroll
@@ -311,7 +311,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 					if (!found && ((mask[d] >> m) & 1u)) { v = loc[d][m] - m; found = true; }
 				lb[d] = v;
 			}
-			const int first = DIMS == 3 ? (lb[2] * T1 + lb[1]) * T0 + lb[0] : lb[1] * T0 + lb[0];
+			const int first = (DIMS == 3 ? lb[2] * S2 : 0) + lb[1] * S1 + lb[0];
 			int* base = acc + first;
 			constexpr unsigned kFull = (1u << M) - 1u;
 			const bool full = mask[0] == kFull && mask[1] == kFull && (DIMS < 3 || mask[2] == kFull);
@@ -321,7 +321,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
 					const int m1 = r % M, m2 = r / M;
 					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-					int* rowp = base + ((DIMS == 3 ? m2 * T1 : 0) + m1) * T0;
+					int* rowp = base + (DIMS == 3 ? m2 * S2 : 0) + m1 * S1;
 #pragma unroll
 					for (int m0 = 0; m0 + 1 < M; m0 += 2) {
 						const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
@@ -337,7 +337,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
 					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
 					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-					int* rowp = base + ((DIMS == 3 ? m2 * T1 : 0) + m1) * T0;
+					int* rowp = base + (DIMS == 3 ? m2 * S2 : 0) + m1 * S1;
 #pragma unroll
 					for (int m0 = 0; m0 + 1 < M; m0 += 2) {
 						const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
@@ -354,7 +354,7 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 				const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
 				if (!rm) continue;
 				const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-				const int row = ((DIMS == 3 ? loc[2][m2] * T1 : 0) + loc[1][m1]) * T0;
+				const int row = (DIMS == 3 ? loc[2][m2] * S2 : 0) + loc[1][m1] * S1;
 #pragma unroll
 				for (int m0 = 0; m0 < M; ++m0)
 					if ((mask[0] >> m0) & rm) fix_add_product(acc + row + loc[0][m0], w[0][m0], w12);
@@ -373,13 +373,13 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
                                             const CompPtrs& fe, int tile, int c)
 {
 	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
-	constexpr int M = D::M, sh = (M - 1) >> 1;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ RangeTable rt;
 
 	const CompGeom& cg = g.comp[c];
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
-	const int TV = T0 * T1 * T2;
+	const SpreadStrides ss = spread_strides(T0, T1, T2, DIMS);
+	const int TV = ss.words;    // padded accumulator words
 	// FP64: acc[TV] doubles.  FP32C: total[TV] doubles, then acc[TV] working words.
 	double* total = reinterpret_cast<double*>(smem_raw);
 	acc_t* acc = PREC == IBK_PRECISION_FP64 ? reinterpret_cast<acc_t*>(smem_raw)
@@ -420,7 +420,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	if constexpr (PREC == IBK_PRECISION_FP64) {
 		for (int it = threadIdx.x; it < ncand; it += NT)
 			spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, 0.0f,
-			                                lo, hi, T0, T1, contig, acc);
+			                                lo, hi, ss.S1, ss.S2, contig, acc);
 	} else {
 		// the tile's largest possible term, max|F| * max|w| * res (max|F| over
 		// its candidate bins, rounded to FP32, hence the 1.001), is scaled to
@@ -433,7 +433,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 			const int stop = min(ncand, base + kFixChunk);
 			for (int it = base + threadIdx.x; it < stop; it += NT)
 				spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, scale,
-				                                lo, hi, T0, T1, contig, acc);
+				                                lo, hi, ss.S1, ss.S2, contig, acc);
 			// fold the working words into the exact FP64 totals
 			__syncthreads();
 			for (int i = threadIdx.x; i < TV; i += NT) {
@@ -454,7 +454,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		const int l1 = r % e1, l2 = r / e1;
 		const size_t gi = (size_t) (lo[0] + l0) + (size_t) cg.points[0] *
 			((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
-		const int li = (l2 * T1 + l1) * T0 + l0;
+		const int li = (DIMS == 3 ? l2 * ss.S2 : 0) + l1 * ss.S1 + l0;
 		if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = acc[li];
 		else out[gi] = total[li] * inv_scale;
 	}
