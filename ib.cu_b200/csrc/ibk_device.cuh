@@ -88,7 +88,7 @@ __device__ __forceinline__ double ref_modulo(double x, double s) {
 
 // ------------------------------------------------------------ deltas ---
 // Each delta: meshwidths M, stencil ordering, phi in FP64 (bit-exact with the
-// reference) and a single-precision evaluation for the compensated path.
+// reference) and a single-precision evaluation for the FP32C form.
 
 enum DeltaKind { kBspline = 0, kPeskin = 1, kRoma = 2, kCosine = 3, kHat = 4 };
 
@@ -271,15 +271,6 @@ __device__ __forceinline__ AxisStep<M> axis_step(const GridGeom& g, const CompGe
 __device__ __forceinline__ int node_index(const GridGeom& g, const CompGeom& cg, int d, int i) {
 	if (g.solid[d]) return i;
 	return wrap_index(i, cg.cells[d]);
-}
-
-// ------------------------------------------------- compensated FP32 ---
-
-// Knuth's TwoSum: s + e == a + b exactly.
-__device__ __forceinline__ void two_sum(float a, float b, float& s, float& e) {
-	s = __fadd_rn(a, b);
-	float bb = __fsub_rn(s, a);
-	e = __fadd_rn(__fsub_rn(a, __fsub_rn(s, bb)), __fsub_rn(b, bb));
 }
 
 } // namespace ibk

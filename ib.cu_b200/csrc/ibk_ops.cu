@@ -106,7 +106,6 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off,
 	                                      PREC == IBK_PRECISION_FP32C ? fl : nullptr, &binmax);
 	if (s != IBK_OK) return s;
-	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
 	// FP64: one double per face; FP32C: an FP64 total and a 32-bit working word
 	const size_t per_face = PREC == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
 	const size_t smem = per_face * (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], DIMS).words;

@@ -257,8 +257,9 @@ def normwise(got, want):
 
 @pytest.mark.parametrize("name", ["single-rbc", "channel"])
 def test_workload_accuracy_fp32c(ibk, oracle, cuda, name):
-    """FP32 weights/products with exact fixed-point (spread) and TwoSum-
-    compensated (interpolate) accumulation vs the FP64 oracle."""
+    """FP32 weights and products with exact fixed-point sums (spread), FP32
+    staged values and row sums with an FP64 total (interpolate), against
+    the FP64 oracle."""
     from ib_cu_b200 import workloads as W
     w = W.CONFIGS[name](seed=12)
     g, plan, ue = _workload_case(ibk, oracle, w, cuda, precision=ibk.FP32C)
