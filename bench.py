@@ -426,6 +426,7 @@ def run_ours(args):
     # of the chosen form against it (the FP64 path matches the oracle: bit for
     # bit in interpolation, to summation order in spread)
     plain = None
+    refgpu = None
     if precision != ibk.FP64:
         plan64 = ibk.Plan(ibk.Mac(w.refinement), dom, ibk.Bspline(3), ibk.FP64)
         plan64.reserve(n)
@@ -464,6 +465,18 @@ def run_ours(args):
                  "steps": k64, "speedup": ms64 / ms_step,
                  "accuracy_vs_fp64": {k: v for k, v in err.items()},
                  "accuracy_note": "normwise: max|err|/max|ref| and rms(err)/rms(ref), worst component"}
+        # the reference's algorithm restated on the GPU, on the same inputs
+        if world == 1:
+            r = run_reference_gpu(ibk, w, plan64.info, x, f, ue)
+            if r is not None:
+                dev_s = max(float((a - b).abs().max()) / max(float(b.abs().max()), 1e-300)
+                            for a, b in zip(r["fe"], fe64))
+                dev_u = float((r["ul"] - ul64).abs().max())
+                refgpu = {k: v for k, v in r.items() if k not in ("fe", "ul")}
+                refgpu["speedup_of_fp32c"] = r["ms_per_step"] / ms_step
+                refgpu["speedup_of_fp64"] = r["ms_per_step"] / ms64
+                refgpu["agreement_with_fp64"] = {"spread_max_rel": dev_s, "interp_max_abs": dev_u}
+                del r
         del fe64, ul64, plan64
 
     extras = {}
@@ -502,12 +515,107 @@ def run_ours(args):
                 "note": "x and F copied in from pinned host memory, U copied out; grid fields stay device-resident"},
         "p50_ms": p50, "p99_ms": p99,
         "plain_fp64": plain,
+        "reference_algorithm_gpu": refgpu,
         "gpu_launches": launches,
         "clocks": clocks,
         "cpu_baseline": cpu,
     }
     line.update(extras)
     print(json.dumps(line), flush=True)
+
+
+# ------------------------------------- the reference's algorithm on the GPU
+REFGPU_LIB = os.path.join(ROOT, "baseline", "ref_gpu", "lib", "librefgpu.so")
+
+
+def grid_geom_struct(info, lengths, boundaries):
+    """The library's device GridGeom for a grid, from ibk_grid_info (same
+    values and IEEE operations as the library's host geometry)."""
+    import ctypes
+
+    class CompGeom(ctypes.Structure):
+        _fields_ = [("points", ctypes.c_int * 3), ("cells", ctypes.c_int * 3),
+                    ("shift", ctypes.c_double * 3), ("s_over_r", ctypes.c_double * 3),
+                    ("size", ctypes.c_longlong)]
+
+    class GridGeom(ctypes.Structure):
+        _fields_ = [("dims", ctypes.c_int), ("solid", ctypes.c_int * 3), ("length", ctypes.c_double * 3),
+                    ("length_safe", ctypes.c_double * 3), ("r", ctypes.c_double), ("res", ctypes.c_double),
+                    ("comp", CompGeom * 3)]
+
+    g = GridGeom()
+    dims = info.dims
+    g.dims = dims
+    r = info.resolution
+    g.r = r
+    res = 1.0
+    for _ in range(dims):
+        res = r * res
+    g.res = res
+    for d in range(dims):
+        g.solid[d] = 0 if boundaries[d] == 0 else 1
+        g.length[d] = lengths[d]
+        g.length_safe[d] = lengths[d] * (1.0 - 2.0 ** -52)
+    for c in range(dims):
+        cg = g.comp[c]
+        for d in range(dims):
+            cg.points[d] = info.points[c][d]
+            cg.cells[d] = info.cells[c][d]
+            cg.shift[d] = info.shift[c][d]
+            cg.s_over_r[d] = info.shift[c][d] / r
+        cg.size = info.size[c]
+    return g
+
+
+def run_reference_gpu(ibk, w, info, x, f, ue, steps=3):
+    """Times the GPU restatement of the reference's own algorithm (sort by
+    cell key, 8 sweeps of segmented sums into 8 planes, plane combine;
+    per-point gathers for interpolation) on the same inputs, FP64, on the
+    legacy default stream as the reference runs.  None when its library is
+    not built."""
+    import ctypes
+    import torch
+    if not os.path.exists(REFGPU_LIB):
+        return None
+    L = ctypes.CDLL(REFGPU_LIB)
+    L.refgpu_spread.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p, ctypes.c_void_p,
+                                ctypes.POINTER(ctypes.c_void_p)]
+    L.refgpu_interpolate.argtypes = [ctypes.c_void_p, ctypes.c_int, ctypes.c_void_p,
+                                     ctypes.POINTER(ctypes.c_void_p), ctypes.c_void_p]
+    L.refgpu_last_error.restype = ctypes.c_char_p
+    g = grid_geom_struct(info, w.lengths, w.boundaries)
+    n = w.n
+    dev = x.device
+    fe = [torch.empty(int(info.size[c]), dtype=torch.float64, device=dev) for c in range(3)]
+    ul = torch.empty(3 * n, dtype=torch.float64, device=dev)
+    fp = (ctypes.c_void_p * 3)(*[a.data_ptr() for a in fe])
+    up = (ctypes.c_void_p * 3)(*[a.data_ptr() for a in ue])
+    default = torch.cuda.default_stream(dev)
+
+    def step():
+        if L.refgpu_spread(ctypes.byref(g), n, x.data_ptr(), f.data_ptr(), fp) != 0:
+            raise RuntimeError(L.refgpu_last_error().decode())
+        if L.refgpu_interpolate(ctypes.byref(g), n, x.data_ptr(), up, ul.data_ptr()) != 0:
+            raise RuntimeError(L.refgpu_last_error().decode())
+
+    torch.cuda.synchronize()
+    step()
+    torch.cuda.synchronize()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    e0.record(default)
+    for _ in range(steps):
+        step()
+    e1.record(default)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / steps
+    return {"value": n / (ms / 1000.0), "unit": "points/s", "ms_per_step": ms, "steps": steps,
+            "fe": fe, "ul": ul,
+            "note": ("GPU restatement of the reference's algorithm, labelled as such (its own CUDA build does "
+                     "not compile with nvcc 12.9): per component a sort of the points by cell key (Thrust), "
+                     "a unique count with a host sync, 8 sweeps of weights, segmented sums (Thrust "
+                     "reduce_by_key) and plane scatters, a combine over 8 planes; interpolation as one thread "
+                     "per point gathering 64 nodes; FP64, temporaries allocated per call as the reference does")}
 
 
 # ------------------------------------------------ batched and serving legs
