@@ -123,6 +123,7 @@ batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int sp
 		i0 = __shfl_sync(0xffffffffu, i0, 0);
 		int key = 0, n = 0, p = 0;
 		const double* f = nullptr;
+		unsigned fbits[kMaxDims] = {0u, 0u, 0u};
 		if (active) {
 			const int i = gp < __ldg(t.pstart + i0 + 1) ? i0 : find_instance(t.pstart, t.count, gp, i0 + 1);
 			const BatchInst& bi = insts[i];
@@ -133,10 +134,11 @@ batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int sp
 			key = spread ? bi.bin_s + bin_key<M, DIMS>(bi.g, bi.ts, x, n, p)
 			             : bi.bin_i + bin_key<M, DIMS>(bi.g, bi.ti, x, n, p);
 			f = forces == 1 ? o.fl : o.fs;
+			if (forces) force_bits<DIMS>(f, n, p, true, fbits);
 		}
 		const unsigned mask = __ballot_sync(0xffffffffu, active);
 		// forces is uniform, and a bound instance with points has its force array
-		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + gp, forces ? f : nullptr, n, p, binmax);
+		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + gp, forces ? fbits : nullptr, binmax);
 	}
 }
 

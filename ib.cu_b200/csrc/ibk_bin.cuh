@@ -76,12 +76,12 @@ __device__ __forceinline__ int bin_key(const GridGeom& g, const TileGeom& tg, co
 }
 
 // Warp-aggregated rank of a point in its bin (one atomic per group of lanes
-// sharing a key); with f != nullptr also raises binmax[key * 3 + c] to the
-// FP32 |f[c * n + p]| of the group.  Every lane of `mask` must call it, all
-// with f null or all with f set.
+// sharing a key); with fbits != nullptr also raises binmax[key * 3 + c] to
+// the group's largest FP32 |F| bit pattern.  Every lane of `mask` must call
+// it, all with fbits null or all with fbits set.
 template <int DIMS>
 __device__ __forceinline__ void bin_rank(unsigned mask, int key, int* __restrict__ count, int2* __restrict__ kr_out,
-                                         const double* __restrict__ f, int n, int p, unsigned* __restrict__ binmax)
+                                         const unsigned* fbits, unsigned* __restrict__ binmax)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned peers = __match_any_sync(mask, key);
@@ -90,14 +90,22 @@ __device__ __forceinline__ void bin_rank(unsigned mask, int key, int* __restrict
 	if (lane == leader) base = atomicAdd(count + key, __popc(peers));
 	base = __shfl_sync(peers, base, leader);
 	*kr_out = make_int2(key, base + __popc(peers & ((1u << lane) - 1u)));
-	if (f != nullptr) {
+	if (fbits != nullptr) {
 #pragma unroll
 		for (int c = 0; c < DIMS; ++c) {
-			const unsigned v = __float_as_uint(fabsf((float) __ldg(f + (size_t) c * n + p)));
-			const unsigned m = __reduce_max_sync(peers, v);
+			const unsigned m = __reduce_max_sync(peers, fbits[c]);
 			if (lane == leader && m != 0u) atomicMax(binmax + (size_t) key * kMaxDims + c, m);
 		}
 	}
+}
+
+// FP32 |f[c * n + p]| bit patterns of one point (0 past the end).
+template <int DIMS>
+__device__ __forceinline__ void force_bits(const double* __restrict__ f, int n, int p, bool active, unsigned* fbits)
+{
+#pragma unroll
+	for (int c = 0; c < DIMS; ++c)
+		fbits[c] = active ? __float_as_uint(fabsf((float) __ldg(f + (size_t) c * n + p))) : 0u;
 }
 
 // With f != nullptr (spread) the kernel also raises binmax[key * 3 + c] to
@@ -112,10 +120,12 @@ bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	const bool active = p < n;
+	unsigned fbits[kMaxDims] = {0u, 0u, 0u};
+	if (f != nullptr) force_bits<DIMS>(f, n, p, active, fbits);   // loads in flight with x's
 	const int key = active ? bin_key<M, DIMS>(g, tg, x, n, p) : 0;
 	const unsigned mask = __ballot_sync(0xffffffffu, active);
 	if (!active) return;
-	bin_rank<DIMS>(mask, key, count, key_rank + p, f, n, p, binmax);
+	bin_rank<DIMS>(mask, key, count, key_rank + p, f != nullptr ? fbits : nullptr, binmax);
 }
 
 // Exclusive scan of the bin counts in two launches.  Each CTA owns a chunk
