@@ -567,7 +567,7 @@ def grid_geom_struct(info, lengths, boundaries):
     return g
 
 
-def run_reference_gpu(ibk, w, info, x, f, ue, steps=3):
+def run_reference_gpu(ibk, w, info, x, f, ue, steps=5):
     """Times the GPU restatement of the reference's own algorithm (sort by
     cell key, 8 sweeps of segmented sums into 8 planes, plane combine;
     per-point gathers for interpolation) on the same inputs, FP64, on the
@@ -601,21 +601,25 @@ def run_reference_gpu(ibk, w, info, x, f, ue, steps=3):
     torch.cuda.synchronize()
     step()
     torch.cuda.synchronize()
-    e0 = torch.cuda.Event(enable_timing=True)
-    e1 = torch.cuda.Event(enable_timing=True)
-    e0.record(default)
+    times = []
     for _ in range(steps):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(default)
         step()
-    e1.record(default)
-    torch.cuda.synchronize()
-    ms = e0.elapsed_time(e1) / steps
+        e1.record(default)
+        torch.cuda.synchronize()
+        times.append(e0.elapsed_time(e1))
+    ms = statistics.median(times)
     return {"value": n / (ms / 1000.0), "unit": "points/s", "ms_per_step": ms, "steps": steps,
+            "ms_min": min(times), "ms_max": max(times),
             "fe": fe, "ul": ul,
             "note": ("GPU restatement of the reference's algorithm, labelled as such (its own CUDA build does "
                      "not compile with nvcc 12.9): per component a sort of the points by cell key (Thrust), "
                      "a unique count with a host sync, 8 sweeps of weights, segmented sums (Thrust "
                      "reduce_by_key) and plane scatters, a combine over 8 planes; interpolation as one thread "
-                     "per point gathering 64 nodes; FP64, temporaries allocated per call as the reference does")}
+                     "per point gathering 64 nodes; FP64, temporaries allocated per call as the reference does "
+                     "(their cudaMalloc / cudaFree are inside the timed steps); median step")}
 
 
 # ------------------------------------------------ batched and serving legs
