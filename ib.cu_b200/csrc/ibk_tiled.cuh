@@ -160,15 +160,14 @@ __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& 
 	__syncthreads();
 }
 
-__device__ __forceinline__ int range_lookup(const RangeTable& rt, int item)
+// The point slot of candidate item (items number the tile's ranges back to
+// back) for a thread whose items only increase: r is the range of its
+// previous item (0 before the first) and moves forward past the ranges that
+// end at or before item (pref[count] is past every item, so the walk stops).
+__device__ __forceinline__ int range_walk(const RangeTable& rt, int& r, int item)
 {
-	int lo = 0, hi = rt.count - 1;
-	while (lo < hi) {                   // largest r with pref[r] <= item
-		int mid = (lo + hi + 1) >> 1;
-		if (rt.pref[mid] <= item) lo = mid;
-		else hi = mid - 1;
-	}
-	return rt.start[lo] + (item - rt.pref[lo]);
+	while (rt.pref[r + 1] <= item) ++r;
+	return rt.start[r] + (item - rt.pref[r]);
 }
 
 // ------------------------------------------------------------ spread ---
@@ -241,15 +240,21 @@ __device__ __forceinline__ int2 fix_terms2(float a0, float a1, float b)
 // contig: the tile spans no periodic axis whole, so the in-tile nodes of a
 // stencil are consecutive along every axis and their accumulators sit at
 // fixed offsets from the first one.
+// near: contig, and every periodic axis has more cells than M + the tile's
+// extent.  A stencil that meets the tile then does so after at most one shift
+// by the period, which places its centre within half a period of the tile's
+// centre; its in-tile nodes follow from the shifted position of node 0
+// without wrapping every node.
 template <typename D, int DIMS, int PREC>
 __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGeom& cg, int n,
                                                  const double* __restrict__ x, const double* __restrict__ fc,
                                                  int p, float scale, const int* lo, const int* hi, int S1, int S2,
-                                                 bool contig, typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
+                                                 bool contig, bool near, typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
 {
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	int loc[DIMS][M];
 	unsigned mask[DIMS];
+	int lb[DIMS];           // near: tile-local position of node 0 (may lie outside)
 	double dl[DIMS];
 	bool any = true;
 #pragma unroll
@@ -257,13 +262,28 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 		AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
 		dl[d] = a.delta;
 		unsigned mk = 0;
+		if (near) {
+			// spread drops nodes outside [0, points) (errors_negative) and this
+			// tile owns [lo, hi): node m is in it iff 0 <= l + m < hi - lo
+			int l = a.base - sh - lo[d];
+			const int e = hi[d] - lo[d];
+			if (!g.solid[d]) {
+				const int C = cg.cells[d], twice = 2 * l + M - e;
+				l += twice > C ? -C : (twice < -C ? C : 0);
+			}
+			const int m_lo = max(0, -l), m_hi = min(M, e - l);
+			mk = m_hi > m_lo ? ((1u << m_hi) - 1u) & ~((1u << m_lo) - 1u) : 0u;
+			lb[d] = l;
 #pragma unroll
-		for (int m = 0; m < M; ++m) {
-			// spread drops nodes outside [0, points) (errors_negative);
-			// this tile owns [lo, hi)
-			const int j = node_index(g, cg, d, a.base + m - sh);
-			loc[d][m] = j - lo[d];
-			mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
+			for (int m = 0; m < M; ++m) loc[d][m] = l + m;
+		} else {
+			lb[d] = 0;
+#pragma unroll
+			for (int m = 0; m < M; ++m) {
+				const int j = node_index(g, cg, d, a.base + m - sh);
+				loc[d][m] = j - lo[d];
+				mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
+			}
 		}
 		mask[d] = mk;
 		any = any && mk;
@@ -301,15 +321,16 @@ __device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGe
 		if (contig) {
 			// node (m0, m1, m2) at first + m2 * S2 + m1 * S1 + m0, where
 			// first is the (possibly outside) position of node (0, 0, 0)
-			int lb[DIMS];
+			if (!near) {
 #pragma unroll
-			for (int d = 0; d < DIMS; ++d) {
-				int v = 0;
-				bool found = false;
+				for (int d = 0; d < DIMS; ++d) {
+					int v = 0;
+					bool found = false;
 #pragma unroll
-				for (int m = 0; m < M; ++m)
-					if (!found && ((mask[d] >> m) & 1u)) { v = loc[d][m] - m; found = true; }
-				lb[d] = v;
+					for (int m = 0; m < M; ++m)
+						if (!found && ((mask[d] >> m) & 1u)) { v = loc[d][m] - m; found = true; }
+					lb[d] = v;
+				}
 			}
 			const int first = (DIMS == 3 ? lb[2] * S2 : 0) + lb[1] * S1 + lb[0];
 			int* base = acc + first;
@@ -387,13 +408,15 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, tile, tc);
 	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
-	bool contig = true;
+	bool contig = true, near = true;
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
 		lo[d] = tc[d] * tg.T[d];
 		hi[d] = min(lo[d] + tg.T[d], cg.points[d]);
 		contig = contig && (g.solid[d] || tg.ntiles[d] > 1);
+		near = near && (g.solid[d] || D::M + tg.T[d] < cg.cells[d]);
 	}
+	near = near && contig;
 	build_ranges<DIMS>(g, tg, tc, off, rt, true, binmax, c);
 	const double* __restrict__ fc = fl + (size_t) c * n;
 	const int e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = DIMS == 3 ? hi[2] - lo[2] : 1;
@@ -418,9 +441,10 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 
 	double inv_scale = 1.0;     // FP32C: back to force density (exact power of two)
 	if constexpr (PREC == IBK_PRECISION_FP64) {
+		int r = 0;
 		for (int it = threadIdx.x; it < ncand; it += NT)
-			spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, 0.0f,
-			                                lo, hi, ss.S1, ss.S2, contig, acc);
+			spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_walk(rt, r, it)) - pbase, 0.0f,
+			                                lo, hi, ss.S1, ss.S2, contig, near, acc);
 	} else {
 		// the tile's largest possible term, max|F| * max|w| * res (max|F| over
 		// its candidate bins, rounded to FP32, hence the 1.001), is scaled to
@@ -429,11 +453,12 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		int e;
 		frexpf(bound, &e);                      // bound < 2^e
 		const float scale = ldexpf(1.0f, min(kFixTermLog2 - e, 126));
+		int r = 0;              // this thread's items increase across the chunks
 		for (int base = 0; base < ncand; base += kFixChunk) {
 			const int stop = min(ncand, base + kFixChunk);
 			for (int it = base + threadIdx.x; it < stop; it += NT)
-				spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_lookup(rt, it)) - pbase, scale,
-				                                lo, hi, ss.S1, ss.S2, contig, acc);
+				spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_walk(rt, r, it)) - pbase, scale,
+				                                lo, hi, ss.S1, ss.S2, contig, near, acc);
 			// fold the working words into the exact FP64 totals
 			__syncthreads();
 			for (int i = threadIdx.x; i < TV; i += NT) {
@@ -572,6 +597,7 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 		__syncthreads();
 		if (threadIdx.x == 0) {
 			if (maps_global) tensormap_acquire(maps + c);
+			fence_proxy_async_smem();       // a persistent CTA's accesses to the previous tile's region
 			mbar_arrive_expect_tx(&bar, (unsigned) (sizeof(double) * E[0] * E[1] * E[2]));
 			if constexpr (DIMS == 3) tma_load_3d(reg, maps + c, rlo[0], rlo[1], rlo[2], &bar);
 			else tma_load_2d(reg, maps + c, rlo[0], rlo[1], &bar);

@@ -38,6 +38,14 @@ __device__ __forceinline__ void mbar_inval(uint64_t* bar)
 	asm volatile("mbarrier.inval.shared::cta.b64 [%0];" :: "r"(smem_addr(bar)) : "memory");
 }
 
+// Orders this thread's earlier generic-proxy accesses to shared memory
+// (reads of a staged box, patches, in-place rounding) before a later
+// tensor copy that overwrites the same bytes.
+__device__ __forceinline__ void fence_proxy_async_smem()
+{
+	asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+}
+
 // A tensor map in global memory written before the launch (by a copy from
 // the host) is made visible to the tensor-copy proxy before its first use.
 __device__ __forceinline__ void tensormap_acquire(const CUtensorMap* map)
