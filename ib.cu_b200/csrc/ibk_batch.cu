@@ -56,6 +56,7 @@ struct BatchHeader {
 	int total_points;       // bound points of all instances
 	int num_active;         // instances bound with points
 	int items_s, items_i;   // work items of the active instances
+	int chunks;             // binning chunks (kBinThreads points of one instance)
 };
 
 // Device views of the bound table (all in one allocation).
@@ -66,6 +67,7 @@ struct BatchTable {
 	const int* active;      // [num_active]: instances bound with points
 	const int* spre;        // [num_active + 1]: prefix of their spread items
 	const int* ipre;        // [num_active + 1]: prefix of their interpolation items
+	const int* cpre;        // [num_active + 1]: prefix of their binning chunks
 	const CUtensorMap* maps; // [count * 3]: velocity grids of the active instances
 	const int* use_tma;     // [count]: 1 when the maps are valid for TMA staging
 	int count;
@@ -101,44 +103,47 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src)
 	for (int i = threadIdx.x; i < (int) (sizeof(T) / 4); i += blockDim.x) d[i] = __ldg(s + i);
 }
 
-// Binning of every bound point of the batch (grid-stride over the bound
-// points).  spread: bin by the spread tiles (else the interpolation tiles);
-// moved: positions xn (else x); forces: 1 = fl, 2 = fs (per-bin max|F| into
+// Binning of every bound point of the batch.  The points of each active
+// instance are cut into chunks of kBinThreads (cpre: prefix of the chunk
+// counts) and each block iteration bins one chunk, so the instance is found
+// by one search per chunk and its geometry read from a shared-memory copy.
+// spread: bin by the spread tiles (else the interpolation tiles); moved:
+// positions xn (else x); forces: 1 = fl, 2 = fs (per-bin max|F| into
 // binmax), 0 = none.
 template <int M, int DIMS>
 __global__ void __launch_bounds__(kBinThreads)
 batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved, int forces,
                        int* __restrict__ counts, int2* __restrict__ key_rank, unsigned* __restrict__ binmax)
 {
-	const int total = __ldg(&t.hdr->total_points);
-	for (int base = blockIdx.x * blockDim.x; base < total; base += gridDim.x * blockDim.x) {
-		const int gp = base + threadIdx.x;
-		const bool active = gp < total;
-		// one binary search per warp (its first point), then only the lanes
-		// past an instance boundary search again, from there
-		const int lane = threadIdx.x & 31;
-		const int wfirst = base + (threadIdx.x & ~31);
-		int i0 = 0;
-		if (lane == 0 && wfirst < total) i0 = find_instance(t.pstart, t.count, wfirst);
-		i0 = __shfl_sync(0xffffffffu, i0, 0);
-		int key = 0, n = 0, p = 0;
-		const double* f = nullptr;
+	__shared__ int cur_inst, cur_chunk;
+	__shared__ BatchInst si;
+	__shared__ BatchIO so;
+	const int nchunks = __ldg(&t.hdr->chunks), nact = __ldg(&t.hdr->num_active);
+	for (int k = blockIdx.x; k < nchunks; k += gridDim.x) {
+		if (threadIdx.x == 0) {
+			const int j = find_instance(t.cpre, nact, k);
+			cur_inst = __ldg(t.active + j);
+			cur_chunk = k - __ldg(t.cpre + j);
+		}
+		__syncthreads();
+		copy_to_shared(&si, insts + cur_inst);
+		copy_to_shared(&so, t.io + cur_inst);
+		__syncthreads();
+		const int n = so.n;
+		const int p = cur_chunk * kBinThreads + threadIdx.x;
+		const bool active = p < n;
+		int key = 0;
 		unsigned fbits[kMaxDims] = {0u, 0u, 0u};
 		if (active) {
-			const int i = gp < __ldg(t.pstart + i0 + 1) ? i0 : find_instance(t.pstart, t.count, gp, i0 + 1);
-			const BatchInst& bi = insts[i];
-			const BatchIO& o = t.io[i];
-			n = o.n;
-			p = gp - o.pbase;
-			const double* x = moved ? o.xn : o.x;
-			key = spread ? bi.bin_s + bin_key<M, DIMS>(bi.g, bi.ts, x, n, p)
-			             : bi.bin_i + bin_key<M, DIMS>(bi.g, bi.ti, x, n, p);
-			f = forces == 1 ? o.fl : o.fs;
-			if (forces) force_bits<DIMS>(f, n, p, true, fbits);
+			// forces is uniform, and a bound instance with points has its force array
+			if (forces) force_bits<DIMS>(forces == 1 ? so.fl : so.fs, n, p, true, fbits);
+			const double* x = moved ? so.xn : so.x;
+			key = spread ? si.bin_s + bin_key<M, DIMS>(si.g, si.ts, x, n, p)
+			             : si.bin_i + bin_key<M, DIMS>(si.g, si.ti, x, n, p);
 		}
 		const unsigned mask = __ballot_sync(0xffffffffu, active);
-		// forces is uniform, and a bound instance with points has its force array
-		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + gp, forces ? fbits : nullptr, binmax);
+		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + so.pbase + p, forces ? fbits : nullptr, binmax);
+		__syncthreads();            // the next chunk overwrites the shared copies
 	}
 }
 
@@ -263,8 +268,8 @@ struct Batch {
 	// bindings
 	int capacity = 0;
 	std::vector<BatchIO> io_h;
-	unsigned char* d_table = nullptr; // header, io, pstart, active, spre, ipre
-	size_t table_bytes = 0, off_io = 0, off_pstart = 0, off_active = 0, off_spre = 0, off_ipre = 0;
+	unsigned char* d_table = nullptr; // header, io, pstart, active, spre, ipre, cpre
+	size_t table_bytes = 0, off_io = 0, off_pstart = 0, off_active = 0, off_spre = 0, off_ipre = 0, off_cpre = 0;
 	size_t off_maps = 0, off_tma = 0;
 	// tensor maps of the velocity grids, encoded on the host per instance and
 	// component, reused while the bound pointer and the tile shape stay
@@ -315,6 +320,7 @@ BatchTable table_view(const Batch& b)
 	t.active = reinterpret_cast<const int*>(b.d_table + b.off_active);
 	t.spre = reinterpret_cast<const int*>(b.d_table + b.off_spre);
 	t.ipre = reinterpret_cast<const int*>(b.d_table + b.off_ipre);
+	t.cpre = reinterpret_cast<const int*>(b.d_table + b.off_cpre);
 	t.maps = reinterpret_cast<const CUtensorMap*>(b.d_table + b.off_maps);
 	t.use_tma = reinterpret_cast<const int*>(b.d_table + b.off_tma);
 	t.count = b.count;
@@ -488,10 +494,11 @@ void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 	int* active = reinterpret_cast<int*>(out + b.off_active);
 	int* spre = reinterpret_cast<int*>(out + b.off_spre);
 	int* ipre = reinterpret_cast<int*>(out + b.off_ipre);
+	int* cpre = reinterpret_cast<int*>(out + b.off_cpre);
 	std::memcpy(out + b.off_io, io.data(), sizeof(BatchIO) * io.size());
 	CUtensorMap* maps = reinterpret_cast<CUtensorMap*>(out + b.off_maps);
 	int* use_tma = reinterpret_cast<int*>(out + b.off_tma);
-	int total = 0, nact = 0, ns = 0, ni = 0;
+	int total = 0, nact = 0, ns = 0, ni = 0, nc = 0;
 	for (int i = 0; i < b.count; ++i) {
 		pstart[i] = total;
 		total += io[i].n;
@@ -503,6 +510,8 @@ void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 		active[nact] = i;
 		spre[nact] = ns;
 		ipre[nact] = ni;
+		cpre[nact] = nc;
+		nc += (io[i].n + kBinThreads - 1) / kBinThreads;
 		ns += b.nitem_s[i];
 		ni += b.nitem_i[i];
 		++nact;
@@ -510,10 +519,12 @@ void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 	pstart[b.count] = total;
 	spre[nact] = ns;
 	ipre[nact] = ni;
+	cpre[nact] = nc;
 	h->total_points = total;
 	h->num_active = nact;
 	h->items_s = ns;
 	h->items_i = ni;
+	h->chunks = nc;
 }
 
 // Tiles, bins, work items and shared-memory sizes of a configuration.
@@ -687,7 +698,8 @@ ibk_status ibk_batch_create(int count, const ibk_instance_desc* instances, ibk_d
 	b->off_active = al(b->off_pstart + sizeof(int) * ((size_t) count + 1));
 	b->off_spre = al(b->off_active + sizeof(int) * (size_t) count);
 	b->off_ipre = al(b->off_spre + sizeof(int) * ((size_t) count + 1));
-	b->off_maps = al(b->off_ipre + sizeof(int) * ((size_t) count + 1));
+	b->off_cpre = al(b->off_ipre + sizeof(int) * ((size_t) count + 1));
+	b->off_maps = al(b->off_cpre + sizeof(int) * ((size_t) count + 1));
 	b->off_tma = al(b->off_maps + sizeof(CUtensorMap) * kMaxDims * (size_t) count);
 	b->table_bytes = b->off_tma + sizeof(int) * (size_t) count;
 	b->map_cache.resize((size_t) count * kMaxDims);
