@@ -18,8 +18,9 @@
 // All device memory is allocated at create / configure time; a run launches
 // a fixed sequence (memsets, four binning kernels and one persistent kernel
 // per operator) whose grids depend only on the batch's capacity and
-// configuration (the binning kernels stride over the bound points), so it
-// can be captured once as a CUDA graph and replayed with new bindings.
+// configuration (the binning kernels stride over the bound points, the
+// count kernel in per-instance chunks whose number the bound table holds),
+// so it can be captured once as a CUDA graph and replayed with new bindings.
 #include <algorithm>
 #include <cstring>
 #include <new>
