@@ -283,6 +283,11 @@ def test_workload_accuracy_fp32c(ibk, oracle, cuda, name):
     ([2.0, 1.0, 1.0], [1, 0, 1], 9),    # 18 x 9 x 9: two tiles (14+4) along x
     ([1.0, 1.0, 1.0], [0, 0, 0], 33),   # 33^3: tiles 14+14+5 on every axis
     ([0.75, 0.5, 0.875], [0, 0, 0], 2), # 12 x 8 x 14: every axis a single wrapping tile
+    # periodic axes cut into two tiles where the stencil width plus the tile
+    # extent reaches the period (18 cells: 14+4, nodes wrapped one by one) and
+    # where it stays one cell below it (19 cells: 14+5, one shift per axis)
+    ([2.0, 1.0, 1.0], [0, 1, 0], 9),    # 18 x 9 x 9
+    ([1.0, 1.0, 1.0], [0, 1, 0], 19),   # 19 x 19 x 19
 ])
 def test_tile_decompositions(ibk, oracle, cuda, precision, lengths, solid, ref):
     rng = np.random.default_rng(21)
