@@ -180,7 +180,9 @@ class CpuSampler:
         O.build()
         self.O, self.w = O, w
         self.g = O.geometry(w.dims, w.lengths, w.boundaries, O.TAG_MAC, w.refinement)
-        self.threads = threads or O.max_threads()
+        # every host CPU this process may run on: torchrun sets OMP_NUM_THREADS=1
+        # per rank, which the oracle's explicit thread count overrides
+        self.threads = threads or max(len(os.sched_getaffinity(0)), O.max_threads())
         n = w.n
         xs = w.x.reshape(w.dims, n)
         fs = w.f.reshape(w.dims, n)
