@@ -64,7 +64,6 @@ struct BatchHeader {
 struct BatchTable {
 	const BatchHeader* hdr;
 	const BatchIO* io;      // [count]
-	const int* pstart;      // [count + 1]: first batch point of each instance
 	const int* active;      // [num_active]: instances bound with points
 	const int* spre;        // [num_active + 1]: prefix of their spread items
 	const int* ipre;        // [num_active + 1]: prefix of their interpolation items
@@ -79,16 +78,14 @@ namespace {
 constexpr int kBinThreads = 256;
 constexpr int kRing = 4;
 
-// The last i in [0, count) with pre[i] <= k: the instance holding batch
-// point k (pre = pstart; instances with no points have pstart[i] ==
-// pstart[i + 1]), or the active instance holding work item k (pre = spre or
-// ipre).
-__device__ __forceinline__ int find_instance(const int* __restrict__ pstart, int count, int gp, int lo = 0)
+// The last i in [0, count) with pre[i] <= k: the active instance holding
+// work item k (pre = spre or ipre) or binning chunk k (pre = cpre).
+__device__ __forceinline__ int find_instance(const int* __restrict__ pre, int count, int k)
 {
-	int hi = count - 1;
+	int lo = 0, hi = count - 1;
 	while (lo < hi) {
 		const int mid = (lo + hi + 1) >> 1;
-		if (__ldg(pstart + mid) <= gp) lo = mid;
+		if (__ldg(pre + mid) <= k) lo = mid;
 		else hi = mid - 1;
 	}
 	return lo;
@@ -269,8 +266,8 @@ struct Batch {
 	// bindings
 	int capacity = 0;
 	std::vector<BatchIO> io_h;
-	unsigned char* d_table = nullptr; // header, io, pstart, active, spre, ipre, cpre
-	size_t table_bytes = 0, off_io = 0, off_pstart = 0, off_active = 0, off_spre = 0, off_ipre = 0, off_cpre = 0;
+	unsigned char* d_table = nullptr; // header, io, active, spre, ipre, cpre
+	size_t table_bytes = 0, off_io = 0, off_active = 0, off_spre = 0, off_ipre = 0, off_cpre = 0;
 	size_t off_maps = 0, off_tma = 0;
 	// tensor maps of the velocity grids, encoded on the host per instance and
 	// component, reused while the bound pointer and the tile shape stay
@@ -317,7 +314,6 @@ BatchTable table_view(const Batch& b)
 	BatchTable t;
 	t.hdr = reinterpret_cast<const BatchHeader*>(b.d_table);
 	t.io = reinterpret_cast<const BatchIO*>(b.d_table + b.off_io);
-	t.pstart = reinterpret_cast<const int*>(b.d_table + b.off_pstart);
 	t.active = reinterpret_cast<const int*>(b.d_table + b.off_active);
 	t.spre = reinterpret_cast<const int*>(b.d_table + b.off_spre);
 	t.ipre = reinterpret_cast<const int*>(b.d_table + b.off_ipre);
@@ -485,13 +481,12 @@ bool instance_maps(Batch& b, int i, const BatchIO& o)
 	return ok;
 }
 
-// The table of a binding: header, io, pstart, active list, item prefixes and
+// The table of a binding: header, io, active list, item and chunk prefixes and
 // the active instances' tensor maps.
 void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 {
 	std::memset(out, 0, b.table_bytes);
 	BatchHeader* h = reinterpret_cast<BatchHeader*>(out);
-	int* pstart = reinterpret_cast<int*>(out + b.off_pstart);
 	int* active = reinterpret_cast<int*>(out + b.off_active);
 	int* spre = reinterpret_cast<int*>(out + b.off_spre);
 	int* ipre = reinterpret_cast<int*>(out + b.off_ipre);
@@ -501,7 +496,6 @@ void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 	int* use_tma = reinterpret_cast<int*>(out + b.off_tma);
 	int total = 0, nact = 0, ns = 0, ni = 0, nc = 0;
 	for (int i = 0; i < b.count; ++i) {
-		pstart[i] = total;
 		total += io[i].n;
 		if (io[i].n == 0) continue;
 		if (instance_maps(b, i, io[i])) {
@@ -517,7 +511,6 @@ void build_table(Batch& b, const std::vector<BatchIO>& io, unsigned char* out)
 		ni += b.nitem_i[i];
 		++nact;
 	}
-	pstart[b.count] = total;
 	spre[nact] = ns;
 	ipre[nact] = ni;
 	cpre[nact] = nc;
@@ -695,8 +688,7 @@ ibk_status ibk_batch_create(int count, const ibk_instance_desc* instances, ibk_d
 	ibk_status st = IBK_OK;
 	auto al = [](size_t v) { return (v + 255) & ~size_t(255); };
 	b->off_io = al(sizeof(BatchHeader));
-	b->off_pstart = al(b->off_io + sizeof(BatchIO) * (size_t) count);
-	b->off_active = al(b->off_pstart + sizeof(int) * ((size_t) count + 1));
+	b->off_active = al(b->off_io + sizeof(BatchIO) * (size_t) count);
 	b->off_spre = al(b->off_active + sizeof(int) * (size_t) count);
 	b->off_ipre = al(b->off_spre + sizeof(int) * ((size_t) count + 1));
 	b->off_cpre = al(b->off_ipre + sizeof(int) * ((size_t) count + 1));
