@@ -41,7 +41,7 @@ FP64, FP32C = 0, 1
 # Every symbol include/ibk.h declares (checked by the CPU test suite).
 ABI_SYMBOLS = (
     "ibk_plan_create", "ibk_plan_destroy", "ibk_plan_info", "ibk_plan_reserve", "ibk_plan_set_tiles",
-    "ibk_spread", "ibk_interpolate", "ibk_sort_keys", "ibk_force_moments", "ibk_grid_totals",
+    "ibk_spread", "ibk_interpolate", "ibk_spread_interpolate", "ibk_sort_keys", "ibk_force_moments", "ibk_grid_totals",
     "ibk_plan_set_profiling", "ibk_plan_kernel_stats", "ibk_plan_reset_stats",
     "ibk_plan_launch_count", "ibk_plan_check", "ibk_interpolate_noalloc",
     "ibk_batch_create", "ibk_batch_destroy", "ibk_batch_info", "ibk_batch_bind",
@@ -54,7 +54,7 @@ ABI_SYMBOLS = (
     "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
-OP_SPREAD, OP_INTERPOLATE, OP_STEP = 1, 2, 3
+OP_SPREAD, OP_INTERPOLATE, OP_STEP, OP_SPREAD_INTERPOLATE = 1, 2, 3, 4
 
 
 class IbkError(RuntimeError):
@@ -155,6 +155,8 @@ def lib() -> ctypes.CDLL:
         L.ibk_plan_set_tiles.restype = ctypes.c_int
         L.ibk_spread.argtypes = [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp), _vp]
         L.ibk_interpolate.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_vp), _vp, _vp]
+        L.ibk_spread_interpolate.argtypes = [_vp, ctypes.c_int, _vp, _vp, ctypes.POINTER(_vp),
+                                             ctypes.POINTER(_vp), _vp, _vp]
         L.ibk_sort_keys.argtypes = [_vp, ctypes.c_int, ctypes.c_int, _vp, _vp, _vp]
         L.ibk_force_moments.argtypes = [_vp, ctypes.c_int, _vp, _vp, _vp, _vp]
         L.ibk_force_moments.restype = ctypes.c_int
@@ -373,6 +375,11 @@ class Plan:
     def interpolate(self, n, x, ue, ul, stream=None):
         check(lib().ibk_interpolate(self._h, int(n), _ptr(x), self._comp_ptrs(ue), _ptr(ul),
                                     _stream_handle(stream)))
+
+    def spread_interpolate(self, n, x, fl, fe, ue, ul, stream=None):
+        """spread(n, x, fl, fe) and interpolate(n, x, ue, ul) with one binning of x."""
+        check(lib().ibk_spread_interpolate(self._h, int(n), _ptr(x), _ptr(fl), self._comp_ptrs(fe),
+                                           self._comp_ptrs(ue), _ptr(ul), _stream_handle(stream)))
 
     def set_profiling(self, enable: bool):
         check(lib().ibk_plan_set_profiling(self._h, 1 if enable else 0))

@@ -318,30 +318,21 @@ ibk_status ibk_plan_set_tiles(ibk_plan handle, const int* spread_tile, const int
 	if (!plan) return set_error(IBK_ERR_INVALID_ARGUMENT, "null plan");
 	const int M = plan->info.meshwidths, dims = plan->g.dims;
 	TileGeom ts = plan->spread_tiles, ti = plan->tiles;
+	// extents up to 64 cells: records keep tile-relative origins in 8 bits
 	if (spread_tile) {
 		for (int d = 0; d < dims; ++d)
-			if (spread_tile[d] < M || spread_tile[d] > 256)
-				return set_error(IBK_ERR_INVALID_ARGUMENT, "spread tile extents must lie in [M, 256]");
+			if (spread_tile[d] < M || spread_tile[d] > kMaxTileExtent)
+				return set_error(IBK_ERR_INVALID_ARGUMENT, "spread tile extents must lie in [M, 64]");
 		ts = make_tiles(plan->g, plan->tag, M, spread_tile);
-		long long tv = 1;
-		for (int d = 0; d < dims; ++d) tv *= ts.T[d];
-		const long long words = spread_strides(ts.T[0], ts.T[1], ts.T[2], dims).words;
-		const long long per_face = plan->precision == IBK_PRECISION_FP32C ? 12 : 8;
-		if (words * per_face > 200 * 1024 || tv > 4 * 8192)
+		if (spread_tile_bytes(ts, dims, plan->precision) > 200 * 1024)
 			return set_error(IBK_ERR_UNSUPPORTED, "spread tile needs more than 200 KB of shared memory");
 	}
 	if (interp_tile) {
 		for (int d = 0; d < dims; ++d)
-			if (interp_tile[d] < M || interp_tile[d] > 200)
-				return set_error(IBK_ERR_INVALID_ARGUMENT, "interpolation tile extents must lie in [M, 200]");
+			if (interp_tile[d] < M || interp_tile[d] > kMaxTileExtent)
+				return set_error(IBK_ERR_INVALID_ARGUMENT, "interpolation tile extents must lie in [M, 64]");
 		ti = make_tiles(plan->g, plan->tag, M, interp_tile);
-		long long v = 1;
-		for (int d = 0; d < dims; ++d) {
-			long long e = ti.T[d] + 1 + (M - 1) / 2 + 1 + M / 2;
-			if (d == 0) e = (e + 1) & ~1LL;
-			v *= e;
-		}
-		if (v * 8 + 128 > 200 * 1024)
+		if (interp_region_bytes(plan->g, ti, M) > 200 * 1024)
 			return set_error(IBK_ERR_UNSUPPORTED, "interpolation tile needs more than 200 KB of shared memory");
 	}
 	plan->spread_tiles = ts;
@@ -387,6 +378,24 @@ ibk_status ibk_interpolate(ibk_plan handle, int n, const double* x, const double
 	}
 	OpArgs a{&plan->g, n, x, (cudaStream_t) stream};
 	return plan->ops.interp(*plan, a, in, ul);
+}
+
+ibk_status ibk_spread_interpolate(ibk_plan handle, int n, const double* x, const double* fl,
+                                  double* const* fe, const double* const* ue, double* ul, void* stream)
+{
+	Plan* plan = reinterpret_cast<Plan*>(handle);
+	if (!plan) return set_error(IBK_ERR_INVALID_ARGUMENT, "null plan");
+	if (n <= 0) return IBK_OK;                          // novel.h:201, interpolate.h:96
+	if (!x || !fl || !fe || !ue || !ul) return set_error(IBK_ERR_INVALID_ARGUMENT, "null array");
+	CompPtrs out{};
+	ConstCompPtrs in{};
+	for (int c = 0; c < plan->g.dims; ++c) {
+		if (!fe[c] || !ue[c]) return set_error(IBK_ERR_INVALID_ARGUMENT, "null grid component");
+		out.p[c] = fe[c];
+		in.p[c] = ue[c];
+	}
+	OpArgs a{&plan->g, n, x, (cudaStream_t) stream};
+	return plan->ops.both(*plan, a, fl, out, in, ul);
 }
 
 ibk_status ibk_sort_keys(ibk_plan handle, int component, int n, const double* x, int* keys, void* stream)

@@ -5,9 +5,11 @@
 // grid by grid (include/ib/novel.h:197-227, include/ib/interpolate.h:92-115).
 // Here every instance of a batch is binned into one global bin space
 // (instance i owns bins [bin_base_i, bin_base_i + tiles_i * 3^dims)), the
-// points of all instances are numbered consecutively, and the tile kernels'
-// bodies (spread_tile / interp_tile) run inside persistent CTAs that take
-// (instance, tile, component) work items from a device counter.  The work
+// points of all instances are numbered consecutively (their records carry
+// that number), and the tile kernels' bodies (spread_tile / interp_tile) run
+// inside persistent CTAs that take work items from a device counter: FP32C
+// spread items are (instance, tile), every component at once; FP64 spread
+// and interpolation items are (instance, tile, component).  The work
 // list is that of the instances bound with points: each bind uploads the
 // list of active instances and the prefix sums of their item counts, and a
 // CTA maps item k to (instance, tile, component) by a binary search.  Per
@@ -16,7 +18,7 @@
 // the list is exhausted.
 //
 // All device memory is allocated at create / configure time; a run launches
-// a fixed sequence (memsets, four binning kernels and one persistent kernel
+// a fixed sequence (a memset, four binning kernels and one persistent kernel
 // per operator) whose grids depend only on the batch's capacity and
 // configuration (the binning kernels stride over the bound points, the
 // count kernel in per-instance chunks whose number the bound table holds),
@@ -106,12 +108,11 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src)
 // counts) and each block iteration bins one chunk, so the instance is found
 // by one search per chunk and its geometry read from a shared-memory copy.
 // spread: bin by the spread tiles (else the interpolation tiles); moved:
-// positions xn (else x); forces: 1 = fl, 2 = fs (per-bin max|F| into
-// binmax), 0 = none.
+// positions xn (else x).
 template <int M, int DIMS>
 __global__ void __launch_bounds__(kBinThreads)
-batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved, int forces,
-                       int* __restrict__ counts, int2* __restrict__ key_rank, unsigned* __restrict__ binmax)
+batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved,
+                       int* __restrict__ counts, int2* __restrict__ key_rank)
 {
 	__shared__ int cur_inst, cur_chunk;
 	__shared__ BatchInst si;
@@ -131,34 +132,54 @@ batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int sp
 		const int p = cur_chunk * kBinThreads + threadIdx.x;
 		const bool active = p < n;
 		int key = 0;
-		unsigned fbits[kMaxDims] = {0u, 0u, 0u};
 		if (active) {
-			// forces is uniform, and a bound instance with points has its force array
-			if (forces) force_bits<DIMS>(forces == 1 ? so.fl : so.fs, n, p, true, fbits);
 			const double* x = moved ? so.xn : so.x;
-			key = spread ? si.bin_s + bin_key<M, DIMS>(si.g, si.ts, x, n, p)
-			             : si.bin_i + bin_key<M, DIMS>(si.g, si.ti, x, n, p);
+			key = spread ? si.bin_s + point_bin<M, DIMS>(si.g, si.ts, x, n, p, nullptr)
+			             : si.bin_i + point_bin<M, DIMS>(si.g, si.ti, x, n, p, nullptr);
 		}
 		const unsigned mask = __ballot_sync(0xffffffffu, active);
-		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + so.pbase + p, forces ? fbits : nullptr, binmax);
+		if (active) bin_rank(mask, key, counts, key_rank + so.pbase + p);
 		__syncthreads();            // the next chunk overwrites the shared copies
 	}
 }
 
+// Records of every bound point at their sorted positions, by the same
+// chunks as the count kernel.
+template <int M, int DIMS>
 __global__ void __launch_bounds__(kBinThreads)
-batch_bin_scatter_kernel(BatchTable t, const int2* __restrict__ key_rank, const int* __restrict__ offset,
-                         int* __restrict__ perm)
+batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved,
+                         const int2* __restrict__ key_rank, const int* __restrict__ offset,
+                         PointRec* __restrict__ recs)
 {
-	const int total = __ldg(&t.hdr->total_points);
-	for (int gp = blockIdx.x * blockDim.x + threadIdx.x; gp < total; gp += gridDim.x * blockDim.x) {
-		const int2 kr = key_rank[gp];
-		perm[__ldg(offset + kr.x) + kr.y] = gp;
+	__shared__ int cur_inst, cur_chunk;
+	__shared__ BatchInst si;
+	__shared__ BatchIO so;
+	const int nchunks = __ldg(&t.hdr->chunks), nact = __ldg(&t.hdr->num_active);
+	for (int k = blockIdx.x; k < nchunks; k += gridDim.x) {
+		if (threadIdx.x == 0) {
+			const int j = find_instance(t.cpre, nact, k);
+			cur_inst = __ldg(t.active + j);
+			cur_chunk = k - __ldg(t.cpre + j);
+		}
+		__syncthreads();
+		copy_to_shared(&si, insts + cur_inst);
+		copy_to_shared(&so, t.io + cur_inst);
+		__syncthreads();
+		const int p = cur_chunk * kBinThreads + threadIdx.x;
+		if (p < so.n) {
+			const int gp = so.pbase + p;
+			const int2 kr = __ldg(key_rank + gp);
+			PointRec r;
+			point_bin<M, DIMS>(si.g, spread ? si.ts : si.ti, moved ? so.xn : so.x, so.n, p, &r);
+			r.p = gp;
+			store_rec(recs + __ldg(offset + kr.x) + kr.y, r);
+		}
+		__syncthreads();            // the next chunk overwrites the shared copies
 	}
 }
 
 // Thread 0 takes the next work item of the active instances: instance and
-// item index within it (tile * dims + component), or instance -1 when the
-// list is exhausted.
+// item index within it, or instance -1 when the list is exhausted.
 __device__ __forceinline__ void next_item(int* next, int nitems, int nact, const int* __restrict__ pre,
                                           const int* __restrict__ active, int* inst, int* local)
 {
@@ -169,12 +190,12 @@ __device__ __forceinline__ void next_item(int* next, int nitems, int nact, const
 	*local = k - __ldg(pre + j);
 }
 
-// Persistent spread over the active instances' (tile, component) items.
+// Persistent spread over the active instances' items: tiles (FP32C, every
+// component) or (tile, component) (FP64).
 template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
 batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
-                    const int* __restrict__ perm, const int* __restrict__ off,
-                    const unsigned* __restrict__ binmax, int step)
+                    const PointRec* __restrict__ recs, const int* __restrict__ off, int step)
 {
 	__shared__ int cur_inst, cur_local;
 	__shared__ BatchInst si;
@@ -191,9 +212,12 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		CompPtrs fe;
 #pragma unroll
 		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
-		spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, perm, so.pbase,
-		                           off + si.bin_s, binmax ? binmax + (size_t) si.bin_s * kMaxDims : nullptr, fe,
-		                           local / DIMS, local % DIMS);
+		if constexpr (PREC == IBK_PRECISION_FP32C)
+			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
+			                           off + si.bin_s, fe, local, -1);
+		else
+			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
+			                           off + si.bin_s, fe, local / DIMS, local % DIMS);
 		__syncthreads();
 	}
 }
@@ -203,9 +227,9 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 // allow it, else by plain loads); with step set, the serving epilogue
 // (advection + spring force) is applied.
 template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
+__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 3 : 1)
 batch_interp_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
-                    const int* __restrict__ perm, const int* __restrict__ off, int step, double dt, double k,
+                    const PointRec* __restrict__ recs, const int* __restrict__ off, int step, double dt, double k,
                     int* status)
 {
 	__shared__ int cur_inst, cur_local;
@@ -226,7 +250,7 @@ batch_interp_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		ConstCompPtrs ue;
 #pragma unroll
 		for (int c = 0; c < kMaxDims; ++c) ue.p[c] = so.ue[c];
-		const bool ok = interp_tile<D, DIMS, PREC>(si.g, si.ti, so.n, so.x, perm, so.pbase, off + si.bin_i, ue,
+		const bool ok = interp_tile<D, DIMS, PREC>(si.g, si.ti, so.n, so.x, recs, so.pbase, off + si.bin_i, ue,
 		                                           so.ul, t.maps + (size_t) inst * kMaxDims,
 		                                           __ldg(t.use_tma + inst), true, status,
 		                                           step ? &epi : nullptr, local / DIMS, local % DIMS);
@@ -279,15 +303,16 @@ struct Batch {
 	int ring_next = 0;
 	bool bound = false;
 	// scratch
-	int *d_counts = nullptr, *d_off = nullptr, *d_chunk = nullptr, *d_perm = nullptr, *d_next = nullptr;
+	int *d_counts = nullptr, *d_off = nullptr, *d_chunk = nullptr, *d_next = nullptr;
 	int* d_status = nullptr;
 	int2* d_kr = nullptr;
-	unsigned* d_binmax = nullptr;
+	PointRec* d_recs = nullptr;
 	// step parameters and graphs
 	double dt = 0.0, k = 0.0;
 	cudaStream_t cap_stream = nullptr;
-	cudaGraphExec_t exec[4] = {};
+	cudaGraphExec_t exec[5] = {};
 	long long launches = 0;
+	long long graph_kernels[5] = {};    // kernels in each captured graph
 	int num_sms = 0;
 };
 
@@ -325,26 +350,27 @@ BatchTable table_view(const Batch& b)
 }
 
 // Binning of the bound points by the spread (spread = 1) or interpolation
-// tiles, then the scan and the scatter of the batch permutation.
+// tiles, then the scan and the records in bin order.
 template <int M, int DIMS>
-ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved, int forces)
+ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved)
 {
 	const BatchTable t = table_view(b);
 	const int nbins = spread ? b.bins_s : b.bins_i;
-	if (forces) {
-		ibk_status st = cuda_check(cudaMemsetAsync(b.d_binmax, 0, sizeof(unsigned) * kMaxDims * (size_t) nbins, s),
-		                           "cudaMemsetAsync");
-		if (st != IBK_OK) return st;
-	}
-	batch_bin_count_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, forces,
-	                                                                    b.d_counts, b.d_kr,
-	                                                                    forces ? b.d_binmax : nullptr);
+	batch_bin_count_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved,
+	                                                                    b.d_counts, b.d_kr);
 	const int nchunks = (nbins + kScanChunk - 1) / kScanChunk;
 	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, nbins);
 	bin_scan_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, b.d_off, nbins, nchunks);
-	batch_bin_scatter_kernel<<<b.grid_bin, kBinThreads, 0, s>>>(t, b.d_kr, b.d_off, b.d_perm);
+	batch_bin_scatter_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, b.d_kr,
+	                                                                      b.d_off, b.d_recs);
 	b.launches += 4;
 	return check_launch("batch binning");
+}
+
+bool same_tiles(const ibk_batch_config& c)
+{
+	return c.spread_tile[0] == c.interp_tile[0] && c.spread_tile[1] == c.interp_tile[1] &&
+	       c.spread_tile[2] == c.interp_tile[2];
 }
 
 template <int KIND, int ORDER, int DIMS, int PREC>
@@ -355,21 +381,31 @@ ibk_status batch_run_impl(Batch& b, int op, cudaStream_t s)
 	ibk_status st;
 	if ((st = cuda_check(cudaMemsetAsync(b.d_next, 0, sizeof(int) * 2, s), "cudaMemsetAsync")) != IBK_OK) return st;
 	const bool step = op == IBK_OP_STEP;
-	if (op == IBK_OP_INTERPOLATE || step) {
-		if ((st = batch_bin<D::M, DIMS>(b, s, 0, 0, 0)) != IBK_OK) return st;
+	const bool both = op == IBK_OP_SPREAD_INTERPOLATE;
+	auto interp = [&]() -> ibk_status {
 		batch_interp_kernel<D, DIMS, PREC><<<b.grid_i, kTileThreads, b.smem_i, s>>>(
-			b.d_inst, t, b.d_next + 1, b.d_perm, b.d_off, step ? 1 : 0, b.dt, b.k, b.d_status);
+			b.d_inst, t, b.d_next + 1, b.d_recs, b.d_off, step ? 1 : 0, b.dt, b.k, b.d_status);
 		b.launches += 1;
-		if ((st = check_launch("batch_interp_kernel")) != IBK_OK) return st;
-	}
-	if (op == IBK_OP_SPREAD || step) {
-		const int forces = PREC == IBK_PRECISION_FP32C ? (step ? 2 : 1) : 0;
-		if ((st = batch_bin<D::M, DIMS>(b, s, 1, step ? 1 : 0, forces)) != IBK_OK) return st;
+		return check_launch("batch_interp_kernel");
+	};
+	auto spread = [&]() -> ibk_status {
 		batch_spread_kernel<D, DIMS, PREC><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
-			b.d_inst, t, b.d_next, b.d_perm, b.d_off, PREC == IBK_PRECISION_FP32C ? b.d_binmax : nullptr,
-			step ? 1 : 0);
+			b.d_inst, t, b.d_next, b.d_recs, b.d_off, step ? 1 : 0);
 		b.launches += 1;
-		if ((st = check_launch("batch_spread_kernel")) != IBK_OK) return st;
+		return check_launch("batch_spread_kernel");
+	};
+	if (op == IBK_OP_INTERPOLATE || step) {
+		if ((st = batch_bin<D::M, DIMS>(b, s, 0, 0)) != IBK_OK) return st;
+		if ((st = interp()) != IBK_OK) return st;
+	}
+	if (op == IBK_OP_SPREAD || step || both) {
+		if ((st = batch_bin<D::M, DIMS>(b, s, 1, step ? 1 : 0)) != IBK_OK) return st;
+		if ((st = spread()) != IBK_OK) return st;
+	}
+	if (both) {
+		// the spread's records serve the interpolation when the tiles agree
+		if (!same_tiles(b.config) && (st = batch_bin<D::M, DIMS>(b, s, 0, 0)) != IBK_OK) return st;
+		if ((st = interp()) != IBK_OK) return st;
 	}
 	return IBK_OK;
 }
@@ -443,36 +479,19 @@ ibk_status grow(T** ptr, size_t& cap, size_t want, const char* what)
 	return st;
 }
 
-// Halo extents of the staged interpolation region, as interp_tile lays it out.
-size_t region_bytes(int M, const TileGeom& tg, int dims)
-{
-	const int hl = 1 + ((M - 1) >> 1), hh = 1 + M / 2;
-	size_t v = 1;
-	for (int d = 0; d < dims; ++d) {
-		int e = tg.T[d] + hl + hh;
-		if (d == 0) e = (e + 1) & ~1;
-		v *= (size_t) e;
-	}
-	return sizeof(double) * v + 128;
-}
-
 // Tensor maps of instance i's velocity grids for its interpolation regions,
 // from the cache when the grid pointers are unchanged; false when any grid
 // or box breaks a TMA rule (the instance is then staged by plain loads).
 bool instance_maps(Batch& b, int i, const BatchIO& o)
 {
 	const BatchInst& bi = b.inst_h[i];
-	const int hl = 1 + ((b.M - 1) >> 1), hh = 1 + b.M / 2;
-	if ((bi.ti.T[0] & 1) || (hl & 1)) return false;     // region x origin must stay even
-	int box[3] = {1, 1, 1};
-	for (int d = 0; d < b.dims; ++d) {
-		box[d] = bi.ti.T[d] + hl + hh;
-		if (d == 0) box[d] = (box[d] + 1) & ~1;
-	}
+	if (bi.ti.T[0] & 1) return false;     // region x origins must stay even
 	bool ok = true;
 	for (int c = 0; c < b.dims; ++c) {
 		const size_t k = (size_t) i * kMaxDims + c;
 		if (b.map_ptr[k] != o.ue[c]) {
+			int lower[3], box[3];
+			interp_region(bi.g, bi.ti, b.M, c, lower, box);
 			b.map_ok[k] = o.ue[c] && grid_tensor_map(&b.map_cache[k], o.ue[c], bi.g.comp[c], b.dims, box);
 			b.map_ptr[k] = o.ue[c];
 		}
@@ -527,7 +546,7 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 	std::vector<BatchInst> inst(b.count);
 	std::vector<int> nitem_s(b.count), nitem_i(b.count);
 	long long bins_s = 0, bins_i = 0, items_s = 0, items_i = 0;
-	size_t tv_max = 1, region_max = 0;
+	size_t smem_max = 0, region_max = 0;
 	for (int i = 0; i < b.count; ++i) {
 		BatchInst& bi = inst[i];
 		bi.g = b.geo[i];
@@ -537,17 +556,16 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		bi.bin_i = (int) bins_i;
 		bins_s += bi.ts.num_bins;
 		bins_i += bi.ti.num_bins;
-		nitem_s[i] = bi.ts.num_tiles * b.dims;
+		nitem_s[i] = bi.ts.num_tiles * (b.precision == IBK_PRECISION_FP32C ? 1 : b.dims);
 		nitem_i[i] = bi.ti.num_tiles * b.dims;
 		items_s += nitem_s[i];
 		items_i += nitem_i[i];
 		if (bins_s >= (1LL << 30) || bins_i >= (1LL << 30) || items_s >= (1LL << 30) || items_i >= (1LL << 30))
 			return set_error(IBK_ERR_INVALID_ARGUMENT, "batch has too many tiles");
-		tv_max = std::max(tv_max, (size_t) spread_strides(bi.ts.T[0], bi.ts.T[1], bi.ts.T[2], b.dims).words);
-		region_max = std::max(region_max, region_bytes(b.M, bi.ti, b.dims));
+		smem_max = std::max(smem_max, spread_tile_bytes(bi.ts, b.dims, b.precision));
+		region_max = std::max(region_max, interp_region_bytes(bi.g, bi.ti, b.M));
 	}
-	const size_t per_face = b.precision == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
-	const size_t smem_s = per_face * tv_max;
+	const size_t smem_s = smem_max;
 	if (smem_s > 200 * 1024 || region_max > 200 * 1024)
 		return set_error(IBK_ERR_UNSUPPORTED, "batch tile shape needs more than 200 KB of shared memory");
 	ibk_status st;
@@ -556,15 +574,14 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		// bin arrays sized for the larger bin space (counts start zeroed and
 		// every scan leaves them zeroed)
 		void** bufs[] = {reinterpret_cast<void**>(&b.d_counts), reinterpret_cast<void**>(&b.d_off),
-		                 reinterpret_cast<void**>(&b.d_chunk), reinterpret_cast<void**>(&b.d_binmax)};
-		const size_t bytes[] = {sizeof(int) * nb, sizeof(int) * (nb + 1), sizeof(int) * (nb / kScanChunk + 2),
-		                        sizeof(unsigned) * kMaxDims * nb};
+		                 reinterpret_cast<void**>(&b.d_chunk)};
+		const size_t bytes[] = {sizeof(int) * nb, sizeof(int) * (nb + 1), sizeof(int) * (nb / kScanChunk + 2)};
 		b.bins_cap = 0;
-		for (int j = 0; j < 4; ++j) {
+		for (int j = 0; j < 3; ++j) {
 			if (*bufs[j]) cudaFree(*bufs[j]);
 			*bufs[j] = nullptr;
 		}
-		for (int j = 0; j < 4; ++j)
+		for (int j = 0; j < 3; ++j)
 			if ((st = cuda_check(cudaMalloc(bufs[j], bytes[j]), "cudaMalloc")) != IBK_OK) return st;
 		if ((st = cuda_check(cudaMemset(b.d_counts, 0, bytes[0]), "cudaMemset")) != IBK_OK) return st;
 		b.bins_cap = nb;
@@ -607,8 +624,8 @@ void destroy(Batch* b)
 		if (b->ring_ev[r]) { cudaEventSynchronize(b->ring_ev[r]); cudaEventDestroy(b->ring_ev[r]); }
 		if (b->h_ring[r]) cudaFreeHost(b->h_ring[r]);
 	}
-	void* bufs[] = {b->d_inst, b->d_table, b->d_counts, b->d_off, b->d_chunk, b->d_perm,
-	                b->d_next, b->d_status, b->d_kr, b->d_binmax};
+	void* bufs[] = {b->d_inst, b->d_table, b->d_counts, b->d_off, b->d_chunk, b->d_recs,
+	                b->d_next, b->d_status, b->d_kr};
 	for (void* p : bufs)
 		if (p) cudaFree(p);
 	if (b->cap_stream) cudaStreamDestroy(b->cap_stream);
@@ -625,10 +642,12 @@ ibk_status check_bound(const Batch& b, int op)
 		bool ok = o.x != nullptr;
 		if (op == IBK_OP_SPREAD || op == IBK_OP_STEP)
 			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe[c] != nullptr;
-		if (op == IBK_OP_SPREAD) ok = ok && o.fl != nullptr;
-		if (op == IBK_OP_INTERPOLATE || op == IBK_OP_STEP)
+		if (op == IBK_OP_SPREAD_INTERPOLATE)
+			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe[c] != nullptr;
+		if (op == IBK_OP_SPREAD || op == IBK_OP_SPREAD_INTERPOLATE) ok = ok && o.fl != nullptr;
+		if (op == IBK_OP_INTERPOLATE || op == IBK_OP_STEP || op == IBK_OP_SPREAD_INTERPOLATE)
 			for (int c = 0; c < b.dims; ++c) ok = ok && o.ue[c] != nullptr;
-		if (op == IBK_OP_INTERPOLATE) ok = ok && o.ul != nullptr;
+		if (op == IBK_OP_INTERPOLATE || op == IBK_OP_SPREAD_INTERPOLATE) ok = ok && o.ul != nullptr;
 		if (op == IBK_OP_STEP) ok = ok && o.xn && o.xref && o.fs;
 		if (!ok)
 			return set_error(IBK_ERR_INVALID_ARGUMENT,
@@ -709,7 +728,7 @@ ibk_status ibk_batch_create(int count, const ibk_instance_desc* instances, ibk_d
 	cap = 0;
 	if (st == IBK_OK) st = grow(&b->d_kr, cap, pts, "cudaMalloc");
 	cap = 0;
-	if (st == IBK_OK) st = grow(&b->d_perm, cap, pts, "cudaMalloc");
+	if (st == IBK_OK) st = grow(&b->d_recs, cap, pts, "cudaMalloc");
 	cap = 0;
 	if (st == IBK_OK) st = grow(&b->d_next, cap, 4, "cudaMalloc");
 	cap = 0;
@@ -798,12 +817,12 @@ ibk_status ibk_batch_set_step(ibk_batch handle, double dt, double k)
 ibk_status ibk_batch_run(ibk_batch handle, int op, void* stream)
 {
 	Batch* b = reinterpret_cast<Batch*>(handle);
-	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_STEP) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
+	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_SPREAD_INTERPOLATE) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
 	ibk_status st = check_bound(*b, op);
 	if (st != IBK_OK) return st;
 	cudaStream_t s = static_cast<cudaStream_t>(stream);
 	if (b->exec[op]) {
-		b->launches += (op == IBK_OP_STEP ? 10 : 5);
+		b->launches += b->graph_kernels[op];
 		return cuda_check(cudaGraphLaunch(b->exec[op], s), "cudaGraphLaunch");
 	}
 	return b->ops->run(*b, op, s);
@@ -812,13 +831,14 @@ ibk_status ibk_batch_run(ibk_batch handle, int op, void* stream)
 ibk_status ibk_batch_capture(ibk_batch handle, int op)
 {
 	Batch* b = reinterpret_cast<Batch*>(handle);
-	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_STEP) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
+	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_SPREAD_INTERPOLATE) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
 	if (b->exec[op]) { cudaGraphExecDestroy(b->exec[op]); b->exec[op] = nullptr; }
 	ibk_status st = cuda_check(cudaStreamBeginCapture(b->cap_stream, cudaStreamCaptureModeThreadLocal),
 	                           "cudaStreamBeginCapture");
 	if (st != IBK_OK) return st;
 	const long long before = b->launches;
 	ibk_status rs = b->ops->run(*b, op, b->cap_stream);
+	b->graph_kernels[op] = b->launches - before;
 	b->launches = before;
 	cudaGraph_t graph = nullptr;
 	st = cuda_check(cudaStreamEndCapture(b->cap_stream, &graph), "cudaStreamEndCapture");
@@ -834,9 +854,9 @@ ibk_status ibk_batch_configure(ibk_batch handle, const ibk_batch_config* config)
 	Batch* b = reinterpret_cast<Batch*>(handle);
 	if (!b || !config) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or config");
 	for (int d = 0; d < 3; ++d)
-		if (config->spread_tile[d] < 2 || config->interp_tile[d] < 2 || config->spread_tile[d] > 256 ||
-		    config->interp_tile[d] > 256)
-			return set_error(IBK_ERR_INVALID_ARGUMENT, "tile extents must lie in [2, 256]");
+		if (config->spread_tile[d] < 2 || config->interp_tile[d] < 2 || config->spread_tile[d] > kMaxTileExtent ||
+		    config->interp_tile[d] > kMaxTileExtent)
+			return set_error(IBK_ERR_INVALID_ARGUMENT, "tile extents must lie in [2, 64]");
 	if (config->spread_ctas_per_sm < 0 || config->interp_ctas_per_sm < 0)
 		return set_error(IBK_ERR_INVALID_ARGUMENT, "negative CTAs per SM");
 	const ibk_batch_config old = b->config;
@@ -856,7 +876,7 @@ ibk_status ibk_batch_get_config(ibk_batch handle, ibk_batch_config* config)
 ibk_status ibk_batch_tune(ibk_batch handle, int op, void* stream, ibk_batch_config* best)
 {
 	Batch* b = reinterpret_cast<Batch*>(handle);
-	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_STEP) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
+	if (!b || op < IBK_OP_SPREAD || op > IBK_OP_SPREAD_INTERPOLATE) return set_error(IBK_ERR_INVALID_ARGUMENT, "null batch or unknown op");
 	ibk_status st = check_bound(*b, op);
 	if (st != IBK_OK) return st;
 	cudaStream_t s = static_cast<cudaStream_t>(stream);

@@ -1,16 +1,25 @@
-// Binning: a counting sort of the Lagrangian points by (tile, reach class).
+// Binning: a counting sort of the Lagrangian points by (tile, reach class)
+// that leaves one 32-byte record per point in bin order.
 //
 // Tiles are boxes of T0 x T1 x T2 grid cells.  A point's home tile is the
 // tile holding its stencil origin for the components staggered by 1/2 along
 // each axis; its reach class records, per axis, whether the stencil of ANY
 // component reaches into the lower (0) or upper (2) neighbouring tile or stays
 // inside (1).  Origins are the reference's exact ones (axis_step), so the
-// classes are exact: the owner-computes spread kernel reads exactly the bins
-// whose points can touch its faces.
+// classes are exact: the owner-computes spread reads exactly the bins whose
+// points can touch its faces.
+//
+// The record holds what the tile kernels need of the point, computed once
+// with the reference's FP64 index step: per axis the exact stencil origin of
+// the half-staggered components relative to the home tile, the difference
+// to the origin along the component's own axis (MAC), the fractional
+// offsets of both rounded to FP32, and the point's index.  The tile kernels
+// read records contiguously, bin after bin, and never redo the FP64 step in
+// the FP32C form (the FP64 form redoes it for its exact weights only).
 //
 //   bin_count_kernel    key = tile * 3^dims + class; warp-aggregated rank
 //   bin_scan_kernel     exclusive scan of the bin counts (resets the counts)
-//   bin_scatter_kernel  perm[offset[key] + rank] = point
+//   bin_scatter_kernel  records[offset[key] + rank] = record of the point
 // The non-template kernels are static: each translation unit that launches
 // them carries its own copy.
 #pragma once
@@ -18,70 +27,119 @@
 
 namespace ibk {
 
-// Exact stencil-node span of every component along axis d, relative to the
-// origin `bh` of the components staggered by 1/2 along d.
-template <int M>
-struct AxisReach {
-	int home;      // clamped origin used for the home tile
-	int node_lo;   // lowest node (unwrapped, relative to the same index space)
-	int node_hi;   // highest node
+// Sorted point record.  org: byte d (d < dims) = origin of the half-staggered
+// components along axis d minus the first cell of the home tile (int8);
+// byte 3 bits 2d..2d+1 = 1 + (origin along axis d of the component staggered
+// along d) - (half-staggered origin), periodic differences folded to the
+// nearest image, in {-1, 0, 1}.  dh / dn: sweep::difference of the half-
+// staggered and own-axis components (include/ib/sweep.h:49-62), FP32.
+struct __align__(16) PointRec {
+	int org;
+	float dh[kMaxDims];
+	float dn[kMaxDims];
+	int p;                  // point index (a batch numbers all its points)
 };
+static_assert(sizeof(PointRec) == 32, "point record layout");
 
-template <int M, int DIMS>
-__device__ __forceinline__ AxisReach<M> axis_reach(const GridGeom& g, const TileGeom& tg, int d, double x)
+__device__ __forceinline__ int rec_origin(int org, int d)
 {
-	constexpr int lo_off = (M - 1) >> 1;      // offsets run -lo_off .. M - 1 - lo_off
-	constexpr int hi_off = M - 1 - lo_off;
-	const int half_comp = tg.tag_mac ? (d + 1) % DIMS : 0;
-	const int bh = axis_step<M>(g, g.comp[half_comp], d, x).base;
-	int lo = bh, hi = bh;
-	if (tg.tag_mac) {
-		int bo = axis_step<M>(g, g.comp[d], d, x).base;
-		int diff = bo - bh;
-		if (!g.solid[d]) {
-			const int c = tg.cells[d];
-			if (2 * diff > c) diff -= c;
-			else if (2 * diff < -c) diff += c;
-		}
-		lo = min(bh, bh + diff);
-		hi = max(bh, bh + diff);
-	}
-	AxisReach<M> r;
-	r.home = bh < 0 ? 0 : (bh >= tg.cells[d] ? tg.cells[d] - 1 : bh);
-	r.node_lo = lo - lo_off;
-	r.node_hi = hi + hi_off;
-	return r;
+	return (int) (signed char) ((unsigned) org >> (8 * d));
+}
+__device__ __forceinline__ int rec_own_shift(int org, int d)
+{
+	return (int) (((unsigned) org >> (24 + 2 * d)) & 3u) - 1;
 }
 
-// Bin of point p: home tile * 3^dims + reach class.
-template <int M, int DIMS>
-__device__ __forceinline__ int bin_key(const GridGeom& g, const TileGeom& tg, const double* __restrict__ x,
-                                       int n, int p)
+__device__ __forceinline__ PointRec load_rec(const PointRec* __restrict__ r)
 {
+	const int4 a = __ldg(reinterpret_cast<const int4*>(r));
+	const int4 b = __ldg(reinterpret_cast<const int4*>(r) + 1);
+	PointRec v;
+	v.org = a.x;
+	v.dh[0] = __int_as_float(a.y); v.dh[1] = __int_as_float(a.z); v.dh[2] = __int_as_float(a.w);
+	v.dn[0] = __int_as_float(b.x); v.dn[1] = __int_as_float(b.y); v.dn[2] = __int_as_float(b.z);
+	v.p = b.w;
+	return v;
+}
+
+__device__ __forceinline__ void store_rec(PointRec* r, const PointRec& v)
+{
+	int4* q = reinterpret_cast<int4*>(r);
+	q[0] = make_int4(v.org, __float_as_int(v.dh[0]), __float_as_int(v.dh[1]), __float_as_int(v.dh[2]));
+	q[1] = make_int4(__float_as_int(v.dn[0]), __float_as_int(v.dn[1]), __float_as_int(v.dn[2]), v.p);
+}
+
+// Range of the own-axis origin shift (rec_own_shift) that a grid allows for
+// component c along axis d: MAC components are shifted by 0 (periodic) or 1
+// (solid) along their own axis against 1/2 for the others, so the own origin
+// is the half one or one above it (periodic) / below it (solid); after the
+// wall clamps of the sort key the shift stays in the same range.
+__host__ __device__ inline void own_shift_range(const GridGeom& g, int tag_mac, int c, int d, int* lo, int* hi)
+{
+	*lo = 0;
+	*hi = 0;
+	if (!tag_mac || c != d) return;
+	const double so = g.comp[d].shift[d], sh = g.comp[(d + 1) % g.dims].shift[d];
+	if (so < sh) *hi = 1;
+	else if (so > sh) *lo = -1;
+}
+
+// Bin of point p (home tile * 3^dims + reach class); with rec != nullptr the
+// point's record as well (rec->p is left to the caller).
+template <int M, int DIMS>
+__device__ __forceinline__ int point_bin(const GridGeom& g, const TileGeom& tg, const double* __restrict__ x,
+                                         int n, int p, PointRec* rec)
+{
+	constexpr int sh = (M - 1) >> 1;
 	int tile = 0, cls = 0, ts = 1, cs = 1;
+	unsigned org = 0;
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
-		AxisReach<M> r = axis_reach<M, DIMS>(g, tg, d, __ldg(x + (size_t) d * n + p));
-		const int t = r.home / tg.T[d];
-		const int tlo = t * tg.T[d];
-		const int thi = min(tlo + tg.T[d], tg.cells[d]);
+		const double xd = __ldg(x + (size_t) d * n + p);
+		const int hc = tg.tag_mac ? (d + 1) % DIMS : 0;
+		const AxisStep<M> h = axis_step<M>(g, g.comp[hc], d, xd);
+		int diff = 0;
+		double dn = h.delta;
+		if (tg.tag_mac) {
+			const AxisStep<M> o = axis_step<M>(g, g.comp[d], d, xd);
+			diff = o.base - h.base;
+			if (!g.solid[d]) {
+				const int c = tg.cells[d];
+				if (2 * diff > c) diff -= c;
+				else if (2 * diff < -c) diff += c;
+			}
+			dn = o.delta;
+		}
+		const int home = h.base < 0 ? 0 : (h.base >= tg.cells[d] ? tg.cells[d] - 1 : h.base);
+		const int t = home / tg.T[d];
+		const int lo = t * tg.T[d];
+		const int thi = min(lo + tg.T[d], tg.cells[d]);
+		const int node_lo = min(h.base, h.base + diff) - sh;
+		const int node_hi = max(h.base, h.base + diff) + (M - 1 - sh);
 		int c = 1;
-		if (tg.ntiles[d] > 1) c = r.node_lo < tlo ? 0 : (r.node_hi >= thi ? 2 : 1);
+		if (tg.ntiles[d] > 1) c = node_lo < lo ? 0 : (node_hi >= thi ? 2 : 1);
 		tile += t * ts;
 		ts *= tg.ntiles[d];
 		cls += c * cs;
 		cs *= 3;
+		if (rec) {
+			org |= ((unsigned) (h.base - lo) & 0xffu) << (8 * d);
+			org |= (unsigned) (diff + 1) << (24 + 2 * d);
+			rec->dh[d] = (float) h.delta;
+			rec->dn[d] = (float) dn;
+		}
+	}
+	if (rec) {
+		rec->org = (int) org;
+#pragma unroll
+		for (int d = DIMS; d < kMaxDims; ++d) { rec->dh[d] = 0.0f; rec->dn[d] = 0.0f; }
 	}
 	return tile * tg.nclass + cls;
 }
 
-// Warp-aggregated rank of a point in its bin (one atomic per group of lanes
-// sharing a key); with fbits != nullptr also raises binmax[key * 3 + c] to
-// the group's largest FP32 |F| bit pattern.  Every lane of `mask` must call
-// it, all with fbits null or all with fbits set.
-template <int DIMS>
-__device__ __forceinline__ void bin_rank(unsigned mask, int key, int* __restrict__ count, int2* __restrict__ kr_out,
-                                         const unsigned* fbits, unsigned* __restrict__ binmax)
+// Warp-aggregated rank of a point in its bin: one atomic per group of lanes
+// sharing a key.  Every lane of `mask` must call it.
+__device__ __forceinline__ void bin_rank(unsigned mask, int key, int* __restrict__ count, int2* __restrict__ kr_out)
 {
 	const int lane = threadIdx.x & 31;
 	const unsigned peers = __match_any_sync(mask, key);
@@ -90,42 +148,19 @@ __device__ __forceinline__ void bin_rank(unsigned mask, int key, int* __restrict
 	if (lane == leader) base = atomicAdd(count + key, __popc(peers));
 	base = __shfl_sync(peers, base, leader);
 	*kr_out = make_int2(key, base + __popc(peers & ((1u << lane) - 1u)));
-	if (fbits != nullptr) {
-#pragma unroll
-		for (int c = 0; c < DIMS; ++c) {
-			const unsigned m = __reduce_max_sync(peers, fbits[c]);
-			if (lane == leader && m != 0u) atomicMax(binmax + (size_t) key * kMaxDims + c, m);
-		}
-	}
 }
 
-// FP32 |f[c * n + p]| bit patterns of one point (0 past the end).
-template <int DIMS>
-__device__ __forceinline__ void force_bits(const double* __restrict__ f, int n, int p, bool active, unsigned* fbits)
-{
-#pragma unroll
-	for (int c = 0; c < DIMS; ++c)
-		fbits[c] = active ? __float_as_uint(fabsf((float) __ldg(f + (size_t) c * n + p))) : 0u;
-}
-
-// With f != nullptr (spread) the kernel also raises binmax[key * 3 + c] to
-// the FP32 |F| of every point of the bin, per component; binmax starts at
-// zero and, as all values are non-negative floats, compares as unsigned bit
-// patterns.  The maximum does not depend on the order of the atomics.
 template <int M, int DIMS>
 __global__ void __launch_bounds__(256)
 bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                 int* __restrict__ count, int2* __restrict__ key_rank,
-                 const double* __restrict__ f, unsigned* __restrict__ binmax)
+                 int* __restrict__ count, int2* __restrict__ key_rank)
 {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	const bool active = p < n;
-	unsigned fbits[kMaxDims] = {0u, 0u, 0u};
-	if (f != nullptr) force_bits<DIMS>(f, n, p, active, fbits);   // loads in flight with x's
-	const int key = active ? bin_key<M, DIMS>(g, tg, x, n, p) : 0;
+	const int key = active ? point_bin<M, DIMS>(g, tg, x, n, p, nullptr) : 0;
 	const unsigned mask = __ballot_sync(0xffffffffu, active);
 	if (!active) return;
-	bin_rank<DIMS>(mask, key, count, key_rank + p, f != nullptr ? fbits : nullptr, binmax);
+	bin_rank(mask, key, count, key_rank + p);
 }
 
 // Exclusive scan of the bin counts in two launches.  Each CTA owns a chunk
@@ -214,14 +249,22 @@ bin_scan_kernel(int* __restrict__ count, const int* __restrict__ chunk, int* __r
 	if (blockIdx.x == nchunks - 1 && threadIdx.x == kScanThreads - 1) offset[num_bins] = run;
 }
 
-static __global__ void __launch_bounds__(256)
-bin_scatter_kernel(int n, const int2* __restrict__ key_rank, const int* __restrict__ offset,
-                   int* __restrict__ perm)
+// The record of every point at its sorted position (the FP64 index step is
+// recomputed here rather than stored by the count kernel: it costs less
+// than writing and re-reading the records in input order).
+template <int M, int DIMS>
+__global__ void __launch_bounds__(256)
+bin_scatter_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                   const int2* __restrict__ key_rank, const int* __restrict__ offset,
+                   PointRec* __restrict__ recs)
 {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= n) return;
-	const int2 kr = key_rank[p];
-	perm[__ldg(offset + kr.x) + kr.y] = p;
+	const int2 kr = __ldg(key_rank + p);
+	PointRec r;
+	point_bin<M, DIMS>(g, tg, x, n, p, &r);
+	r.p = p;
+	store_rec(recs + __ldg(offset + kr.x) + kr.y, r);
 }
 
 } // namespace ibk

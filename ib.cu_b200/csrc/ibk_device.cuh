@@ -62,6 +62,7 @@ __host__ __device__ inline SpreadStrides spread_strides(int T0, int T1, int T2, 
 	st.S2 = st.S1 * T1;
 	st.S2 += (24 - st.S2 % 32 + 32) % 32;
 	st.words = dims == 3 ? st.S2 * T2 : st.S1 * T1;
+	st.words = (st.words + 3) & ~3;    // 16-byte multiples (vector zeroing)
 	return st;
 }
 

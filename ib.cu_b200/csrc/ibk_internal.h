@@ -23,11 +23,13 @@ struct Plan;
 using SpreadFn = ibk_status (*)(Plan&, const OpArgs&, const double* fl, CompPtrs fe);
 using InterpFn = ibk_status (*)(Plan&, const OpArgs&, ConstCompPtrs ue, double* ul);
 using KeysFn = ibk_status (*)(Plan&, const OpArgs&, int comp, int* keys);
+using BothFn = ibk_status (*)(Plan&, const OpArgs&, const double* fl, CompPtrs fe, ConstCompPtrs ue, double* ul);
 
 struct OpTable {
 	SpreadFn spread;
 	InterpFn interp;
 	KeysFn keys;
+	BothFn both;             // spread and interpolation at the same positions
 };
 
 // Device scratch owned by a plan: grown on demand outside stream capture,
@@ -45,7 +47,8 @@ struct TimedLaunch {
 struct Plan {
 	GridGeom g{};
 	TileGeom tiles{};          // interpolation tiles (halo staged in shared memory)
-	TileGeom spread_tiles{};   // spread tiles (owner-computes accumulators)
+	TileGeom spread_tiles{};   // spread tiles (owner-computes accumulators); the
+	                           // same as `tiles` unless set apart, so one binning serves both
 	bool tiled = true;         // false: an axis has fewer cells than the stencil width
 	ibk_grid_info info{};
 	int delta_kind = 0, delta_order = 0, precision = 0, tag = 0;
@@ -77,7 +80,19 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 }
 
 // Scratch slots of a plan.
-enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotPerm = 3, kSlotChunk = 4, kSlotBinMax = 5, kSlotSums = 6 };
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotRecs = 3, kSlotChunk = 4, kSlotSums = 6 };
+
+// Largest tile extent in cells per axis (point records keep tile-relative
+// origins in 8 bits).
+constexpr int kMaxTileExtent = 64;
+
+// Shared memory of a spread CTA for tiles tg, and of an interpolation CTA's
+// staged region (largest component, stencil width M), in bytes.
+size_t spread_tile_bytes(const TileGeom& tg, int dims, int precision);
+size_t interp_region_bytes(const GridGeom& g, const TileGeom& tg, int M);
+// Staged interpolation region of component c relative to a tile's first
+// cell: lower corner and extent per axis (the TMA box).
+void interp_region(const GridGeom& g, const TileGeom& tg, int M, int c, int* lower, int* extent);
 
 // Tile decomposition of a plan's grid for stencil width M.
 // pref_extent: preferred tile extent per axis (nullptr: 16 cells).

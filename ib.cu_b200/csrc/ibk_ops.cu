@@ -37,39 +37,30 @@ ibk_status interp_direct(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* 
 	});
 }
 
-// Counting sort of the points by (tile, reach class): perm + bin offsets.
+// Counting sort of the points by (tile, reach class): records in bin order
+// and the bin offsets.
 template <int M, int DIMS>
-ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, int** perm_out, int** off_out,
-                      const double* f = nullptr, unsigned** binmax_out = nullptr)
+ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, const PointRec** recs_out,
+                      const int** off_out)
 {
 	ibk_status s;
 	const int need = a.n > plan.reserved_points ? a.n : plan.reserved_points;
 	if ((s = ensure_scratch(plan, kSlotCount, sizeof(int) * (size_t) tg.num_bins, a.stream, true)) != IBK_OK) return s;
 	if ((s = ensure_scratch(plan, kSlotOffset, sizeof(int) * ((size_t) tg.num_bins + 1), a.stream)) != IBK_OK) return s;
 	if ((s = ensure_scratch(plan, kSlotKeyRank, sizeof(int2) * (size_t) need, a.stream)) != IBK_OK) return s;
-	if ((s = ensure_scratch(plan, kSlotPerm, sizeof(int) * (size_t) need, a.stream)) != IBK_OK) return s;
+	if ((s = ensure_scratch(plan, kSlotRecs, sizeof(PointRec) * (size_t) need, a.stream)) != IBK_OK) return s;
+	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
+	if ((s = ensure_scratch(plan, kSlotChunk, sizeof(int) * ((size_t) nchunks + 1), a.stream)) != IBK_OK) return s;
 	int* count = static_cast<int*>(plan.scratch[kSlotCount].ptr);
 	int* off = static_cast<int*>(plan.scratch[kSlotOffset].ptr);
 	int2* kr = static_cast<int2*>(plan.scratch[kSlotKeyRank].ptr);
-	int* perm = static_cast<int*>(plan.scratch[kSlotPerm].ptr);
+	PointRec* recs = static_cast<PointRec*>(plan.scratch[kSlotRecs].ptr);
+	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
 	const GridGeom& g = *a.g;
 	const int nb = blocks_for(a.n, 256);
-	unsigned* binmax = nullptr;
-	if (f) {
-		// per-bin, per-component max|F| (FP32 bit patterns), zeroed each call
-		const size_t bytes = sizeof(unsigned) * kMaxDims * (size_t) tg.num_bins;
-		if ((s = ensure_scratch(plan, kSlotBinMax, bytes, a.stream)) != IBK_OK) return s;
-		binmax = static_cast<unsigned*>(plan.scratch[kSlotBinMax].ptr);
-		cudaError_t e = cudaMemsetAsync(binmax, 0, bytes, a.stream);
-		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
-		*binmax_out = binmax;
-	}
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
-		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, f, binmax);
+		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr);
 	})) != IBK_OK) return s;
-	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
-	if ((s = ensure_scratch(plan, kSlotChunk, sizeof(int) * ((size_t) nchunks + 1), a.stream)) != IBK_OK) return s;
-	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
 	if ((s = launch(plan, "bin_chunk_sum_kernel", a.stream, [&] {
 		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins);
 	})) != IBK_OK) return s;
@@ -77,9 +68,9 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, int** per
 		bin_scan_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, off, tg.num_bins, nchunks);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scatter_kernel", a.stream, [&] {
-		bin_scatter_kernel<<<nb, 256, 0, a.stream>>>(a.n, kr, off, perm);
+		bin_scatter_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, kr, off, recs);
 	})) != IBK_OK) return s;
-	*perm_out = perm;
+	*recs_out = recs;
 	*off_out = off;
 	return IBK_OK;
 }
@@ -94,33 +85,31 @@ ibk_status set_smem(K kernel, size_t bytes)
 	return IBK_OK;
 }
 
+template <typename D, int DIMS, int PREC>
+ibk_status launch_spread(Plan& plan, const OpArgs& a, const TileGeom& tg, const PointRec* recs, const int* off,
+                         const double* fl, CompPtrs fe)
+{
+	const size_t smem = spread_smem_bytes(tg, DIMS, PREC);
+	auto kern = spread_tile_kernel<D, DIMS, PREC>;
+	ibk_status s = set_smem(kern, smem);
+	if (s != IBK_OK) return s;
+	// FP32C: one CTA per tile for every component; FP64: per (tile, component)
+	const dim3 grid(tg.num_tiles, PREC == IBK_PRECISION_FP32C ? 1 : DIMS);
+	return launch(plan, "spread_tile_kernel", a.stream, [&] {
+		kern<<<grid, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, fe);
+	});
+}
+
 template <int KIND, int ORDER, int DIMS, int PREC>
 ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs fe)
 {
 	using D = Delta<KIND, ORDER>;
-	const GridGeom& g = *a.g;
-	const TileGeom& tg = plan.spread_tiles;
 	if (!plan.tiled) return spread_direct<D, DIMS>(plan, a, fl, fe);
-	int *perm = nullptr, *off = nullptr;
-	unsigned* binmax = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off,
-	                                      PREC == IBK_PRECISION_FP32C ? fl : nullptr, &binmax);
+	const PointRec* recs = nullptr;
+	const int* off = nullptr;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off);
 	if (s != IBK_OK) return s;
-	// FP64: one double per face; FP32C: an FP64 total and a 32-bit working word
-	const size_t per_face = PREC == IBK_PRECISION_FP32C ? sizeof(double) + sizeof(int) : sizeof(double);
-	const size_t smem = per_face * (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], DIMS).words;
-	// threads per CTA: 256 per 4096 faces of the tile (FP32C), 256 (FP64)
-	const int tv = tg.T[0] * tg.T[1] * (DIMS == 3 ? tg.T[2] : 1);
-	int nt = 256;
-	auto kern = spread_tile_kernel<D, DIMS, PREC, 256>;
-	if constexpr (PREC == IBK_PRECISION_FP32C) {
-		if (tv > 8192) { nt = 1024; kern = spread_tile_kernel<D, DIMS, PREC, 1024>; }
-		else if (tv > 4096) { nt = 512; kern = spread_tile_kernel<D, DIMS, PREC, 512>; }
-	}
-	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
-	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<dim3(tg.num_tiles, DIMS), nt, smem, a.stream>>>(g, tg, a.n, a.x, fl, perm, off, binmax, fe);
-	});
+	return launch_spread<D, DIMS, PREC>(plan, a, plan.spread_tiles, recs, off, fl, fe);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -174,35 +163,66 @@ bool grid_tensor_map(CUtensorMap* map, const double* base, const CompGeom& cg, i
 
 namespace {
 
+template <typename D, int DIMS, int PREC>
+ibk_status launch_interp(Plan& plan, const OpArgs& a, const TileGeom& tg, const PointRec* recs, const int* off,
+                         ConstCompPtrs ue, double* ul)
+{
+	const GridGeom& g = *a.g;
+	const size_t smem = interp_smem_bytes<D::M>(g, tg);
+	// TMA needs every region's x origin on a 16-byte boundary: even tile
+	// extents along x (the region's lower x offset is even by construction)
+	TmaMaps maps{};
+	int use_tma = tg.T[0] % 2 == 0;
+	for (int c = 0; c < DIMS && use_tma; ++c) {
+		int lower[3], box[3];
+		region_of<D::M>(g, tg, c, lower, box);
+		use_tma = grid_tensor_map(&maps.map[c], ue.p[c], g.comp[c], DIMS, box);
+	}
+	auto kern = interp_tile_kernel<D, DIMS, PREC>;
+	ibk_status s = set_smem(kern, smem);
+	if (s != IBK_OK) return s;
+	return launch(plan, "interp_tile_kernel", a.stream, [&] {
+		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, recs, off, ue, ul,
+		                                                                   maps, use_tma, plan.d_status);
+	});
+}
+
 template <int KIND, int ORDER, int DIMS, int PREC>
 ibk_status interp_impl(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* ul)
 {
 	using D = Delta<KIND, ORDER>;
-	const GridGeom& g = *a.g;
-	const TileGeom& tg = plan.tiles;
 	if (!plan.tiled) return interp_direct<D, DIMS>(plan, a, ue, ul);
-	int *perm = nullptr, *off = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, tg, &perm, &off);
+	const PointRec* recs = nullptr;
+	const int* off = nullptr;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.tiles, &recs, &off);
 	if (s != IBK_OK) return s;
-	constexpr int HL = Halo<D::M>::lo;
-	int box[3] = {1, 1, 1};
-	size_t ev = 1;
-	for (int d = 0; d < DIMS; ++d) {
-		box[d] = region_extent<D::M>(tg.T[d], d);
-		ev *= (size_t) box[d];
+	return launch_interp<D, DIMS, PREC>(plan, a, plan.tiles, recs, off, ue, ul);
+}
+
+bool same_tiles(const TileGeom& a, const TileGeom& b)
+{
+	return a.T[0] == b.T[0] && a.T[1] == b.T[1] && a.T[2] == b.T[2];
+}
+
+// Spread and interpolation at the same positions: one binning serves both
+// when the plan's spread and interpolation tiles agree.
+template <int KIND, int ORDER, int DIMS, int PREC>
+ibk_status both_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs fe, ConstCompPtrs ue, double* ul)
+{
+	using D = Delta<KIND, ORDER>;
+	if (!plan.tiled) {
+		ibk_status s = spread_direct<D, DIMS>(plan, a, fl, fe);
+		return s != IBK_OK ? s : interp_direct<D, DIMS>(plan, a, ue, ul);
 	}
-	const size_t smem = sizeof(double) * ev + 128;   // + slack for 128-byte alignment
-	// TMA needs every region's x origin (tile origin - halo) on a 16-byte boundary
-	TmaMaps maps{};
-	int use_tma = (tg.T[0] % 2 == 0) && (HL % 2 == 0);
-	for (int c = 0; c < DIMS && use_tma; ++c)
-		use_tma = grid_tensor_map(&maps.map[c], ue.p[c], g.comp[c], DIMS, box);
-	auto kern = interp_tile_kernel<D, DIMS, PREC>;
-	if ((s = set_smem(kern, smem)) != IBK_OK) return s;
-	return launch(plan, "interp_tile_kernel", a.stream, [&] {
-		kern<<<dim3(tg.num_tiles, DIMS), kTileThreads, smem, a.stream>>>(g, tg, a.n, a.x, perm, off, ue, ul,
-		                                                                   maps, use_tma, plan.d_status);
-	});
+	const PointRec* recs = nullptr;
+	const int* off = nullptr;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off);
+	if (s != IBK_OK) return s;
+	if ((s = launch_spread<D, DIMS, PREC>(plan, a, plan.spread_tiles, recs, off, fl, fe)) != IBK_OK) return s;
+	if (!same_tiles(plan.spread_tiles, plan.tiles)) {
+		if ((s = bin_points<D::M, DIMS>(plan, a, plan.tiles, &recs, &off)) != IBK_OK) return s;
+	}
+	return launch_interp<D, DIMS, PREC>(plan, a, plan.tiles, recs, off, ue, ul);
 }
 
 template <int KIND, int ORDER, int DIMS>
@@ -218,7 +238,7 @@ template <int KIND, int ORDER, int DIMS, int PREC>
 constexpr OpTable make_table()
 {
 	return OpTable{&spread_impl<KIND, ORDER, DIMS, PREC>, &interp_impl<KIND, ORDER, DIMS, PREC>,
-	               &keys_impl<KIND, ORDER, DIMS>};
+	               &keys_impl<KIND, ORDER, DIMS>, &both_impl<KIND, ORDER, DIMS, PREC>};
 }
 
 struct Entry { int kind, order, dims, prec; OpTable ops; };
@@ -283,6 +303,34 @@ TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
 	tg.nclass = ipow3(g.dims);
 	tg.num_bins = tg.num_tiles * tg.nclass;
 	return tg;
+}
+
+size_t spread_tile_bytes(const TileGeom& tg, int dims, int precision)
+{
+	return spread_smem_bytes(tg, dims, precision);
+}
+
+void interp_region(const GridGeom& g, const TileGeom& tg, int M, int c, int* lower, int* extent)
+{
+	switch (M) {
+	case 2: region_of<2>(g, tg, c, lower, extent); return;
+	case 3: region_of<3>(g, tg, c, lower, extent); return;
+	case 4: region_of<4>(g, tg, c, lower, extent); return;
+	case 5: region_of<5>(g, tg, c, lower, extent); return;
+	case 6: region_of<6>(g, tg, c, lower, extent); return;
+	}
+}
+
+size_t interp_region_bytes(const GridGeom& g, const TileGeom& tg, int M)
+{
+	switch (M) {
+	case 2: return interp_smem_bytes<2>(g, tg);
+	case 3: return interp_smem_bytes<3>(g, tg);
+	case 4: return interp_smem_bytes<4>(g, tg);
+	case 5: return interp_smem_bytes<5>(g, tg);
+	case 6: return interp_smem_bytes<6>(g, tg);
+	}
+	return 0;
 }
 
 const OpTable* find_ops(int kind, int order, int dims, int precision)

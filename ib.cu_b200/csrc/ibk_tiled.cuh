@@ -1,29 +1,32 @@
 // Tiled kernels: the throughput path of spread and interpolate.
 //
-// Points are binned by (home tile, reach class) (ibk_bin.cuh).  One CTA owns
-// one tile of T0 x T1 x T2 grid cells for every MAC component.
+// Points are binned by (home tile, reach class) into 32-byte records in bin
+// order (ibk_bin.cuh).  A tile is a box of T0 x T1 x T2 grid cells.
 //
-// spread_tile_kernel  -- owner computes.  The CTA visits every point whose
-//   stencil can touch its tile (its own bins plus the neighbours' bins whose
-//   reach class points at it), accumulates the in-tile contributions in shared
+// spread_tile  -- owner computes.  The CTA visits every point whose stencil
+//   can touch its tile (its own bins plus the neighbours' bins whose reach
+//   class points at it), accumulates the in-tile contributions in shared
 //   memory, and writes every face of its tile exactly once (zeros included).
 //   No global atomics, no zero-fill pass: each face is written by one CTA.
-//     FP64:  FP64 shared-memory accumulation.
-//     FP32C: FP32 weights and products, each quantised to fixed point and
-//            summed exactly (32-bit integer shared atomics folded into FP64
-//            totals; order-independent).  See fix_add below.
+//     FP32C: one CTA per tile for every component.  FP32 weights and
+//            products, each rounded once to a per-(tile, component) fixed
+//            point and summed exactly with 32-bit integer shared atomics
+//            (order-independent; see the fixed-point notes below).
+//     FP64:  one CTA per (tile, component), FP64 shared-memory accumulation,
+//            the reference's exact weights.
 //
-// interp_tile_kernel  -- one CTA per (tile, component) stages the tile plus
-//   its stencil halo in shared memory with one TMA bulk tensor copy; at a
-//   domain edge the out-of-range slabs are then patched with loads that wrap
-//   periodic halos and clamp wall halos exactly as the reference clamps node
-//   indices.  Every point of the tile then gathers its M^dims nodes from
-//   shared memory.
+// interp_tile  -- one CTA per (tile, component) stages the tile plus the
+//   stencil halo of that component in shared memory with one TMA bulk tensor
+//   copy; at a domain edge the out-of-range slabs are then patched with loads
+//   that wrap periodic halos and clamp wall halos exactly as the reference
+//   clamps node indices.  Every point of the tile then gathers its M^dims
+//   nodes from shared memory.
 //     FP64:  exact weights, sums in the reference's pattern order (bit-exact).
 //     FP32C: the staged values rounded to FP32 in shared memory (half the
 //            shared-memory traffic of the gathers), FP32 weights, FP32 row
 //            sums of M products, FP64 sum of the rows.
 #pragma once
+#include <algorithm>
 #include "ibk_device.cuh"
 #include "ibk_bin.cuh"
 #include "ibk_tma.cuh"
@@ -31,12 +34,6 @@
 namespace ibk {
 
 constexpr int kTileThreads = 256;
-
-// Tile-local description of one dimension for one component.
-struct TileAxis {
-	int lo;      // first face index of the tile
-	int hi;      // one past the last face owned by the tile (clipped to points)
-};
 
 __device__ __forceinline__ void tile_coords(const TileGeom& tg, int t, int* tc)
 {
@@ -75,92 +72,113 @@ __host__ __device__ constexpr float max_weight()
 	return (D::M == 4 && !D::every_other) ? (DIMS == 3 ? 8.0f / 27.0f : 4.0f / 9.0f) : 1.0f;
 }
 
+// Axis d of a packed per-axis int8 triple.
+__device__ __forceinline__ int unpack8(int v, int d) { return (int) (signed char) ((unsigned) v >> (8 * d)); }
+
 // ------------------------------------------------------------ ranges ---
-// The bins a tile must visit: per axis five (neighbour offset, class)
-// choices: (-1, upper), (0, lower), (0, inside), (0, upper), (+1, lower).
-constexpr int kMaxRanges = 125;
+// The bins a spread tile must visit.  Per axis five (neighbour offset,
+// class) choices: (-1, upper), (0, lower), (0, inside), (0, upper),
+// (+1, lower); the 3^dims choices with offset 0 on every axis are the tile's
+// own bins, one contiguous range.  Non-empty ranges are compacted; each
+// keeps the offset from this tile's first cell to its home tile's first cell
+// (unwrapped across periodic boundaries) so a record's home-relative origin
+// becomes a tile-local one by one addition.
+constexpr int kMaxRanges = 128;
 
 struct RangeTable {
 	int start[kMaxRanges];
 	int pref[kMaxRanges + 1];
+	int shift[kMaxRanges];  // per axis int8: home tile's first cell - this tile's first cell
 	int count;
-	unsigned fmax_bits;     // spread: max over the candidate bins of binmax[bin][comp]
 };
 
 template <int DIMS>
 __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& tg, const int* tc,
-                                             const int* __restrict__ off, RangeTable& rt, bool neighbours,
-                                             const unsigned* __restrict__ binmax = nullptr, int comp = 0)
+                                             const int* __restrict__ off, RangeTable& rt)
 {
-	const int nent = neighbours ? (DIMS == 3 ? 125 : 25) : 1;
+	constexpr int nent = DIMS == 3 ? 125 : 25;
 	const int tid = threadIdx.x;
 	int len = 0, st = 0;
-	unsigned fm = 0;
+	unsigned sft = 0;
 	if (tid < nent) {
 		int tile = 0, cls = 0, ts = 1, cs = 1;
-		bool ok = true;
+		bool ok = true, home = true, first_home = true;
 		int e = tid;
+#pragma unroll
 		for (int d = 0; d < DIMS; ++d) {
-			int k = neighbours ? e % 5 : 1;
+			const int k = e % 5;
 			e /= 5;
-			int o = k == 0 ? -1 : (k == 4 ? 1 : 0);
-			int c = k == 0 ? 2 : (k == 4 ? 0 : k - 1);
-			int nt = tg.ntiles[d];
+			const int o = k == 0 ? -1 : (k == 4 ? 1 : 0);
+			const int c = k == 0 ? 2 : (k == 4 ? 0 : k - 1);
+			home = home && o == 0;
+			first_home = first_home && k == 1;
+			const int nt = tg.ntiles[d];
 			int t = tc[d] + o;
+			int lo_home = t * tg.T[d];
 			if (o != 0) {
 				if (nt == 1) ok = false;
 				else if (g.solid[d]) ok = ok && t >= 0 && t < nt;
-				else t = (t + nt) % nt;
+				else if (t < 0) { t = nt - 1; lo_home = t * tg.T[d] - tg.cells[d]; }
+				else if (t >= nt) { t = 0; lo_home = tg.cells[d]; }
 			}
+			sft |= ((unsigned) (lo_home - tc[d] * tg.T[d]) & 0xffu) << (8 * d);
 			tile += t * ts;
 			ts *= nt;
 			cls += c * cs;
 			cs *= 3;
 		}
-		if (!neighbours) {
-			// the tile's own points: all classes, one contiguous range
-			st = off[tile * tg.nclass];
-			len = off[tile * tg.nclass + tg.nclass] - st;
+		if (home) {
+			if (first_home) {
+				st = __ldg(off + tile * tg.nclass);
+				len = __ldg(off + (tile + 1) * tg.nclass) - st;
+			}
 		} else if (ok) {
 			const int bin = tile * tg.nclass + cls;
-			st = off[bin];
-			len = off[bin + 1] - st;
-			if (binmax != nullptr && len > 0) fm = binmax[(size_t) bin * kMaxDims + comp];
+			st = __ldg(off + bin);
+			len = __ldg(off + bin + 1) - st;
 		}
-		rt.start[tid] = st;
 	}
-	// block-wide exclusive scan of len over the first 128 threads
-	__shared__ int warp_tot[4];
-	__shared__ unsigned warp_fm[4];
+	// compaction: slot = number of non-empty entries before this one, pref =
+	// exclusive sum of the lengths (the first 128 threads, 4 warps)
+	__shared__ int warp_slots[4], warp_len[4];
 	const int lane = tid & 31, warp = tid >> 5;
-	int incl = (tid < 128) ? len : 0;
+	const bool nz = len > 0;
+	int incl = 0, before = 0;
+	unsigned ball = 0;
 	if (tid < 128) {
+		ball = __ballot_sync(0xffffffffu, nz);
+		before = __popc(ball & ((1u << lane) - 1u));
+		incl = len;
 #pragma unroll
 		for (int o = 1; o < 32; o <<= 1) {
-			int v = __shfl_up_sync(0xffffffffu, incl, o);
+			const int v = __shfl_up_sync(0xffffffffu, incl, o);
 			if (lane >= o) incl += v;
 		}
-		const unsigned wm = __reduce_max_sync(0xffffffffu, fm);
 		if (lane == 31) {
-			warp_tot[warp] = incl;
-			warp_fm[warp] = wm;
+			warp_slots[warp] = __popc(ball);
+			warp_len[warp] = incl;
 		}
 	}
 	__syncthreads();
 	if (tid < 128) {
-		int base = 0;
-		for (int w = 0; w < warp; ++w) base += warp_tot[w];
-		if (tid < nent) rt.pref[tid] = base + incl - len;
-		if (tid == nent - 1) {
-			rt.pref[nent] = base + incl;
-			rt.count = nent;
-			rt.fmax_bits = max(max(warp_fm[0], warp_fm[1]), max(warp_fm[2], warp_fm[3]));
+		int sb = 0, lb = 0;
+		for (int w = 0; w < warp; ++w) { sb += warp_slots[w]; lb += warp_len[w]; }
+		if (nz) {
+			const int slot = sb + before;
+			rt.start[slot] = st;
+			rt.pref[slot] = lb + incl - len;
+			rt.shift[slot] = (int) sft;
+		}
+		if (tid == 127) {
+			const int cnt = sb + __popc(ball);
+			rt.count = cnt;
+			rt.pref[cnt] = lb + incl;
 		}
 	}
 	__syncthreads();
 }
 
-// The point slot of candidate item (items number the tile's ranges back to
+// The record slot of candidate item (items number the tile's ranges back to
 // back) for a thread whose items only increase: r is the range of its
 // previous item (0 before the first) and moves forward past the ranges that
 // end at or before item (pref[count] is past every item, so the walk stops).
@@ -172,54 +190,31 @@ __device__ __forceinline__ int range_walk(const RangeTable& rt, int& r, int item
 
 // ------------------------------------------------------------ spread ---
 
-// arr[m] for a run-time m without dynamic register indexing.
-template <int M, typename T>
-__device__ __forceinline__ T select_m(const T* arr, int m)
-{
-	T r = arr[0];
-#pragma unroll
-	for (int k = 1; k < M; ++k) r = (m == k) ? arr[k] : r;
-	return r;
-}
+template <int PREC> struct SpreadAcc;
+template <> struct SpreadAcc<IBK_PRECISION_FP64> { using type = double; };
+template <> struct SpreadAcc<IBK_PRECISION_FP32C> { using type = int; };
 
-template <typename D, int DIMS, int PREC>
-struct SpreadSmem;
-template <typename D, int DIMS>
-struct SpreadSmem<D, DIMS, IBK_PRECISION_FP64> { using acc_t = double; };
-template <typename D, int DIMS>
-struct SpreadSmem<D, DIMS, IBK_PRECISION_FP32C> { using acc_t = int; };
-
-// Fixed point of the FP32C spread.  Each FP32 product is scaled so that the
-// largest possible term of the tile (max|w| * res * max|F| over the tile's
-// candidate points) is below 2^22, rounded to an integer with the float magic
-// number 1.5 * 2^23 (x + magic carries rint(x) in its low mantissa bits for
-// |x| <= 2^22: an FADD and an integer subtract, no conversion instruction),
-// and added to the face's 32-bit working word with one integer shared atomic.
-// At most kFixChunk candidates are summed between folds (kFixChunk * 2^22 <
-// 2^31, so a working word cannot overflow); each fold adds the working words
-// exactly into an FP64 total per face (integers below 2^53 are exact in
-// FP64).  The sum is therefore exact and independent of the order in which
-// points are visited (the binning order is not deterministic; the result
-// is); the only rounding is each product's quantisation to 2^-23 of the
-// tile's largest possible term, and the final scaling is exact.
+// Fixed point of the FP32C spread.  Per (tile, component) a power-of-two
+// scale is chosen so that the sum of |term| over every candidate point of
+// the tile, max|w| * sum |res * F|, is at most 2^30 and every single |term|
+// below 2^22 (the sum of |F| is bounded exactly and order-independently
+// before the accumulation: see spread_scales).  Each FP32 product is scaled,
+// rounded once to an integer with the float magic number 1.5 * 2^23 (x +
+// magic carries rint(x) in its low mantissa bits for |x| <= 2^22: an FFMA and
+// an integer subtract, no conversion instruction) and added to the face's
+// 32-bit word with one integer shared atomic.  A face's final sum is at most
+// 2^30 + (candidates)/2 in magnitude, below 2^31, so it is exact (intermediate
+// wrap-around of the two's-complement word cancels) and independent of the
+// order in which points are visited (the binning order is not deterministic;
+// the result is); the only rounding is each product's quantisation to the
+// scale's unit.
 constexpr float kMagic = 12582912.0f;           // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
-constexpr int kFixChunk = 511;                  // candidates between folds
-constexpr int kFixTermLog2 = 22;                // largest term * scale < 2^22
+constexpr int kFixSumLog2 = 30;                 // bound on sum |term| * scale
+constexpr int kFixTermLog2 = 22;                // bound on one |term| * scale
 
-__device__ __forceinline__ void fix_add(int* word, float s)
-{
-	atomicAdd(word, __float_as_int(s + kMagic) - kMagicBits);   // rint(s)
-}
-
-// fix_add of the product a * b, rounded once (rint of the exact product).
-__device__ __forceinline__ void fix_add_product(int* word, float a, float b)
-{
-	atomicAdd(word, __float_as_int(__fmaf_rn(a, b, kMagic)) - kMagicBits);
-}
-
-// The fixed-point increments of a0 * b and a1 * b (each rounded once, as in
-// fix_add_product), from one packed two-lane FP32 FMA.
+// The fixed-point increments of a0 * b and a1 * b (each rounded once), from
+// one packed two-lane FP32 FMA.
 __device__ __forceinline__ int2 fix_terms2(float a0, float a1, float b)
 {
 	float r0, r1;
@@ -233,278 +228,464 @@ __device__ __forceinline__ int2 fix_terms2(float a0, float a1, float b)
 	return make_int2(__float_as_int(r0) - kMagicBits, __float_as_int(r1) - kMagicBits);
 }
 
-// One candidate point p of a spread tile [lo, hi): its in-tile stencil
-// contributions added to the tile's accumulators (F is read only when the
-// stencil touches the tile).  FP32C: the FP32 product res * F is scaled by
-// the tile's fixed-point scale.
-// contig: the tile spans no periodic axis whole, so the in-tile nodes of a
-// stencil are consecutive along every axis and their accumulators sit at
-// fixed offsets from the first one.
-// near: contig, and every periodic axis has more cells than M + the tile's
-// extent.  A stencil that meets the tile then does so after at most one shift
-// by the period, which places its centre within half a period of the tile's
-// centre; its in-tile nodes follow from the shifted position of node 0
-// without wrapping every node.
-template <typename D, int DIMS, int PREC>
-__device__ __forceinline__ void spread_candidate(const GridGeom& g, const CompGeom& cg, int n,
-                                                 const double* __restrict__ x, const double* __restrict__ fc,
-                                                 int p, float scale, const int* lo, const int* hi, int S1, int S2,
-                                                 bool contig, bool near, typename SpreadSmem<D, DIMS, PREC>::acc_t* acc)
+__device__ __forceinline__ int fix_term(float a, float b)
+{
+	return __float_as_int(__fmaf_rn(a, b, kMagic)) - kMagicBits;
+}
+
+// Shared-memory reduction (no return value) at a 32-bit shared address.
+__device__ __forceinline__ void red_shared(unsigned addr, int v)
+{
+	asm volatile("red.shared.add.s32 [%0], %1;" :: "r"(addr), "r"(v) : "memory");
+}
+
+// In-tile node mask of one axis: bit m set when node (j0 + m) lies in [0, e).
+template <int M>
+__device__ __forceinline__ unsigned axis_mask(int j0, int e)
+{
+	const int mlo = max(0, -j0), mhi = min(M, e - j0);
+	return mhi > mlo ? ((1u << mhi) - 1u) & ~((1u << mlo) - 1u) : 0u;
+}
+
+// One FP32C contribution set: the in-tile nodes of a point's stencil for one
+// component.  l: tile-local stencil origin per axis; dl: fractional offsets;
+// f: res * F * scale; e: faces of the tile per axis; acc: shared byte address
+// of the component's accumulator words (row stride S1, plane stride S2).
+template <typename D, int DIMS>
+__device__ __forceinline__ void spread_fix(unsigned acc, const int* l, const float* dl, float f, const int* e,
+                                           int S1, int S2)
 {
 	constexpr int M = D::M, sh = (M - 1) >> 1;
-	int loc[DIMS][M];
-	unsigned mask[DIMS];
-	int lb[DIMS];           // near: tile-local position of node 0 (may lie outside)
-	double dl[DIMS];
+	unsigned mk[DIMS];
 	bool any = true;
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
-		AxisStep<M> a = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p));
-		dl[d] = a.delta;
-		unsigned mk = 0;
-		if (near) {
-			// spread drops nodes outside [0, points) (errors_negative) and this
-			// tile owns [lo, hi): node m is in it iff 0 <= l + m < hi - lo
-			int l = a.base - sh - lo[d];
-			const int e = hi[d] - lo[d];
-			if (!g.solid[d]) {
-				const int C = cg.cells[d], twice = 2 * l + M - e;
-				l += twice > C ? -C : (twice < -C ? C : 0);
-			}
-			const int m_lo = max(0, -l), m_hi = min(M, e - l);
-			mk = m_hi > m_lo ? ((1u << m_hi) - 1u) & ~((1u << m_lo) - 1u) : 0u;
-			lb[d] = l;
-#pragma unroll
-			for (int m = 0; m < M; ++m) loc[d][m] = l + m;
-		} else {
-			lb[d] = 0;
-#pragma unroll
-			for (int m = 0; m < M; ++m) {
-				const int j = node_index(g, cg, d, a.base + m - sh);
-				loc[d][m] = j - lo[d];
-				mk |= (unsigned) (j >= lo[d] && j < hi[d]) << m;
-			}
-		}
-		mask[d] = mk;
-		any = any && mk;
+		mk[d] = axis_mask<M>(l[d] - sh, e[d]);
+		any = any && mk[d] != 0u;
 	}
 	if (!any) return;
-	if constexpr (PREC == IBK_PRECISION_FP64) {
-		const double f = __dmul_rn(g.res, __ldg(fc + p));
-		double w[DIMS][M];
+	float w[DIMS][M];
 #pragma unroll
-		for (int d = 0; d < DIMS; ++d)
+	for (int d = 0; d < DIMS; ++d) weights32<D>(dl[d], w[d]);
 #pragma unroll
-			for (int m = 0; m < M; ++m)
-				w[d][m] = (mask[d] >> m & 1u) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
+	for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
+	const int first = (l[0] - sh) + (l[1] - sh) * S1 + (DIMS == 3 ? (l[2] - sh) * S2 : 0);
+	const unsigned base = acc + 4u * (unsigned) first;   // wraps for negative origins; in-tile nodes land inside
+	constexpr int R = DIMS == 3 ? M * M : M;
 #pragma unroll
-		for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
+	for (int r = 0; r < R; ++r) {
+		const int m1 = r % M, m2 = r / M;
+		const unsigned rm = DIMS == 3 ? (mk[1] >> m1) & (mk[2] >> m2) & 1u : (mk[1] >> m1) & 1u;
+		if (!rm) continue;      // rows outside the tile (mostly warp-uniform)
+		const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+		const unsigned row = base + 4u * (unsigned) (m1 * S1 + (DIMS == 3 ? m2 * S2 : 0));
 #pragma unroll
-		for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-			const int m1 = r % M, m2 = r / M;
-			const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
-			if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
-			const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
-			const int row = (DIMS == 3 ? loc[2][m2] * S2 : 0) + loc[1][m1] * S1;
-#pragma unroll
-			for (int m0 = 0; m0 < M; ++m0)
-				if ((mask[0] >> m0) & rm)
-					atomicAdd(acc + row + loc[0][m0], __dmul_rn(w[0][m0], w12));
+		for (int m0 = 0; m0 + 1 < M; m0 += 2) {
+			const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
+			if ((mk[0] >> m0) & 1u) red_shared(row + 4u * m0, t.x);
+			if ((mk[0] >> (m0 + 1)) & 1u) red_shared(row + 4u * (m0 + 1), t.y);
 		}
-	} else {
-		const float f = (float) (g.res * __ldg(fc + p)) * scale;
-		float w[DIMS][M];
-#pragma unroll
-		for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w[d]);
-#pragma unroll
-		for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
-		if (contig) {
-			// node (m0, m1, m2) at first + m2 * S2 + m1 * S1 + m0, where
-			// first is the (possibly outside) position of node (0, 0, 0)
-			if (!near) {
-#pragma unroll
-				for (int d = 0; d < DIMS; ++d) {
-					int v = 0;
-					bool found = false;
-#pragma unroll
-					for (int m = 0; m < M; ++m)
-						if (!found && ((mask[d] >> m) & 1u)) { v = loc[d][m] - m; found = true; }
-					lb[d] = v;
-				}
-			}
-			const int first = (DIMS == 3 ? lb[2] * S2 : 0) + lb[1] * S1 + lb[0];
-			int* base = acc + first;
-			constexpr unsigned kFull = (1u << M) - 1u;
-			const bool full = mask[0] == kFull && mask[1] == kFull && (DIMS < 3 || mask[2] == kFull);
-			if (full) {
-				// the whole stencil inside the tile: no per-node tests
-#pragma unroll
-				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-					const int m1 = r % M, m2 = r / M;
-					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-					int* rowp = base + (DIMS == 3 ? m2 * S2 : 0) + m1 * S1;
-#pragma unroll
-					for (int m0 = 0; m0 + 1 < M; m0 += 2) {
-						const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
-						atomicAdd(rowp + m0, t.x);
-						atomicAdd(rowp + m0 + 1, t.y);
-					}
-					if (M & 1) fix_add_product(rowp + (M - 1), w[0][M - 1], w12);
-				}
-			} else {
-#pragma unroll
-				for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-					const int m1 = r % M, m2 = r / M;
-					const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
-					if (!rm) continue;   // rows outside the tile (mostly warp-uniform)
-					const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-					int* rowp = base + (DIMS == 3 ? m2 * S2 : 0) + m1 * S1;
-#pragma unroll
-					for (int m0 = 0; m0 + 1 < M; m0 += 2) {
-						const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
-						if ((mask[0] >> m0) & 1u) atomicAdd(rowp + m0, t.x);
-						if ((mask[0] >> (m0 + 1)) & 1u) atomicAdd(rowp + m0 + 1, t.y);
-					}
-					if ((M & 1) && ((mask[0] >> (M - 1)) & 1u)) fix_add_product(rowp + (M - 1), w[0][M - 1], w12);
-				}
-			}
-		} else {
-#pragma unroll
-			for (int r = 0; r < (DIMS == 3 ? M * M : M); ++r) {
-				const int m1 = r % M, m2 = r / M;
-				const unsigned rm = DIMS == 3 ? (mask[1] >> m1) & (mask[2] >> m2) & 1u : (mask[1] >> m1) & 1u;
-				if (!rm) continue;
-				const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-				const int row = (DIMS == 3 ? loc[2][m2] * S2 : 0) + loc[1][m1] * S1;
-#pragma unroll
-				for (int m0 = 0; m0 < M; ++m0)
-					if ((mask[0] >> m0) & rm) fix_add_product(acc + row + loc[0][m0], w[0][m0], w12);
-			}
-		}
+		if ((M & 1) && ((mk[0] >> (M - 1)) & 1u)) red_shared(row + 4u * (M - 1), fix_term(w[0][M - 1], w12));
 	}
 }
 
-// One (tile, component) of the spread; every thread of the CTA calls it.
-// perm holds point indices offset by pbase (a batch numbers the points of
-// all its instances consecutively); off and binmax are this grid's bins.
+// Node index along axis d of a tile that spans a whole periodic axis (the
+// stencil wraps inside the tile): the wrapped local index, always in range.
+// Elsewhere the local index and whether it lies in [0, e).
+__device__ __forceinline__ int local_node(int j, int e, int cells, bool wrap, bool& ok)
+{
+	if (wrap) {
+		ok = true;
+		return wrap_index(j, cells);
+	}
+	ok = j >= 0 && j < e;
+	return j;
+}
+
+// The general form of spread_fix / spread_f64 for tiles with a wrapping
+// axis: per-node local indices (each face of the tile may be reached from
+// both sides of the period).
+template <typename D, int DIMS, typename Acc, typename Term>
+__device__ __forceinline__ void spread_wrapped(const int* l, const int* e, const int* cells, const bool* wrap,
+                                               int S1, int S2, Acc&& add, Term&& weight_row)
+{
+	constexpr int M = D::M, sh = (M - 1) >> 1;
+	int loc[DIMS][M];
+	unsigned mk[DIMS];
+#pragma unroll
+	for (int d = 0; d < DIMS; ++d) {
+		mk[d] = 0u;
+#pragma unroll
+		for (int m = 0; m < M; ++m) {
+			bool ok;
+			loc[d][m] = local_node(l[d] - sh + m, e[d], cells[d], wrap[d], ok);
+			mk[d] |= (unsigned) ok << m;
+		}
+	}
+	constexpr int R = DIMS == 3 ? M * M : M;
+#pragma unroll
+	for (int r = 0; r < R; ++r) {
+		const int m1 = r % M, m2 = r / M;
+		const unsigned rm = DIMS == 3 ? (mk[1] >> m1) & (mk[2] >> m2) & 1u : (mk[1] >> m1) & 1u;
+		if (!rm) continue;
+		const int row = (DIMS == 3 ? loc[2][m2] * S2 : 0) + loc[1][m1] * S1;
+#pragma unroll
+		for (int m0 = 0; m0 < M; ++m0)
+			if ((mk[0] >> m0) & 1u) add(row + loc[0][m0], weight_row(m0, m1, m2));
+	}
+}
+
+// FP64 contribution set (the reference's arithmetic: w0 * (res F) times
+// w1 * w2, exact weights), tile without wrapping axes.
+template <typename D, int DIMS>
+__device__ __forceinline__ void spread_f64(double* acc, const int* l, const double* dl, double f, const int* e,
+                                           int S1, int S2)
+{
+	constexpr int M = D::M, sh = (M - 1) >> 1;
+	unsigned mk[DIMS];
+	bool any = true;
+#pragma unroll
+	for (int d = 0; d < DIMS; ++d) {
+		mk[d] = axis_mask<M>(l[d] - sh, e[d]);
+		any = any && mk[d] != 0u;
+	}
+	if (!any) return;
+	double w[DIMS][M];
+#pragma unroll
+	for (int d = 0; d < DIMS; ++d)
+#pragma unroll
+		for (int m = 0; m < M; ++m)
+			w[d][m] = (mk[d] >> m & 1u) ? D::phi64(__dadd_rn(dl[d], (double) (m - sh))) : 0.0;
+#pragma unroll
+	for (int m0 = 0; m0 < M; ++m0) w[0][m0] = __dmul_rn(w[0][m0], f);
+	const int first = (l[0] - sh) + (l[1] - sh) * S1 + (DIMS == 3 ? (l[2] - sh) * S2 : 0);
+	constexpr int R = DIMS == 3 ? M * M : M;
+#pragma unroll
+	for (int r = 0; r < R; ++r) {
+		const int m1 = r % M, m2 = r / M;
+		const unsigned rm = DIMS == 3 ? (mk[1] >> m1) & (mk[2] >> m2) & 1u : (mk[1] >> m1) & 1u;
+		if (!rm) continue;
+		const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
+		double* row = acc + first + m1 * S1 + (DIMS == 3 ? m2 * S2 : 0);
+#pragma unroll
+		for (int m0 = 0; m0 < M; ++m0)
+			if ((mk[0] >> m0) & 1u) atomicAdd(row + m0, __dmul_rn(w[0][m0], w12));
+	}
+}
+
+// Block-wide reduction of per-component values (max of unsigned bit
+// patterns, or a sum), result in out[c] for every thread after the call.
+template <int NT, bool MAX>
+__device__ __forceinline__ void block_reduce3(unsigned* v, unsigned* out)
+{
+	__shared__ unsigned part[NT / 32][kMaxDims];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+	for (int c = 0; c < kMaxDims; ++c) {
+		const unsigned r = MAX ? __reduce_max_sync(0xffffffffu, v[c]) : __reduce_add_sync(0xffffffffu, v[c]);
+		if (lane == 0) part[warp][c] = r;
+	}
+	__syncthreads();
+	if (threadIdx.x < kMaxDims) {
+		unsigned r = 0u;
+		for (int w = 0; w < NT / 32; ++w) r = MAX ? max(r, part[w][threadIdx.x]) : r + part[w][threadIdx.x];
+		out[threadIdx.x] = r;
+	}
+	__syncthreads();
+}
+
+// Fixed-point scales of the FP32C spread, one per component, into scale[c]
+// (0 when every candidate's force component is 0).  Two passes over the
+// candidates' forces: the largest |f| (f = FP32 res * F), then
+// S = sum of (ceil(1024 |f| / max|f|) + 1), an integer and therefore
+// independent of the visiting order; max|f| * S / 1024 bounds sum |f|, and
+// the scale is the largest power of two with max|w| * bound * scale < 2^30
+// and max|w| * max|f| * scale < 2^22.
+template <typename D, int DIMS, int NT>
+__device__ __forceinline__ void spread_scales(const GridGeom& g, const RangeTable& rt, int ncand,
+                                              const PointRec* __restrict__ recs, int pbase, int n,
+                                              const double* __restrict__ fl, float* scale)
+{
+	__shared__ unsigned red_out[kMaxDims];
+	unsigned mx[kMaxDims] = {0u, 0u, 0u};
+	int r = 0;
+	for (int it = threadIdx.x; it < ncand; it += NT) {
+		const int p = __ldg(&recs[range_walk(rt, r, it)].p) - pbase;
+#pragma unroll
+		for (int c = 0; c < DIMS; ++c)
+			mx[c] = max(mx[c], __float_as_uint(fabsf((float) (g.res * __ldg(fl + (size_t) c * n + p)))));
+	}
+	block_reduce3<NT, true>(mx, red_out);
+	float inv[kMaxDims];
+#pragma unroll
+	for (int c = 0; c < kMaxDims; ++c) {
+		mx[c] = red_out[c];
+		inv[c] = mx[c] ? 1024.0f / __uint_as_float(mx[c]) : 0.0f;
+	}
+	// units per |f| == max|f|: 1024 while the 32-bit sum of (units + 1) per
+	// candidate cannot overflow, coarser for huge tiles
+	const float q = ncand < (1 << 21) ? 1024.0f : (ncand < (1 << 27) ? 16.0f : 0.0f);
+#pragma unroll
+	for (int c = 0; c < kMaxDims; ++c) inv[c] *= q * (1.0f / 1024.0f);
+	unsigned sum[kMaxDims] = {0u, 0u, 0u};
+	r = 0;
+	for (int it = threadIdx.x; it < ncand; it += NT) {
+		const int p = __ldg(&recs[range_walk(rt, r, it)].p) - pbase;
+#pragma unroll
+		for (int c = 0; c < DIMS; ++c) {
+			const float a = fabsf((float) (g.res * __ldg(fl + (size_t) c * n + p)));
+			sum[c] += (unsigned) ceilf(a * inv[c]) + 1u;
+		}
+	}
+	block_reduce3<NT, false>(sum, red_out);
+	if (threadIdx.x < kMaxDims) {
+		const int c = threadIdx.x;
+		float s = 0.0f;
+		if (c < DIMS && mx[c] != 0u) {
+			// sum |f| <= max|f| * S / q (q = 0: at most max|f| per candidate)
+			const double fmax = (double) __uint_as_float(mx[c]);
+			const double wmax = (double) max_weight<D, DIMS>() * 1.001;
+			const double sum_f = q > 0.0f ? fmax * (double) red_out[c] / (double) q : fmax * (double) ncand;
+			int ex_sum, ex_term;
+			frexp(sum_f * wmax, &ex_sum);            // bound on sum |term| < 2^ex_sum
+			frexp(fmax * wmax, &ex_term);            // bound on one |term| < 2^ex_term
+			// the sum stays below 2^30 and every single term below 2^22 (the
+			// magic-number rounding's range)
+			const int k = min(kFixSumLog2 - ex_sum, kFixTermLog2 - ex_term);
+			s = ldexpf(1.0f, max(-126, min(k, 126)));
+		}
+		scale[c] = s;
+	}
+	__syncthreads();
+}
+
+// Writes the tile's faces of component c: out = value(li) for every face.
+template <int DIMS, int NT, typename V>
+__device__ __forceinline__ void write_tile(double* __restrict__ out, const CompGeom& cg, const int* lo, const int* e,
+                                           int S1, int S2, V&& value)
+{
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	const int lpr = e[0] <= 8 ? 8 : (e[0] <= 16 ? 16 : 32);   // lanes per row
+	const int rpw = 32 / lpr;                                 // rows per warp step
+	const int l0 = lane & (lpr - 1);
+	const int rows = e[1] * (DIMS == 3 ? e[2] : 1);
+	for (int r0 = warp * rpw; r0 < rows; r0 += (NT / 32) * rpw) {
+		const int r = r0 + lane / lpr;
+		if (r >= rows) continue;
+		const int l1 = r % e[1], l2 = r / e[1];
+		const size_t gb = (size_t) cg.points[0] *
+		                  ((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0)) +
+		                  (size_t) lo[0];
+		const int lb = (DIMS == 3 ? l2 * S2 : 0) + l1 * S1;
+		for (int x0 = l0; x0 < e[0]; x0 += lpr) out[gb + x0] = value(lb + x0);
+	}
+}
+
+// One spread tile; every thread of the CTA calls it.  comp < 0: every
+// component (FP32C); else that component only (FP64).  Records carry point
+// indices offset by pbase (a batch numbers the points of all its instances
+// consecutively); off is this grid's bin table.
 template <typename D, int DIMS, int PREC, int NT = kTileThreads>
 __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
-                                            const double* __restrict__ fl, const int* __restrict__ perm, int pbase,
-                                            const int* __restrict__ off, const unsigned* __restrict__ binmax,
-                                            const CompPtrs& fe, int tile, int c)
+                                            const double* __restrict__ fl, const PointRec* __restrict__ recs, int pbase,
+                                            const int* __restrict__ off, const CompPtrs& fe, int tile, int comp)
 {
-	using acc_t = typename SpreadSmem<D, DIMS, PREC>::acc_t;
+	using acc_t = typename SpreadAcc<PREC>::type;
+	constexpr int M = D::M;
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	__shared__ RangeTable rt;
+	__shared__ float s_scale[kMaxDims];
 
-	const CompGeom& cg = g.comp[c];
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
 	const SpreadStrides ss = spread_strides(T0, T1, T2, DIMS);
-	const int TV = ss.words;    // padded accumulator words
-	// FP64: acc[TV] doubles.  FP32C: total[TV] doubles, then acc[TV] working words.
-	double* total = reinterpret_cast<double*>(smem_raw);
-	acc_t* acc = PREC == IBK_PRECISION_FP64 ? reinterpret_cast<acc_t*>(smem_raw)
-	                                        : reinterpret_cast<acc_t*>(total + TV);
+	const int c_lo = comp < 0 ? 0 : comp, c_hi = comp < 0 ? DIMS : comp + 1;
+	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw);
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, tile, tc);
-	int lo[3] = {0, 0, 0}, hi[3] = {1, 1, 1};
-	bool contig = true, near = true;
+	int lo[3] = {0, 0, 0};
+	bool wrap[3] = {false, false, false};
+	bool wrap_any = false;
+	int cells[3] = {1, 1, 1};
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
 		lo[d] = tc[d] * tg.T[d];
-		hi[d] = min(lo[d] + tg.T[d], cg.points[d]);
-		contig = contig && (g.solid[d] || tg.ntiles[d] > 1);
-		near = near && (g.solid[d] || D::M + tg.T[d] < cg.cells[d]);
+		cells[d] = tg.cells[d];
+		wrap[d] = !g.solid[d] && tg.ntiles[d] == 1;
+		wrap_any = wrap_any || wrap[d];
 	}
-	near = near && contig;
-	build_ranges<DIMS>(g, tg, tc, off, rt, true, binmax, c);
-	const double* __restrict__ fc = fl + (size_t) c * n;
-	const int e0 = hi[0] - lo[0], e1 = hi[1] - lo[1], e2 = DIMS == 3 ? hi[2] - lo[2] : 1;
-	double* __restrict__ out = fe.p[c];
+	build_ranges<DIMS>(g, tg, tc, off, rt);
 	const int ncand = rt.pref[rt.count];
 	if (ncand == 0) {
 		// no point reaches the tile: its faces are zero
-		for (int i = threadIdx.x; i < e1 * e2 * T0; i += NT) {
-			const int l0 = i % T0;
-			const int r = i / T0;
-			if (l0 >= e0) continue;
-			const int l1 = r % e1, l2 = r / e1;
-			out[(size_t) (lo[0] + l0) + (size_t) cg.points[0] *
-			    ((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0))] = 0.0;
+		for (int c = c_lo; c < c_hi; ++c) {
+			int e[3] = {1, 1, 1};
+#pragma unroll
+			for (int d = 0; d < DIMS; ++d) e[d] = min(tg.T[d], g.comp[c].points[d] - lo[d]);
+			write_tile<DIMS, NT>(fe.p[c], g.comp[c], lo, e, ss.S1, ss.S2, [](int) { return 0.0; });
 		}
 		return;
 	}
-	for (int i = threadIdx.x; i < TV; i += NT) acc[i] = (acc_t) 0;
-	if constexpr (PREC == IBK_PRECISION_FP32C)
-		for (int i = threadIdx.x; i < TV; i += NT) total[i] = 0.0;
-	__syncthreads();
-
-	double inv_scale = 1.0;     // FP32C: back to force density (exact power of two)
-	if constexpr (PREC == IBK_PRECISION_FP64) {
-		int r = 0;
-		for (int it = threadIdx.x; it < ncand; it += NT)
-			spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_walk(rt, r, it)) - pbase, 0.0f,
-			                                lo, hi, ss.S1, ss.S2, contig, near, acc);
-	} else {
-		// the tile's largest possible term, max|F| * max|w| * res (max|F| over
-		// its candidate bins, rounded to FP32, hence the 1.001), is scaled to
-		// below 2^22; at most kFixChunk candidates between folds
-		const float bound = __uint_as_float(rt.fmax_bits) * 1.001f * max_weight<D, DIMS>() * (float) g.res + 1e-30f;
-		int e;
-		frexpf(bound, &e);                      // bound < 2^e
-		const float scale = ldexpf(1.0f, min(kFixTermLog2 - e, 126));
-		int r = 0;              // this thread's items increase across the chunks
-		for (int base = 0; base < ncand; base += kFixChunk) {
-			const int stop = min(ncand, base + kFixChunk);
-			for (int it = base + threadIdx.x; it < stop; it += NT)
-				spread_candidate<D, DIMS, PREC>(g, cg, n, x, fc, __ldg(perm + range_walk(rt, r, it)) - pbase, scale,
-				                                lo, hi, ss.S1, ss.S2, contig, near, acc);
-			// fold the working words into the exact FP64 totals
-			__syncthreads();
-			for (int i = threadIdx.x; i < TV; i += NT) {
-				total[i] += (double) acc[i];
-				acc[i] = 0;
-			}
-			__syncthreads();
+	const int nwords = ss.words * (c_hi - c_lo);
+	for (int i = threadIdx.x * 4; i < nwords; i += NT * 4) {
+		if constexpr (PREC == IBK_PRECISION_FP32C) *reinterpret_cast<int4*>(acc + i) = make_int4(0, 0, 0, 0);
+		else {
+			*reinterpret_cast<double2*>(acc + i) = make_double2(0.0, 0.0);
+			*reinterpret_cast<double2*>(acc + i + 2) = make_double2(0.0, 0.0);
 		}
-		inv_scale = 1.0 / (double) scale;
+	}
+	if constexpr (PREC == IBK_PRECISION_FP32C) spread_scales<D, DIMS, NT>(g, rt, ncand, recs, pbase, n, fl, s_scale);
+	else __syncthreads();
+
+	const unsigned acc_addr = smem_addr(acc);
+	int r = 0;
+	for (int it = threadIdx.x; it < ncand; it += NT) {
+		const int slot = range_walk(rt, r, it);
+		const PointRec rec = load_rec(recs + slot);
+		const int sft = rt.shift[r];
+		const int p = rec.p - pbase;
+		int lh[DIMS];
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) lh[d] = rec_origin(rec.org, d) + unpack8(sft, d);
+#pragma unroll 1
+		for (int c = c_lo; c < c_hi; ++c) {
+			const CompGeom& cg = g.comp[c];
+			int l[DIMS], e[DIMS];
+#pragma unroll
+			for (int d = 0; d < DIMS; ++d) {
+				const bool own = tg.tag_mac && d == c;
+				l[d] = lh[d] + (own ? rec_own_shift(rec.org, d) : 0);
+				e[d] = min(tg.T[d], cg.points[d] - lo[d]);
+			}
+			if constexpr (PREC == IBK_PRECISION_FP32C) {
+				const float sc = s_scale[c];
+				if (sc == 0.0f) continue;
+				const float f = (float) (g.res * __ldg(fl + (size_t) c * n + p)) * sc;
+				float dl[DIMS];
+#pragma unroll
+				for (int d = 0; d < DIMS; ++d) dl[d] = (tg.tag_mac && d == c) ? rec.dn[d] : rec.dh[d];
+				const unsigned a = acc_addr + 4u * (unsigned) (ss.words * (c - c_lo));
+				if (!wrap_any) {
+					spread_fix<D, DIMS>(a, l, dl, f, e, ss.S1, ss.S2);
+				} else {
+					float w[DIMS][M];
+#pragma unroll
+					for (int d = 0; d < DIMS; ++d) weights32<D>(dl[d], w[d]);
+					spread_wrapped<D, DIMS>(l, e, cells, wrap, ss.S1, ss.S2,
+						[&](int li, int v) { red_shared(a + 4u * (unsigned) li, v); },
+						[&](int m0, int m1, int m2) {
+							const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+							return fix_term(w[0][m0] * f, w12);
+						});
+				}
+			} else {
+				const double f = __dmul_rn(g.res, __ldg(fl + (size_t) c * n + p));
+				double dl[DIMS];
+#pragma unroll
+				for (int d = 0; d < DIMS; ++d) dl[d] = axis_step<M>(g, cg, d, __ldg(x + (size_t) d * n + p)).delta;
+				double* a = reinterpret_cast<double*>(acc) + (size_t) ss.words * (c - c_lo);
+				if (!wrap_any) {
+					spread_f64<D, DIMS>(a, l, dl, f, e, ss.S1, ss.S2);
+				} else {
+					constexpr int sh = (M - 1) >> 1;
+					double w[DIMS][M];
+#pragma unroll
+					for (int d = 0; d < DIMS; ++d)
+#pragma unroll
+						for (int m = 0; m < M; ++m) w[d][m] = D::phi64(__dadd_rn(dl[d], (double) (m - sh)));
+					spread_wrapped<D, DIMS>(l, e, cells, wrap, ss.S1, ss.S2,
+						[&](int li, double v) { atomicAdd(a + li, v); },
+						[&](int m0, int m1, int m2) {
+							const double w12 = DIMS == 3 ? __dmul_rn(w[1][m1], w[2][m2]) : w[1][m1];
+							return __dmul_rn(__dmul_rn(w[0][m0], f), w12);
+						});
+				}
+			}
+		}
 	}
 	__syncthreads();
 
 	// every face of the tile, written once
-	for (int i = threadIdx.x; i < e1 * e2 * T0; i += NT) {
-		const int l0 = i % T0;
-		const int r = i / T0;
-		if (l0 >= e0) continue;
-		const int l1 = r % e1, l2 = r / e1;
-		const size_t gi = (size_t) (lo[0] + l0) + (size_t) cg.points[0] *
-			((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0));
-		const int li = (DIMS == 3 ? l2 * ss.S2 : 0) + l1 * ss.S1 + l0;
-		if constexpr (PREC == IBK_PRECISION_FP64) out[gi] = acc[li];
-		else out[gi] = total[li] * inv_scale;
+	for (int c = c_lo; c < c_hi; ++c) {
+		int e[3] = {1, 1, 1};
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) e[d] = min(tg.T[d], g.comp[c].points[d] - lo[d]);
+		const acc_t* ac = acc + (size_t) ss.words * (c - c_lo);
+		if constexpr (PREC == IBK_PRECISION_FP64) {
+			write_tile<DIMS, NT>(fe.p[c], g.comp[c], lo, e, ss.S1, ss.S2, [&](int li) { return ac[li]; });
+		} else {
+			const float sc = s_scale[c];
+			const double inv = sc != 0.0f ? 1.0 / (double) sc : 0.0;
+			write_tile<DIMS, NT>(fe.p[c], g.comp[c], lo, e, ss.S1, ss.S2,
+			                     [&](int li) { return (double) ac[li] * inv; });
+		}
 	}
 }
 
-// NT threads per CTA; FP32C CTAs are capped at 64 registers per thread so
-// that 1024 threads of them fit on an SM, FP64 ones (256 threads) at 85 so
-// that three fit.
-template <typename D, int DIMS, int PREC, int NT>
-__global__ void __launch_bounds__(NT, PREC == IBK_PRECISION_FP32C ? 1024 / NT : 3)
-spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                   const double* __restrict__ fl, const int* __restrict__ perm,
-                   const int* __restrict__ off, const unsigned* __restrict__ binmax, CompPtrs fe)
+// Shared memory of a spread CTA: the accumulator words of the components it
+// covers (FP32C: every component, 4 bytes per face; FP64: one, 8 bytes).
+__host__ __device__ inline size_t spread_smem_bytes(const TileGeom& tg, int dims, int precision)
 {
-	// grid: (tile, component)
-	spread_tile<D, DIMS, PREC, NT>(g, tg, n, x, fl, perm, 0, off, binmax, fe, blockIdx.x, blockIdx.y);
+	const size_t words = (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], dims).words;
+	return precision == IBK_PRECISION_FP32C ? words * 4 * (size_t) dims : words * 8;
+}
+
+// FP32C: 256-thread CTAs capped at 64 registers so that four fit on an SM
+// (their accumulators take 54 KB each at 16^3 tiles); FP64 ones at 85 so
+// that three fit.
+template <typename D, int DIMS, int PREC>
+__global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
+spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                   const double* __restrict__ fl, const PointRec* __restrict__ recs,
+                   const int* __restrict__ off, CompPtrs fe)
+{
+	// grid: tiles (FP32C) or (tile, component) (FP64)
+	spread_tile<D, DIMS, PREC>(g, tg, n, x, fl, recs, 0, off, fe, blockIdx.x,
+	                           PREC == IBK_PRECISION_FP32C ? -1 : (int) blockIdx.y);
 }
 
 // ------------------------------------------------------------ interp ---
 
-// Halo of the staged region around the tile, per side.
-template <int M> struct Halo {
-	static constexpr int lo = 1 + ((M - 1) >> 1);
-	static constexpr int hi = 1 + M / 2;
-};
+// Staged region of component c along one axis, relative to the tile's first
+// cell: every node of every point of the tile lies in [lower, lower + extent)
+// (own-axis origin shifts in [dlo, dhi]).  The x range starts on an even
+// cell and has an even extent so a TMA box row is a multiple of 16 bytes.
+template <int M>
+__host__ __device__ inline void region_axis(int T, int dlo, int dhi, bool x_axis, int* lower, int* extent)
+{
+	constexpr int sh = (M - 1) >> 1;
+	int lw = dlo - sh;
+	const int up = T - 1 + dhi - sh + M - 1;
+	if (x_axis) lw &= ~1;
+	int ext = up - lw + 1;
+	if (x_axis) ext = (ext + 1) & ~1;
+	*lower = lw;
+	*extent = ext;
+}
+
+template <int M>
+__host__ __device__ inline void region_of(const GridGeom& g, const TileGeom& tg, int c, int* lower, int* extent)
+{
+	for (int d = 0; d < kMaxDims; ++d) { lower[d] = 0; extent[d] = 1; }
+	for (int d = 0; d < g.dims; ++d) {
+		int dlo, dhi;
+		own_shift_range(g, tg.tag_mac, c, d, &dlo, &dhi);
+		region_axis<M>(tg.T[d], dlo, dhi, d == 0, &lower[d], &extent[d]);
+	}
+}
+
+// Largest staged region of any component, in bytes, plus 128 bytes of slack
+// for aligning the TMA destination by hand.
+template <int M>
+inline size_t interp_smem_bytes(const GridGeom& g, const TileGeom& tg)
+{
+	size_t best = 0;
+	for (int c = 0; c < g.dims; ++c) {
+		int lw[3], ex[3];
+		region_of<M>(g, tg, c, lw, ex);
+		best = std::max(best, (size_t) ex[0] * ex[1] * ex[2]);
+	}
+	return sizeof(double) * best + 128;
+}
 
 // Fold a region coordinate onto the grid: wrap periodic axes, clamp walls.
 __device__ __forceinline__ int fold(const GridGeom& g, const CompGeom& cg, int d, int v)
@@ -513,15 +694,6 @@ __device__ __forceinline__ int fold(const GridGeom& g, const CompGeom& cg, int d
 	if (g.solid[d]) return v < 0 ? 0 : (v >= pd ? pd - 1 : v);
 	if (v < 0 || v >= pd) v = wrap_index(v, cg.cells[d]);
 	return v;
-}
-
-// Staged-region geometry shared by host and device: the x extent is padded to
-// an even count so a TMA box row is a multiple of 16 bytes.
-template <int M>
-__host__ __device__ inline int region_extent(int T, int d)
-{
-	const int e = T + Halo<M>::lo + Halo<M>::hi;
-	return d == 0 ? (e + 1) & ~1 : e;
 }
 
 // Epilogue of the serving step, applied to each interpolated velocity U of
@@ -535,6 +707,54 @@ struct StepEpilogue {
 	double dt, k;
 };
 
+// Global gather of one point whose stencil leaves the staged region (points
+// beyond a wall, whose clamped origin lies outside the tile's halo): node
+// indices wrapped (periodic) or clamped (walls) as the reference clamps them
+// (include/ib/interpolate.h:16-22), weights from the fractional offsets
+// (the exact FP64 ones in the FP64 form), summed in the reference's pattern
+// order.  b: stencil origin per axis in the component's index space
+// (unwrapped); solid: bit d set for a wall axis.  Out of line: it is rare
+// and its registers would otherwise weigh on the staged path.
+template <typename D, int DIMS>
+__device__ __noinline__ double interp_global(const double* __restrict__ u, int b0, int b1, int b2, double d0,
+                                             double d1, double d2, int p0, int p1, int p2, int c0, int c1, int c2,
+                                             int solid)
+{
+	using P = Pattern<D::M, DIMS, D::every_other>;
+	constexpr int M = D::M, sh = (M - 1) >> 1;
+	const int b[3] = {b0, b1, b2}, pts[3] = {p0, p1, p2}, cells[3] = {c0, c1, c2};
+	const double dl[3] = {d0, d1, d2};
+	int gidx[DIMS][M];
+	double w[DIMS][M];
+#pragma unroll
+	for (int d = 0; d < DIMS; ++d) {
+#pragma unroll
+		for (int m = 0; m < M; ++m) {
+			int j = b[d] + m - sh;
+			if (!((solid >> d) & 1)) j = wrap_index(j, cells[d]);
+			gidx[d][m] = j < 0 ? 0 : (j >= pts[d] ? pts[d] - 1 : j);
+			w[d][m] = D::phi64(__dadd_rn(dl[d], (double) (m - sh)));
+		}
+	}
+	double v = 0.0;
+#pragma unroll
+	for (int e = 0; e < P::V; ++e) {
+		const int m0 = P::m(e, 0), m1 = P::m(e, 1);
+		double wt;
+		long long k;
+		if constexpr (DIMS == 3) {
+			const int m2 = P::m(e, 2);
+			wt = __dmul_rn(w[0][m0], __dmul_rn(w[1][m1], w[2][m2]));
+			k = gidx[0][m0] + (long long) p0 * (gidx[1][m1] + (long long) p1 * gidx[2][m2]);
+		} else {
+			wt = __dmul_rn(w[0][m0], w[1][m1]);
+			k = gidx[0][m0] + (long long) p0 * gidx[1][m1];
+		}
+		v = __dadd_rn(v, __dmul_rn(wt, __ldg(u + k)));
+	}
+	return v;
+}
+
 // One (tile, component) of the interpolation; every thread of the CTA calls
 // it.  maps/use_tma select TMA staging (maps_global: the maps live in global
 // memory, written by a copy before the launch); epi, when not null, adds the
@@ -543,14 +763,13 @@ struct StepEpilogue {
 // the CTA must stop).
 template <typename D, int DIMS, int PREC>
 __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
-                                            const int* __restrict__ perm, int pbase, const int* __restrict__ off,
+                                            const PointRec* __restrict__ recs, int pbase, const int* __restrict__ off,
                                             const ConstCompPtrs& ue, double* __restrict__ ul,
                                             const CUtensorMap* maps, int use_tma, bool maps_global, int* status,
                                             const StepEpilogue* epi, int t, int c)
 {
 	using P = Pattern<D::M, DIMS, D::every_other>;
 	constexpr int M = D::M, sh = (M - 1) >> 1;
-	constexpr int HL = Halo<M>::lo;
 	// The region pointer is aligned to 128 bytes by hand (TMA destination);
 	// the launch adds 128 bytes of slack for it.
 	extern __shared__ __align__(16) unsigned char interp_smem[];
@@ -564,13 +783,13 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 	const double* __restrict__ u = ue.p[c];
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, t, tc);
-	int rlo[3] = {0, 0, 0}, E[3] = {1, 1, 1};
+	int lower[3], E[3], rlo[3] = {0, 0, 0};
+	region_of<M>(g, tg, c, lower, E);
 	bool tma = use_tma != 0;        // stage with one bulk tensor copy
 	bool interior = true;           // the region lies inside the grid
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) {
-		rlo[d] = tc[d] * tg.T[d] - HL;
-		E[d] = region_extent<M>(tg.T[d], d);
+		rlo[d] = tc[d] * tg.T[d] + lower[d];
 		interior = interior && rlo[d] >= 0 && rlo[d] + E[d] <= cg.points[d];
 	}
 	// self-check of the TMA preconditions: 128-byte destination, x origin
@@ -580,15 +799,10 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 		if (threadIdx.x == 0 && status) atomicExch(status, 2);
 		tma = false;
 	}
-	// first point of this thread, fetched while the region is staged
+	// first record of this thread, fetched while the region is staged
 	int it = start + threadIdx.x;
-	int p_next = 0;
-	double z_next[DIMS];
-	if (it < end) {
-		p_next = __ldg(perm + it) - pbase;
-#pragma unroll
-		for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
-	}
+	PointRec rec_next{};
+	if (it < end) rec_next = load_rec(recs + it);
 	if (tma) {
 		// one bulk tensor copy of the box; at a domain edge the box starts at a
 		// negative or past-the-end coordinate and the copy zero-fills those
@@ -715,34 +929,28 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 		}
 	}
 	for (; it < end; it += kTileThreads) {
-		const int p = p_next;
-		double z[DIMS];
-#pragma unroll
-		for (int d = 0; d < DIMS; ++d) z[d] = z_next[d];
-		if (it + kTileThreads < end) {          // prefetch the next point
-			p_next = __ldg(perm + it + kTileThreads) - pbase;
-#pragma unroll
-			for (int d = 0; d < DIMS; ++d) z_next[d] = __ldg(x + (size_t) d * n + p_next);
-		}
-		int loc[DIMS];          // local index of the stencil's first node
-		double dl[DIMS];
+		const PointRec rec = rec_next;
+		if (it + kTileThreads < end) rec_next = load_rec(recs + it + kTileThreads);   // prefetch the next point
+		const int p = rec.p - pbase;
+		int loc[DIMS];          // region index of the stencil's first node
 		bool inside = true;
 #pragma unroll
 		for (int d = 0; d < DIMS; ++d) {
-			AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
-			dl[d] = a.delta;
-			int b = a.base;
-			if (!g.solid[d] && tg.ntiles[d] > 1) {
-				const int cells = cg.cells[d];
-				const int diff = b - (rlo[d] + HL);
-				if (2 * diff > cells) b -= cells;
-				else if (2 * diff < -cells) b += cells;
-			}
-			const int l = b - sh - rlo[d];
-			loc[d] = l;
-			inside = inside && l >= 0 && l + M <= E[d];
+			const bool own = tg.tag_mac && d == c;
+			const int l = rec_origin(rec.org, d) + (own ? rec_own_shift(rec.org, d) : 0);
+			loc[d] = l - sh - lower[d];
+			inside = inside && loc[d] >= 0 && loc[d] + M <= E[d];
 		}
 		double v;
+		double zc = 0.0;
+		if (PREC == IBK_PRECISION_FP64 || epi != nullptr) zc = __ldg(x + (size_t) c * n + p);
+		// FP64: the exact fractional offsets of this component
+		double dl64[DIMS];
+		if constexpr (PREC == IBK_PRECISION_FP64) {
+#pragma unroll
+			for (int d = 0; d < DIMS; ++d)
+				dl64[d] = axis_step<M>(g, cg, d, d == c ? zc : __ldg(x + (size_t) d * n + p)).delta;
+		}
 		if (inside) {
 			const int base = DIMS == 3 ? (loc[2] * E[1] + loc[1]) * E[0] + loc[0] : loc[1] * E[0] + loc[0];
 			if constexpr (PREC == IBK_PRECISION_FP64) {
@@ -750,7 +958,7 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 #pragma unroll
 				for (int d = 0; d < DIMS; ++d)
 #pragma unroll
-					for (int m = 0; m < M; ++m) w[d][m] = D::phi64(__dadd_rn(dl[d], (double) (m - sh)));
+					for (int m = 0; m < M; ++m) w[d][m] = D::phi64(__dadd_rn(dl64[d], (double) (m - sh)));
 				v = 0.0;
 #pragma unroll
 				for (int e = 0; e < P::V; ++e) {
@@ -771,7 +979,8 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 				// FP32 weights and FP32 staged values; FP32 row sums, FP64 total
 				float w32[DIMS][M];
 #pragma unroll
-				for (int d = 0; d < DIMS; ++d) weights32<D>((float) dl[d], w32[d]);
+				for (int d = 0; d < DIMS; ++d)
+					weights32<D>((tg.tag_mac && d == c) ? rec.dn[d] : rec.dh[d], w32[d]);
 				const float* regf = reinterpret_cast<const float*>(reg);
 				v = 0.0;
 				constexpr int R = DIMS == 3 ? M * M : M;
@@ -787,43 +996,22 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 				}
 			}
 		} else {
-			// stencil leaves the staged region: exact global gather
-			int gidx[DIMS][M];
-			double w[DIMS][M];
+			// stencil leaves the staged region: global gather
+			int b[3] = {0, 0, 0}, sol = 0;
+			double dd[3] = {0.0, 0.0, 0.0};
 #pragma unroll
 			for (int d = 0; d < DIMS; ++d) {
-				AxisStep<M> a = axis_step<M>(g, cg, d, z[d]);
-#pragma unroll
-				for (int m = 0; m < M; ++m) {
-					const int j = node_index(g, cg, d, a.base + m - sh);
-					const int pd = cg.points[d];
-					gidx[d][m] = j < 0 ? 0 : (j >= pd ? pd - 1 : j);
-					w[d][m] = D::phi64(__dadd_rn(a.delta, (double) (m - sh)));
-				}
+				b[d] = loc[d] + sh + lower[d] + tc[d] * tg.T[d];
+				sol |= g.solid[d] << d;
+				if constexpr (PREC == IBK_PRECISION_FP64) dd[d] = dl64[d];
+				else dd[d] = (double) ((tg.tag_mac && d == c) ? rec.dn[d] : rec.dh[d]);
 			}
-			v = 0.0;
-#pragma unroll
-			for (int e = 0; e < P::V; ++e) {
-				const int m0 = P::m(e, 0), m1 = P::m(e, 1);
-				double wt;
-				long long k;
-				if constexpr (DIMS == 3) {
-					const int m2 = P::m(e, 2);
-					wt = __dmul_rn(w[0][m0], __dmul_rn(w[1][m1], w[2][m2]));
-					k = gidx[0][m0] + (long long) cg.points[0] * (gidx[1][m1] + (long long) cg.points[1] * gidx[2][m2]);
-				} else {
-					wt = __dmul_rn(w[0][m0], w[1][m1]);
-					k = gidx[0][m0] + (long long) cg.points[0] * gidx[1][m1];
-				}
-				v = __dadd_rn(v, __dmul_rn(wt, __ldg(u + k)));
-			}
+			v = interp_global<D, DIMS>(u, b[0], b[1], b[2], dd[0], dd[1], dd[2], cg.points[0], cg.points[1],
+			                           cg.points[2], cg.cells[0], cg.cells[1], cg.cells[2], sol);
 		}
 		const size_t i = (size_t) c * n + p;
 		if (ul != nullptr) ul[i] = v;
 		if (epi != nullptr) {
-			double zc = z[0];
-#pragma unroll
-			for (int d = 1; d < DIMS; ++d) zc = d == c ? z[d] : zc;
 			const double xn = __dadd_rn(zc, __dmul_rn(epi->dt, v));
 			epi->xn[i] = xn;
 			epi->fl[i] = __dmul_rn(-epi->k, __dsub_rn(xn, __ldg(epi->xref + i)));
@@ -833,14 +1021,14 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 }
 
 template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 2 : 1)
+__global__ void __launch_bounds__(kTileThreads, D::M <= 4 ? 3 : 1)
 interp_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
-                   const int* __restrict__ perm, const int* __restrict__ off,
+                   const PointRec* __restrict__ recs, const int* __restrict__ off,
                    ConstCompPtrs ue, double* __restrict__ ul,
                    const __grid_constant__ TmaMaps maps, int use_tma, int* status)
 {
 	// grid: (tile, component)
-	interp_tile<D, DIMS, PREC>(g, tg, n, x, perm, 0, off, ue, ul, maps.map, use_tma, false, status, nullptr,
+	interp_tile<D, DIMS, PREC>(g, tg, n, x, recs, 0, off, ue, ul, maps.map, use_tma, false, status, nullptr,
 	                           blockIdx.x, blockIdx.y);
 }
 

@@ -63,10 +63,11 @@ typedef enum {
 /* Arithmetic of the operators.  FP64: the reference's arithmetic (keys,
  * origins and weights bit-exact; interpolation sums in the reference's order;
  * spread differs from the reference only by summation order).  FP32C: the
- * same FP64 index step and FP32 weights; spread sums the FP32 products
- * exactly in fixed point (order-independent, so results do not depend on
- * scheduling), interpolation applies the FP32 weights to the FP64 values
- * with FP64 accumulation; FP64 inputs and outputs. */
+ * same FP64 index step (exact stencil origins) and FP32 weights; spread sums
+ * the FP32 products exactly in a per-tile fixed point (order-independent, so
+ * results do not depend on scheduling), interpolation applies the FP32
+ * weights to the grid values rounded to FP32, with FP32 row sums and an FP64
+ * total; FP64 inputs and outputs.  Forces must be finite. */
 typedef enum { IBK_PRECISION_FP64 = 0, IBK_PRECISION_FP32C = 1 } ibk_precision;
 
 /* fd::domain of fd::dimension{length, boundary} (include/fd/domain.h:15-33,
@@ -106,11 +107,13 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement,
 ibk_status ibk_plan_destroy(ibk_plan plan);
 ibk_status ibk_plan_info(ibk_plan plan, ibk_grid_info* info);
 
-/* Preferred tile extents in cells per axis for the spread (owner-computes
- * accumulator tiles) and interpolation (staged halo regions) kernels; either
- * may be NULL to keep the current shape.  Each axis is shrunk so its last
- * tile keeps at least M cells.  Defaults: 16^3 for both.  Results do not depend on the shape
- * except through the FP32C fixed-point scale, which is per tile. */
+/* Preferred tile extents in cells per axis, in [M, 64], for the spread
+ * (owner-computes accumulator tiles) and interpolation (staged halo regions)
+ * kernels; either may be NULL to keep the current shape.  Each axis is
+ * shrunk so its last tile keeps at least M cells.  Defaults: 16^3 for both
+ * (equal shapes let ibk_spread_interpolate bin the points once).  Results do
+ * not depend on the shape except through the FP32C fixed-point scale, which
+ * is per tile. */
 ibk_status ibk_plan_set_tiles(ibk_plan plan, const int* spread_tile, const int* interp_tile);
 
 /* Pre-size the plan's device scratch for up to max_points points, so that
@@ -129,6 +132,17 @@ ibk_status ibk_spread(ibk_plan plan, int n, const double* x, const double* fl,
  * pointers; ul: device, dims*n doubles. */
 ibk_status ibk_interpolate(ibk_plan plan, int n, const double* x,
                            const double* const* ue, double* ul, void* stream);
+
+/* Spread and interpolation at the same positions, as the reference's time
+ * step calls ib::spread and ib::interpolate on one x (include/ib/novel.h:
+ * 197-227, include/ib/interpolate.h:92-115; test/ib-whole.cc:226-286 shows
+ * the step).  The result is that of ibk_spread(plan, n, x, fl, fe, stream)
+ * followed by ibk_interpolate(plan, n, x, ue, ul, stream); the points are
+ * binned once when the plan's spread and interpolation tiles agree (the
+ * default) instead of once per operator. */
+ibk_status ibk_spread_interpolate(ibk_plan plan, int n, const double* x, const double* fl,
+                                  double* const* fe, const double* const* ue, double* ul,
+                                  void* stream);
 
 /* ib::sweep::sort (include/ib/sweep.h:64-77): the reference's 32-bit sort key
  * of every point for component `component` (device output, n ints). */
@@ -224,7 +238,10 @@ typedef enum {
 	/* One coupled immersed-boundary step: U = interpolate(x, ue) (written to
 	 * ul when ul is not NULL); xn = x + dt*U (forward Euler); fs = -k*(xn -
 	 * xref) (linear spring to the rest shape); fe <- spread(xn, fs). */
-	IBK_OP_STEP = 3
+	IBK_OP_STEP = 3,
+	/* fe <- spread(x, fl) and ul <- interpolate(x, ue): the points are binned
+	 * once when the spread and interpolation tiles agree. */
+	IBK_OP_SPREAD_INTERPOLATE = 4
 } ibk_batch_op;
 
 /* Launch shape of a batch: preferred tile extents in cells per axis (shrunk
