@@ -314,8 +314,8 @@ def run_ours(args):
     flush = None if big else torch.empty(2 * L2_BYTES // 4, dtype=torch.float32, device=dev)
 
     def step():
-        plan.spread(n, x, f, fe, stream)
-        plan.interpolate(n, x, ue, ul, stream)
+        # one spread and one interpolation at the same positions (one binning)
+        plan.spread_interpolate(n, x, f, fe, ue, ul, stream)
 
     def barrier():
         if world > 1:
@@ -427,8 +427,7 @@ def run_ours(args):
             ev["in"][b].record(s_in)
             stream.wait_event(ev["in"][b])
             stream.wait_event(ev["out"][b])          # U buffer b downloaded (step i-2)
-            plan.spread(n, xs[b], fs_[b], fe, stream)
-            plan.interpolate(n, xs[b], ue, uls[b], stream)
+            plan.spread_interpolate(n, xs[b], fs_[b], fe, ue, uls[b], stream)
             ev["comp"][b].record(stream)
             s_out.wait_event(ev["comp"][b])
             with torch.cuda.stream(s_out):
@@ -480,8 +479,7 @@ def run_ours(args):
         ul64 = torch.empty(3 * n, dtype=torch.float64, device=dev)
 
         def step64():
-            plan64.spread(n, x, f, fe64, stream)
-            plan64.interpolate(n, x, ue, ul64, stream)
+            plan64.spread_interpolate(n, x, f, fe64, ue, ul64, stream)
 
         for _ in range(2):
             step64()
@@ -726,15 +724,14 @@ def run_batched(ibk, W, dev, seed, steps, rank=0, world=1):
     cube_faces = [3 * int(round(w.lengths[0] / 0.025)) ** 3 for w in everything]
     shards = sharding.partition([sharding.instance_cost(w.n, f) for w, f in zip(everything, cube_faces)], world)
     insts_w = [everything[i] for i in shards[rank]]
-    ops = (ibk.OP_SPREAD, ibk.OP_INTERPOLATE)
+    ops = (ibk.OP_SPREAD_INTERPOLATE,)      # spread and interpolation, one binning
     out = {"instances": len(everything), "instances_this_rank": len(insts_w),
            "scaling": "strong", "parallelism": f"instances partitioned over {world} rank(s)"}
     batch, io, total = ensemble_arrays(ibk, W, insts_w, ibk.FP32C, dev, 2000 + seed)
     faces = sum(cube_faces)
     assert world > 1 or faces == sum(sum(batch.sizes(i)) for i in range(len(insts_w)))
     t_default = max_over_ranks(time_batch(batch, ops, steps, stream), world, dev)
-    cfg_s = batch.tune(ibk.OP_SPREAD, stream)
-    cfg = batch.tune(ibk.OP_INTERPOLATE, stream)
+    cfg = batch.tune(ibk.OP_SPREAD_INTERPOLATE, stream)
     for op in ops:
         batch.capture(op)
     l0 = batch.launch_count()
@@ -775,8 +772,7 @@ def run_batched(ibk, W, dev, seed, steps, rank=0, world=1):
 
     def loop():
         for p_, e in zip(plans, io):
-            p_.spread(e["n"], e["x"], e["fl"], e["fe"], stream)
-            p_.interpolate(e["n"], e["x"], e["ue"], e["ul"], stream)
+            p_.spread_interpolate(e["n"], e["x"], e["fl"], e["fe"], e["ue"], e["ul"], stream)
 
     for _ in range(2):
         loop()

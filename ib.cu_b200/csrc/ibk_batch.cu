@@ -108,11 +108,20 @@ __device__ __forceinline__ void copy_to_shared(T* dst, const T* src)
 // counts) and each block iteration bins one chunk, so the instance is found
 // by one search per chunk and its geometry read from a shared-memory copy.
 // spread: bin by the spread tiles (else the interpolation tiles); moved:
-// positions xn (else x).
+// positions xn (else x); forces: 1 = fl, 2 = fs (the bins' force
+// statistics for the FP32C scale, see BinStats), 0 = none.
+template <int DIMS>
+__device__ __forceinline__ void instance_forces(const BatchInst& si, const BatchIO& so, int forces, int p, float* a)
+{
+	const double* f = forces == 1 ? so.fl : so.fs;
+#pragma unroll
+	for (int c = 0; c < DIMS; ++c) a[c] = fabsf((float) (si.g.res * __ldg(f + (size_t) c * so.n + p)));
+}
+
 template <int M, int DIMS>
 __global__ void __launch_bounds__(kBinThreads)
-batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved,
-                       int* __restrict__ counts, int2* __restrict__ key_rank)
+batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved, int forces,
+                       int* __restrict__ counts, int2* __restrict__ key_rank, unsigned* __restrict__ binmax)
 {
 	__shared__ int cur_inst, cur_chunk;
 	__shared__ BatchInst si;
@@ -132,13 +141,16 @@ batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int sp
 		const int p = cur_chunk * kBinThreads + threadIdx.x;
 		const bool active = p < n;
 		int key = 0;
+		float a[kMaxDims] = {0.0f, 0.0f, 0.0f};
 		if (active) {
+			// forces is uniform, and a bound instance with points has its force array
+			if (forces) instance_forces<DIMS>(si, so, forces, p, a);
 			const double* x = moved ? so.xn : so.x;
 			key = spread ? si.bin_s + point_bin<M, DIMS>(si.g, si.ts, x, n, p, nullptr)
 			             : si.bin_i + point_bin<M, DIMS>(si.g, si.ti, x, n, p, nullptr);
 		}
 		const unsigned mask = __ballot_sync(0xffffffffu, active);
-		if (active) bin_rank(mask, key, counts, key_rank + so.pbase + p);
+		if (active) bin_rank<DIMS>(mask, key, counts, key_rank + so.pbase + p, forces ? a : nullptr, binmax);
 		__syncthreads();            // the next chunk overwrites the shared copies
 	}
 }
@@ -147,9 +159,10 @@ batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int sp
 // chunks as the count kernel.
 template <int M, int DIMS>
 __global__ void __launch_bounds__(kBinThreads)
-batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved,
+batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved, int forces,
                          const int2* __restrict__ key_rank, const int* __restrict__ offset,
-                         PointRec* __restrict__ recs)
+                         PointRec* __restrict__ recs, const unsigned* __restrict__ binmax,
+                         unsigned long long* __restrict__ binsum)
 {
 	__shared__ int cur_inst, cur_chunk;
 	__shared__ BatchInst si;
@@ -166,6 +179,14 @@ batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int 
 		copy_to_shared(&so, t.io + cur_inst);
 		__syncthreads();
 		const int p = cur_chunk * kBinThreads + threadIdx.x;
+		if (forces) {
+			const unsigned mask = __ballot_sync(0xffffffffu, p < so.n);
+			if (p < so.n) {
+				float a[kMaxDims] = {0.0f, 0.0f, 0.0f};
+				instance_forces<DIMS>(si, so, forces, p, a);
+				bin_sum<DIMS>(mask, __ldg(&key_rank[so.pbase + p].x), a, binmax, binsum);
+			}
+		}
 		if (p < so.n) {
 			const int gp = so.pbase + p;
 			const int2 kr = __ldg(key_rank + gp);
@@ -195,7 +216,8 @@ __device__ __forceinline__ void next_item(int* next, int nitems, int nact, const
 template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
 batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
-                    const PointRec* __restrict__ recs, const int* __restrict__ off, int step)
+                    const PointRec* __restrict__ recs, const int* __restrict__ off, const unsigned* __restrict__ binmax,
+                    const unsigned long long* __restrict__ binsum, int step)
 {
 	__shared__ int cur_inst, cur_local;
 	__shared__ BatchInst si;
@@ -212,12 +234,14 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		CompPtrs fe;
 #pragma unroll
 		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
-		if constexpr (PREC == IBK_PRECISION_FP32C)
+		if constexpr (PREC == IBK_PRECISION_FP32C) {
+			const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims, binsum + (size_t) si.bin_s * kMaxDims};
 			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
-			                           off + si.bin_s, fe, local, -1);
-		else
+			                           off + si.bin_s, bs, fe, local, -1);
+		} else {
 			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
-			                           off + si.bin_s, fe, local / DIMS, local % DIMS);
+			                           off + si.bin_s, BinStatsView{nullptr, nullptr}, fe, local / DIMS, local % DIMS);
+		}
 		__syncthreads();
 	}
 }
@@ -307,6 +331,8 @@ struct Batch {
 	int* d_status = nullptr;
 	int2* d_kr = nullptr;
 	PointRec* d_recs = nullptr;
+	unsigned* d_binmax = nullptr;               // spread bins' force statistics (FP32C)
+	unsigned long long* d_binsum = nullptr;
 	// step parameters and graphs
 	double dt = 0.0, k = 0.0;
 	cudaStream_t cap_stream = nullptr;
@@ -352,17 +378,25 @@ BatchTable table_view(const Batch& b)
 // Binning of the bound points by the spread (spread = 1) or interpolation
 // tiles, then the scan and the records in bin order.
 template <int M, int DIMS>
-ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved)
+ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved, int forces)
 {
 	const BatchTable t = table_view(b);
 	const int nbins = spread ? b.bins_s : b.bins_i;
-	batch_bin_count_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved,
-	                                                                    b.d_counts, b.d_kr);
+	if (forces) {
+		ibk_status st = cuda_check(cudaMemsetAsync(b.d_binmax, 0, sizeof(unsigned) * kMaxDims * (size_t) nbins, s),
+		                           "cudaMemsetAsync");
+		if (st == IBK_OK)
+			st = cuda_check(cudaMemsetAsync(b.d_binsum, 0, sizeof(unsigned long long) * kMaxDims * (size_t) nbins, s),
+			                "cudaMemsetAsync");
+		if (st != IBK_OK) return st;
+	}
+	batch_bin_count_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, forces,
+	                                                                    b.d_counts, b.d_kr, b.d_binmax);
 	const int nchunks = (nbins + kScanChunk - 1) / kScanChunk;
 	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, nbins);
 	bin_scan_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, b.d_off, nbins, nchunks);
-	batch_bin_scatter_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, b.d_kr,
-	                                                                      b.d_off, b.d_recs);
+	batch_bin_scatter_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, forces, b.d_kr,
+	                                                                      b.d_off, b.d_recs, b.d_binmax, b.d_binsum);
 	b.launches += 4;
 	return check_launch("batch binning");
 }
@@ -390,21 +424,23 @@ ibk_status batch_run_impl(Batch& b, int op, cudaStream_t s)
 	};
 	auto spread = [&]() -> ibk_status {
 		batch_spread_kernel<D, DIMS, PREC><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
-			b.d_inst, t, b.d_next, b.d_recs, b.d_off, step ? 1 : 0);
+			b.d_inst, t, b.d_next, b.d_recs, b.d_off, b.d_binmax, b.d_binsum, step ? 1 : 0);
 		b.launches += 1;
 		return check_launch("batch_spread_kernel");
 	};
+	// FP32C spreads take the bins' force statistics from the binning
+	const int forces = PREC == IBK_PRECISION_FP32C ? (step ? 2 : 1) : 0;
 	if (op == IBK_OP_INTERPOLATE || step) {
-		if ((st = batch_bin<D::M, DIMS>(b, s, 0, 0)) != IBK_OK) return st;
+		if ((st = batch_bin<D::M, DIMS>(b, s, 0, 0, 0)) != IBK_OK) return st;
 		if ((st = interp()) != IBK_OK) return st;
 	}
 	if (op == IBK_OP_SPREAD || step || both) {
-		if ((st = batch_bin<D::M, DIMS>(b, s, 1, step ? 1 : 0)) != IBK_OK) return st;
+		if ((st = batch_bin<D::M, DIMS>(b, s, 1, step ? 1 : 0, forces)) != IBK_OK) return st;
 		if ((st = spread()) != IBK_OK) return st;
 	}
 	if (both) {
 		// the spread's records serve the interpolation when the tiles agree
-		if (!same_tiles(b.config) && (st = batch_bin<D::M, DIMS>(b, s, 0, 0)) != IBK_OK) return st;
+		if (!same_tiles(b.config) && (st = batch_bin<D::M, DIMS>(b, s, 0, 0, 0)) != IBK_OK) return st;
 		if ((st = interp()) != IBK_OK) return st;
 	}
 	return IBK_OK;
@@ -574,14 +610,16 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		// bin arrays sized for the larger bin space (counts start zeroed and
 		// every scan leaves them zeroed)
 		void** bufs[] = {reinterpret_cast<void**>(&b.d_counts), reinterpret_cast<void**>(&b.d_off),
-		                 reinterpret_cast<void**>(&b.d_chunk)};
-		const size_t bytes[] = {sizeof(int) * nb, sizeof(int) * (nb + 1), sizeof(int) * (nb / kScanChunk + 2)};
+		                 reinterpret_cast<void**>(&b.d_chunk), reinterpret_cast<void**>(&b.d_binmax),
+		                 reinterpret_cast<void**>(&b.d_binsum)};
+		const size_t bytes[] = {sizeof(int) * nb, sizeof(int) * (nb + 1), sizeof(int) * (nb / kScanChunk + 2),
+		                        sizeof(unsigned) * kMaxDims * nb, sizeof(unsigned long long) * kMaxDims * nb};
 		b.bins_cap = 0;
-		for (int j = 0; j < 3; ++j) {
+		for (int j = 0; j < 5; ++j) {
 			if (*bufs[j]) cudaFree(*bufs[j]);
 			*bufs[j] = nullptr;
 		}
-		for (int j = 0; j < 3; ++j)
+		for (int j = 0; j < 5; ++j)
 			if ((st = cuda_check(cudaMalloc(bufs[j], bytes[j]), "cudaMalloc")) != IBK_OK) return st;
 		if ((st = cuda_check(cudaMemset(b.d_counts, 0, bytes[0]), "cudaMemset")) != IBK_OK) return st;
 		b.bins_cap = nb;
@@ -625,7 +663,7 @@ void destroy(Batch* b)
 		if (b->h_ring[r]) cudaFreeHost(b->h_ring[r]);
 	}
 	void* bufs[] = {b->d_inst, b->d_table, b->d_counts, b->d_off, b->d_chunk, b->d_recs,
-	                b->d_next, b->d_status, b->d_kr};
+	                b->d_next, b->d_status, b->d_kr, b->d_binmax, b->d_binsum};
 	for (void* p : bufs)
 		if (p) cudaFree(p);
 	if (b->cap_stream) cudaStreamDestroy(b->cap_stream);

@@ -80,7 +80,8 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 }
 
 // Scratch slots of a plan.
-enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotRecs = 3, kSlotChunk = 4, kSlotSums = 6 };
+enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotRecs = 3, kSlotChunk = 4, kSlotBinMax = 5,
+       kSlotSums = 6, kSlotBinSum = 7 };
 
 // Largest tile extent in cells per axis (point records keep tile-relative
 // origins in 8 bits).

@@ -38,10 +38,11 @@ ibk_status interp_direct(Plan& plan, const OpArgs& a, ConstCompPtrs ue, double* 
 }
 
 // Counting sort of the points by (tile, reach class): records in bin order
-// and the bin offsets.
+// and the bin offsets; with forces f (a spread follows) also the bins' force
+// statistics for the FP32C scale.
 template <int M, int DIMS>
 ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, const PointRec** recs_out,
-                      const int** off_out)
+                      const int** off_out, const double* f = nullptr, BinStatsView* stats_out = nullptr)
 {
 	ibk_status s;
 	const int need = a.n > plan.reserved_points ? a.n : plan.reserved_points;
@@ -58,8 +59,22 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, const Poi
 	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
 	const GridGeom& g = *a.g;
 	const int nb = blocks_for(a.n, 256);
+	BinStats st{nullptr, g.res, nullptr, nullptr};
+	if (f) {
+		const size_t nm = sizeof(unsigned) * kMaxDims * (size_t) tg.num_bins;
+		const size_t ns = sizeof(unsigned long long) * kMaxDims * (size_t) tg.num_bins;
+		if ((s = ensure_scratch(plan, kSlotBinMax, nm, a.stream)) != IBK_OK) return s;
+		if ((s = ensure_scratch(plan, kSlotBinSum, ns, a.stream)) != IBK_OK) return s;
+		st.f = f;
+		st.binmax = static_cast<unsigned*>(plan.scratch[kSlotBinMax].ptr);
+		st.binsum = static_cast<unsigned long long*>(plan.scratch[kSlotBinSum].ptr);
+		cudaError_t e = cudaMemsetAsync(st.binmax, 0, nm, a.stream);
+		if (e == cudaSuccess) e = cudaMemsetAsync(st.binsum, 0, ns, a.stream);
+		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+		*stats_out = BinStatsView{st.binmax, st.binsum};
+	}
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
-		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr);
+		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, st);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_chunk_sum_kernel", a.stream, [&] {
 		bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, tg.num_bins);
@@ -68,7 +83,7 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, const Poi
 		bin_scan_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, off, tg.num_bins, nchunks);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scatter_kernel", a.stream, [&] {
-		bin_scatter_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, kr, off, recs);
+		bin_scatter_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, kr, off, recs, st);
 	})) != IBK_OK) return s;
 	*recs_out = recs;
 	*off_out = off;
@@ -87,7 +102,7 @@ ibk_status set_smem(K kernel, size_t bytes)
 
 template <typename D, int DIMS, int PREC>
 ibk_status launch_spread(Plan& plan, const OpArgs& a, const TileGeom& tg, const PointRec* recs, const int* off,
-                         const double* fl, CompPtrs fe)
+                         BinStatsView bs, const double* fl, CompPtrs fe)
 {
 	const size_t smem = spread_smem_bytes(tg, DIMS, PREC);
 	auto kern = spread_tile_kernel<D, DIMS, PREC>;
@@ -96,7 +111,7 @@ ibk_status launch_spread(Plan& plan, const OpArgs& a, const TileGeom& tg, const 
 	// FP32C: one CTA per tile for every component; FP64: per (tile, component)
 	const dim3 grid(tg.num_tiles, PREC == IBK_PRECISION_FP32C ? 1 : DIMS);
 	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<grid, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, fe);
+		kern<<<grid, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, bs, fe);
 	});
 }
 
@@ -107,9 +122,11 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	if (!plan.tiled) return spread_direct<D, DIMS>(plan, a, fl, fe);
 	const PointRec* recs = nullptr;
 	const int* off = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off);
+	BinStatsView bs{nullptr, nullptr};
+	constexpr bool fix = PREC == IBK_PRECISION_FP32C;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off, fix ? fl : nullptr, &bs);
 	if (s != IBK_OK) return s;
-	return launch_spread<D, DIMS, PREC>(plan, a, plan.spread_tiles, recs, off, fl, fe);
+	return launch_spread<D, DIMS, PREC>(plan, a, plan.spread_tiles, recs, off, bs, fl, fe);
 }
 
 // cuTensorMapEncodeTiled through the runtime's driver entry point (no link
@@ -216,9 +233,11 @@ ibk_status both_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs fe,
 	}
 	const PointRec* recs = nullptr;
 	const int* off = nullptr;
-	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off);
+	BinStatsView bs{nullptr, nullptr};
+	constexpr bool fix = PREC == IBK_PRECISION_FP32C;
+	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off, fix ? fl : nullptr, &bs);
 	if (s != IBK_OK) return s;
-	if ((s = launch_spread<D, DIMS, PREC>(plan, a, plan.spread_tiles, recs, off, fl, fe)) != IBK_OK) return s;
+	if ((s = launch_spread<D, DIMS, PREC>(plan, a, plan.spread_tiles, recs, off, bs, fl, fe)) != IBK_OK) return s;
 	if (!same_tiles(plan.spread_tiles, plan.tiles)) {
 		if ((s = bin_points<D::M, DIMS>(plan, a, plan.tiles, &recs, &off)) != IBK_OK) return s;
 	}

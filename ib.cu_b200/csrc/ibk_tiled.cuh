@@ -92,14 +92,32 @@ struct RangeTable {
 	int count;
 };
 
+// Per-bin force statistics of a grid's bins for the FP32C scale (see
+// BinStats), or null pointers.
+struct BinStatsView {
+	const unsigned* binmax;
+	const unsigned long long* binsum;
+};
+
+// The scale of each component from the statistics of the candidate bins:
+// every bin contributes its largest |f| and the bound binmax * binsum / 1024
+// on its sum of |f|; the scale is the largest power of two that keeps
+// max|w| * (sum bound) * scale below 2^kFixSumLog2 and max|w| * max|f| *
+// scale below 2^kFixTermLog2 (0 when the component's forces are all 0).
+template <int DIMS>
+__device__ __forceinline__ void bin_scales(unsigned* fm, double* sb, float wmax, float* scale);
+
 template <int DIMS>
 __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& tg, const int* tc,
-                                             const int* __restrict__ off, RangeTable& rt)
+                                             const int* __restrict__ off, RangeTable& rt,
+                                             BinStatsView bs = BinStatsView{nullptr, nullptr},
+                                             float wmax = 1.0f, float* scale = nullptr)
 {
 	constexpr int nent = DIMS == 3 ? 125 : 25;
 	const int tid = threadIdx.x;
 	int len = 0, st = 0;
 	unsigned sft = 0;
+	int sbin = -1;          // the bin whose statistics this thread contributes
 	if (tid < nent) {
 		int tile = 0, cls = 0, ts = 1, cs = 1;
 		bool ok = true, home = true, first_home = true;
@@ -132,11 +150,25 @@ __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& 
 				st = __ldg(off + tile * tg.nclass);
 				len = __ldg(off + (tile + 1) * tg.nclass) - st;
 			}
+			sbin = tile * tg.nclass + cls;   // each home class bin once
 		} else if (ok) {
 			const int bin = tile * tg.nclass + cls;
 			st = __ldg(off + bin);
 			len = __ldg(off + bin + 1) - st;
+			sbin = bin;
 		}
+	}
+	if (scale != nullptr) {
+		unsigned fm[kMaxDims] = {0u, 0u, 0u};
+		double sb[kMaxDims] = {0.0, 0.0, 0.0};
+		if (sbin >= 0) {
+#pragma unroll
+			for (int c = 0; c < DIMS; ++c) {
+				fm[c] = __ldg(bs.binmax + (size_t) sbin * kMaxDims + c);
+				sb[c] = (double) __uint_as_float(fm[c]) * (double) __ldg(bs.binsum + (size_t) sbin * kMaxDims + c);
+			}
+		}
+		bin_scales<DIMS>(fm, sb, wmax, scale);
 	}
 	// compaction: slot = number of non-empty entries before this one, pref =
 	// exclusive sum of the lengths (the first 128 threads, 4 warps)
@@ -197,17 +229,17 @@ template <> struct SpreadAcc<IBK_PRECISION_FP32C> { using type = int; };
 // Fixed point of the FP32C spread.  Per (tile, component) a power-of-two
 // scale is chosen so that the sum of |term| over every candidate point of
 // the tile, max|w| * sum |res * F|, is at most 2^30 and every single |term|
-// below 2^22 (the sum of |F| is bounded exactly and order-independently
-// before the accumulation: see spread_scales).  Each FP32 product is scaled,
-// rounded once to an integer with the float magic number 1.5 * 2^23 (x +
-// magic carries rint(x) in its low mantissa bits for |x| <= 2^22: an FFMA and
-// an integer subtract, no conversion instruction) and added to the face's
-// 32-bit word with one integer shared atomic.  A face's final sum is at most
-// 2^30 + (candidates)/2 in magnitude, below 2^31, so it is exact (intermediate
-// wrap-around of the two's-complement word cancels) and independent of the
-// order in which points are visited (the binning order is not deterministic;
-// the result is); the only rounding is each product's quantisation to the
-// scale's unit.
+// below 2^22 (the sum of |F| is bounded exactly and order-independently by
+// the binning's per-bin statistics: see BinStats and bin_scales).  Each FP32
+// product is scaled, rounded once to an integer with the float magic number
+// 1.5 * 2^23 (x + magic carries rint(x) in its low mantissa bits for |x| <=
+// 2^22: an FFMA and an integer subtract, no conversion instruction) and added
+// to the face's 32-bit word with one integer shared atomic.  A face's final
+// sum is at most 2^30 + (candidates)/2 in magnitude, below 2^31, so it is
+// exact (intermediate wrap-around of the two's-complement word cancels) and
+// independent of the order in which points are visited (the binning order is
+// not deterministic; the result is); the only rounding is each product's
+// quantisation to the scale's unit.
 constexpr float kMagic = 12582912.0f;           // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
 constexpr int kFixSumLog2 = 30;                 // bound on sum |term| * scale
@@ -233,11 +265,71 @@ __device__ __forceinline__ int fix_term(float a, float b)
 	return __float_as_int(__fmaf_rn(a, b, kMagic)) - kMagicBits;
 }
 
+template <int DIMS>
+__device__ __forceinline__ void bin_scales(unsigned* fm, double* sb, float wmax, float* scale)
+{
+	// threads 0..127 hold one bin each (or nothing); fixed-order reduction,
+	// so the result does not depend on anything but the bin statistics
+	__shared__ unsigned part_m[4][kMaxDims];
+	__shared__ double part_s[4][kMaxDims];
+	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+	if (threadIdx.x < 128) {
+#pragma unroll
+		for (int c = 0; c < DIMS; ++c) {
+			const unsigned m = __reduce_max_sync(0xffffffffu, fm[c]);
+			double v = sb[c];
+#pragma unroll
+			for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+			if (lane == 0) { part_m[warp][c] = m; part_s[warp][c] = v; }
+		}
+	}
+	__syncthreads();
+	if (threadIdx.x < kMaxDims) {
+		const int c = threadIdx.x;
+		float s = 0.0f;
+		if (c < DIMS) {
+			unsigned m = 0u;
+			double sum = 0.0;
+			for (int w = 0; w < 4; ++w) { m = max(m, part_m[w][c]); sum += part_s[w][c]; }
+			if (m != 0u) {
+				const double wm = (double) wmax * 1.001;
+				int ex_sum, ex_term;
+				frexp(sum * (1.0 / 1024.0) * wm, &ex_sum);             // bound on sum |term| < 2^ex_sum
+				frexp((double) __uint_as_float(m) * wm, &ex_term);    // bound on one |term| < 2^ex_term
+				const int k = min(kFixSumLog2 - ex_sum, kFixTermLog2 - ex_term);
+				s = ldexpf(1.0f, max(-126, min(k, 126)));
+			}
+		}
+		scale[c] = s;
+	}
+}
+
 // Shared-memory reduction (no return value) at a 32-bit shared address.
 __device__ __forceinline__ void red_shared(unsigned addr, int v)
 {
 	asm volatile("red.shared.add.s32 [%0], %1;" :: "r"(addr), "r"(v) : "memory");
 }
+
+// The four reductions of one stencil row of a 4-point delta: node m0 at
+// row + 4 m0 bytes, one block with immediate offsets.  Nodes outside the tile
+// carry zero weight (their addresses stay inside the shared accumulators),
+// so no node needs a predicate or a branch.
+__device__ __forceinline__ void red_row4(unsigned row, int t0, int t1, int t2, int t3)
+{
+	asm volatile("red.shared.add.s32 [%0], %1;\n\tred.shared.add.s32 [%0+4], %2;\n\t"
+	             "red.shared.add.s32 [%0+8], %3;\n\tred.shared.add.s32 [%0+12], %4;"
+	             :: "r"(row), "r"(t0), "r"(t1), "r"(t2), "r"(t3) : "memory");
+}
+
+// Per-lane scratch row that takes the reductions of stencil rows lying
+// outside the tile (cheaper than a branch around them): lane l's row starts
+// at word l * kTrashStride, an odd stride, so the lanes of one instruction
+// hit distinct banks.  The accumulators start kGuardWords after the dynamic
+// shared memory: a row's out-of-tile columns (zero terms) may fall up to
+// M - 1 words before the first row of the first component.
+constexpr int kTrashStride = 7;
+constexpr int kTrashWords = 32 * kTrashStride;
+constexpr int kGuardWords = 8;
 
 // In-tile node mask of one axis: bit m set when node (j0 + m) lies in [0, e).
 template <int M>
@@ -250,10 +342,11 @@ __device__ __forceinline__ unsigned axis_mask(int j0, int e)
 // One FP32C contribution set: the in-tile nodes of a point's stencil for one
 // component.  l: tile-local stencil origin per axis; dl: fractional offsets;
 // f: res * F * scale; e: faces of the tile per axis; acc: shared byte address
-// of the component's accumulator words (row stride S1, plane stride S2).
+// of the component's accumulator words (row stride S1, plane stride S2);
+// trash: this lane's scratch row.
 template <typename D, int DIMS>
-__device__ __forceinline__ void spread_fix(unsigned acc, const int* l, const float* dl, float f, const int* e,
-                                           int S1, int S2)
+__device__ __forceinline__ void spread_fix(unsigned acc, unsigned trash, const int* l, const float* dl, float f,
+                                           const int* e, int S1, int S2)
 {
 	constexpr int M = D::M, sh = (M - 1) >> 1;
 	unsigned mk[DIMS];
@@ -267,8 +360,10 @@ __device__ __forceinline__ void spread_fix(unsigned acc, const int* l, const flo
 	float w[DIMS][M];
 #pragma unroll
 	for (int d = 0; d < DIMS; ++d) weights32<D>(dl[d], w[d]);
+	// columns outside the tile: zero weight (in-row addresses stay inside the
+	// accumulators: padding columns, a neighbouring row or the guard words)
 #pragma unroll
-	for (int m0 = 0; m0 < M; ++m0) w[0][m0] *= f;
+	for (int m0 = 0; m0 < M; ++m0) w[0][m0] = (mk[0] >> m0) & 1u ? w[0][m0] * f : 0.0f;
 	const int first = (l[0] - sh) + (l[1] - sh) * S1 + (DIMS == 3 ? (l[2] - sh) * S2 : 0);
 	const unsigned base = acc + 4u * (unsigned) first;   // wraps for negative origins; in-tile nodes land inside
 	constexpr int R = DIMS == 3 ? M * M : M;
@@ -276,16 +371,22 @@ __device__ __forceinline__ void spread_fix(unsigned acc, const int* l, const flo
 	for (int r = 0; r < R; ++r) {
 		const int m1 = r % M, m2 = r / M;
 		const unsigned rm = DIMS == 3 ? (mk[1] >> m1) & (mk[2] >> m2) & 1u : (mk[1] >> m1) & 1u;
-		if (!rm) continue;      // rows outside the tile (mostly warp-uniform)
 		const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-		const unsigned row = base + 4u * (unsigned) (m1 * S1 + (DIMS == 3 ? m2 * S2 : 0));
+		// rows outside the tile go to this lane's scratch row
+		const unsigned row = rm ? base + 4u * (unsigned) (m1 * S1 + (DIMS == 3 ? m2 * S2 : 0)) : trash;
+		if constexpr (M == 4) {
+			const int2 a = fix_terms2(w[0][0], w[0][1], w12);
+			const int2 b = fix_terms2(w[0][2], w[0][3], w12);
+			red_row4(row, a.x, a.y, b.x, b.y);
+		} else {
 #pragma unroll
-		for (int m0 = 0; m0 + 1 < M; m0 += 2) {
-			const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
-			if ((mk[0] >> m0) & 1u) red_shared(row + 4u * m0, t.x);
-			if ((mk[0] >> (m0 + 1)) & 1u) red_shared(row + 4u * (m0 + 1), t.y);
+			for (int m0 = 0; m0 + 1 < M; m0 += 2) {
+				const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
+				red_shared(row + 4u * m0, t.x);
+				red_shared(row + 4u * (m0 + 1), t.y);
+			}
+			if (M & 1) red_shared(row + 4u * (M - 1), fix_term(w[0][M - 1], w12));
 		}
-		if ((M & 1) && ((mk[0] >> (M - 1)) & 1u)) red_shared(row + 4u * (M - 1), fix_term(w[0][M - 1], w12));
 	}
 }
 
@@ -373,111 +474,28 @@ __device__ __forceinline__ void spread_f64(double* acc, const int* l, const doub
 	}
 }
 
-// Block-wide reduction of per-component values (max of unsigned bit
-// patterns, or a sum), result in out[c] for every thread after the call.
-template <int NT, bool MAX>
-__device__ __forceinline__ void block_reduce3(unsigned* v, unsigned* out)
-{
-	__shared__ unsigned part[NT / 32][kMaxDims];
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-	for (int c = 0; c < kMaxDims; ++c) {
-		const unsigned r = MAX ? __reduce_max_sync(0xffffffffu, v[c]) : __reduce_add_sync(0xffffffffu, v[c]);
-		if (lane == 0) part[warp][c] = r;
-	}
-	__syncthreads();
-	if (threadIdx.x < kMaxDims) {
-		unsigned r = 0u;
-		for (int w = 0; w < NT / 32; ++w) r = MAX ? max(r, part[w][threadIdx.x]) : r + part[w][threadIdx.x];
-		out[threadIdx.x] = r;
-	}
-	__syncthreads();
-}
-
-// Fixed-point scales of the FP32C spread, one per component, into scale[c]
-// (0 when every candidate's force component is 0).  Two passes over the
-// candidates' forces: the largest |f| (f = FP32 res * F), then
-// S = sum of (ceil(1024 |f| / max|f|) + 1), an integer and therefore
-// independent of the visiting order; max|f| * S / 1024 bounds sum |f|, and
-// the scale is the largest power of two with max|w| * bound * scale < 2^30
-// and max|w| * max|f| * scale < 2^22.
-template <typename D, int DIMS, int NT>
-__device__ __forceinline__ void spread_scales(const GridGeom& g, const RangeTable& rt, int ncand,
-                                              const PointRec* __restrict__ recs, int pbase, int n,
-                                              const double* __restrict__ fl, float* scale)
-{
-	__shared__ unsigned red_out[kMaxDims];
-	unsigned mx[kMaxDims] = {0u, 0u, 0u};
-	int r = 0;
-	for (int it = threadIdx.x; it < ncand; it += NT) {
-		const int p = __ldg(&recs[range_walk(rt, r, it)].p) - pbase;
-#pragma unroll
-		for (int c = 0; c < DIMS; ++c)
-			mx[c] = max(mx[c], __float_as_uint(fabsf((float) (g.res * __ldg(fl + (size_t) c * n + p)))));
-	}
-	block_reduce3<NT, true>(mx, red_out);
-	float inv[kMaxDims];
-#pragma unroll
-	for (int c = 0; c < kMaxDims; ++c) {
-		mx[c] = red_out[c];
-		inv[c] = mx[c] ? 1024.0f / __uint_as_float(mx[c]) : 0.0f;
-	}
-	// units per |f| == max|f|: 1024 while the 32-bit sum of (units + 1) per
-	// candidate cannot overflow, coarser for huge tiles
-	const float q = ncand < (1 << 21) ? 1024.0f : (ncand < (1 << 27) ? 16.0f : 0.0f);
-#pragma unroll
-	for (int c = 0; c < kMaxDims; ++c) inv[c] *= q * (1.0f / 1024.0f);
-	unsigned sum[kMaxDims] = {0u, 0u, 0u};
-	r = 0;
-	for (int it = threadIdx.x; it < ncand; it += NT) {
-		const int p = __ldg(&recs[range_walk(rt, r, it)].p) - pbase;
-#pragma unroll
-		for (int c = 0; c < DIMS; ++c) {
-			const float a = fabsf((float) (g.res * __ldg(fl + (size_t) c * n + p)));
-			sum[c] += (unsigned) ceilf(a * inv[c]) + 1u;
-		}
-	}
-	block_reduce3<NT, false>(sum, red_out);
-	if (threadIdx.x < kMaxDims) {
-		const int c = threadIdx.x;
-		float s = 0.0f;
-		if (c < DIMS && mx[c] != 0u) {
-			// sum |f| <= max|f| * S / q (q = 0: at most max|f| per candidate)
-			const double fmax = (double) __uint_as_float(mx[c]);
-			const double wmax = (double) max_weight<D, DIMS>() * 1.001;
-			const double sum_f = q > 0.0f ? fmax * (double) red_out[c] / (double) q : fmax * (double) ncand;
-			int ex_sum, ex_term;
-			frexp(sum_f * wmax, &ex_sum);            // bound on sum |term| < 2^ex_sum
-			frexp(fmax * wmax, &ex_term);            // bound on one |term| < 2^ex_term
-			// the sum stays below 2^30 and every single term below 2^22 (the
-			// magic-number rounding's range)
-			const int k = min(kFixSumLog2 - ex_sum, kFixTermLog2 - ex_term);
-			s = ldexpf(1.0f, max(-126, min(k, 126)));
-		}
-		scale[c] = s;
-	}
-	__syncthreads();
-}
-
 // Writes the tile's faces of component c: out = value(li) for every face.
+// Lanes run along x (8, 16 or 32 per row), the warps' row groups along y,
+// planes one after the other: no division per face.
 template <int DIMS, int NT, typename V>
 __device__ __forceinline__ void write_tile(double* __restrict__ out, const CompGeom& cg, const int* lo, const int* e,
                                            int S1, int S2, V&& value)
 {
 	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 	const int lpr = e[0] <= 8 ? 8 : (e[0] <= 16 ? 16 : 32);   // lanes per row
-	const int rpw = 32 / lpr;                                 // rows per warp step
+	const int rpw = 32 / lpr;                                 // rows per warp
 	const int l0 = lane & (lpr - 1);
-	const int rows = e[1] * (DIMS == 3 ? e[2] : 1);
-	for (int r0 = warp * rpw; r0 < rows; r0 += (NT / 32) * rpw) {
-		const int r = r0 + lane / lpr;
-		if (r >= rows) continue;
-		const int l1 = r % e[1], l2 = r / e[1];
-		const size_t gb = (size_t) cg.points[0] *
-		                  ((size_t) (lo[1] + l1) + (DIMS == 3 ? (size_t) cg.points[1] * (size_t) (lo[2] + l2) : 0)) +
-		                  (size_t) lo[0];
-		const int lb = (DIMS == 3 ? l2 * S2 : 0) + l1 * S1;
-		for (int x0 = l0; x0 < e[0]; x0 += lpr) out[gb + x0] = value(lb + x0);
+	const int rstep = (NT / 32) * rpw;                        // rows per CTA step
+	const int planes = DIMS == 3 ? e[2] : 1;
+	const size_t P0 = (size_t) cg.points[0];
+	const size_t P01 = P0 * (size_t) cg.points[1];
+	for (int l2 = 0; l2 < planes; ++l2) {
+		const size_t pb = (size_t) lo[0] + P0 * (size_t) lo[1] + (DIMS == 3 ? P01 * (size_t) (lo[2] + l2) : 0);
+		for (int l1 = warp * rpw + lane / lpr; l1 < e[1]; l1 += rstep) {
+			double* o = out + pb + P0 * (size_t) l1;
+			const int lb = (DIMS == 3 ? l2 * S2 : 0) + l1 * S1;
+			for (int x0 = l0; x0 < e[0]; x0 += lpr) o[x0] = value(lb + x0);
+		}
 	}
 }
 
@@ -488,7 +506,8 @@ __device__ __forceinline__ void write_tile(double* __restrict__ out, const CompG
 template <typename D, int DIMS, int PREC, int NT = kTileThreads>
 __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
                                             const double* __restrict__ fl, const PointRec* __restrict__ recs, int pbase,
-                                            const int* __restrict__ off, const CompPtrs& fe, int tile, int comp)
+                                            const int* __restrict__ off, BinStatsView bs, const CompPtrs& fe,
+                                            int tile, int comp)
 {
 	using acc_t = typename SpreadAcc<PREC>::type;
 	constexpr int M = D::M;
@@ -499,7 +518,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	const int T0 = tg.T[0], T1 = tg.T[1], T2 = DIMS == 3 ? tg.T[2] : 1;
 	const SpreadStrides ss = spread_strides(T0, T1, T2, DIMS);
 	const int c_lo = comp < 0 ? 0 : comp, c_hi = comp < 0 ? DIMS : comp + 1;
-	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw);
+	acc_t* acc = reinterpret_cast<acc_t*>(smem_raw + 4 * kGuardWords);
 	int tc[3] = {0, 0, 0};
 	tile_coords(tg, tile, tc);
 	int lo[3] = {0, 0, 0};
@@ -513,7 +532,8 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		wrap[d] = !g.solid[d] && tg.ntiles[d] == 1;
 		wrap_any = wrap_any || wrap[d];
 	}
-	build_ranges<DIMS>(g, tg, tc, off, rt);
+	if constexpr (PREC == IBK_PRECISION_FP32C) build_ranges<DIMS>(g, tg, tc, off, rt, bs, max_weight<D, DIMS>(), s_scale);
+	else build_ranges<DIMS>(g, tg, tc, off, rt);
 	const int ncand = rt.pref[rt.count];
 	if (ncand == 0) {
 		// no point reaches the tile: its faces are zero
@@ -533,10 +553,11 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 			*reinterpret_cast<double2*>(acc + i + 2) = make_double2(0.0, 0.0);
 		}
 	}
-	if constexpr (PREC == IBK_PRECISION_FP32C) spread_scales<D, DIMS, NT>(g, rt, ncand, recs, pbase, n, fl, s_scale);
-	else __syncthreads();
+	__syncthreads();
 
 	const unsigned acc_addr = smem_addr(acc);
+	// this lane's scratch row, past the accumulators (FP32C)
+	const unsigned trash = acc_addr + 4u * (unsigned) (nwords + (threadIdx.x & 31) * kTrashStride);
 	int r = 0;
 	for (int it = threadIdx.x; it < ncand; it += NT) {
 		const int slot = range_walk(rt, r, it);
@@ -565,7 +586,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 				for (int d = 0; d < DIMS; ++d) dl[d] = (tg.tag_mac && d == c) ? rec.dn[d] : rec.dh[d];
 				const unsigned a = acc_addr + 4u * (unsigned) (ss.words * (c - c_lo));
 				if (!wrap_any) {
-					spread_fix<D, DIMS>(a, l, dl, f, e, ss.S1, ss.S2);
+					spread_fix<D, DIMS>(a, trash, l, dl, f, e, ss.S1, ss.S2);
 				} else {
 					float w[DIMS][M];
 #pragma unroll
@@ -622,11 +643,13 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 }
 
 // Shared memory of a spread CTA: the accumulator words of the components it
-// covers (FP32C: every component, 4 bytes per face; FP64: one, 8 bytes).
+// covers (FP32C: every component, 4 bytes per face, and the lanes' scratch
+// rows; FP64: one component, 8 bytes per face).
 __host__ __device__ inline size_t spread_smem_bytes(const TileGeom& tg, int dims, int precision)
 {
 	const size_t words = (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], dims).words;
-	return precision == IBK_PRECISION_FP32C ? words * 4 * (size_t) dims : words * 8;
+	return precision == IBK_PRECISION_FP32C ? (words * (size_t) dims + kTrashWords + kGuardWords) * 4
+	                                        : words * 8 + 4 * kGuardWords;
 }
 
 // FP32C: 256-thread CTAs capped at 64 registers so that four fit on an SM
@@ -636,10 +659,10 @@ template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
 spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const double* __restrict__ fl, const PointRec* __restrict__ recs,
-                   const int* __restrict__ off, CompPtrs fe)
+                   const int* __restrict__ off, BinStatsView bs, CompPtrs fe)
 {
 	// grid: tiles (FP32C) or (tile, component) (FP64)
-	spread_tile<D, DIMS, PREC>(g, tg, n, x, fl, recs, 0, off, fe, blockIdx.x,
+	spread_tile<D, DIMS, PREC>(g, tg, n, x, fl, recs, 0, off, bs, fe, blockIdx.x,
 	                           PREC == IBK_PRECISION_FP32C ? -1 : (int) blockIdx.y);
 }
 
