@@ -266,6 +266,7 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 	plan->delta_order = delta.kind == kBspline ? delta.order : 0;
 	plan->precision = precision;
 	cudaGetDevice(&plan->device);
+	cudaDeviceGetAttribute(&plan->num_sms, cudaDevAttrMultiProcessorCount, plan->device);
 
 	ibk_status gs = make_geometry(domain, tag, refinement, meshwidths_of(delta.kind, plan->delta_order),
 	                              plan->g, plan->info);
@@ -324,7 +325,7 @@ ibk_status ibk_plan_set_tiles(ibk_plan handle, const int* spread_tile, const int
 			if (spread_tile[d] < M || spread_tile[d] > kMaxTileExtent)
 				return set_error(IBK_ERR_INVALID_ARGUMENT, "spread tile extents must lie in [M, 64]");
 		ts = make_tiles(plan->g, plan->tag, M, spread_tile);
-		if (spread_tile_bytes(ts, dims, plan->precision) > 200 * 1024)
+		if (spread_tile_bytes(plan->g, ts, M, plan->precision) > 200 * 1024)
 			return set_error(IBK_ERR_UNSUPPORTED, "spread tile needs more than 200 KB of shared memory");
 	}
 	if (interp_tile) {

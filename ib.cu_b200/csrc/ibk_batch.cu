@@ -159,10 +159,9 @@ batch_bin_count_kernel(const BatchInst* __restrict__ insts, BatchTable t, int sp
 // chunks as the count kernel.
 template <int M, int DIMS>
 __global__ void __launch_bounds__(kBinThreads)
-batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved, int forces,
+batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int spread, int moved,
                          const int2* __restrict__ key_rank, const int* __restrict__ offset,
-                         PointRec* __restrict__ recs, const unsigned* __restrict__ binmax,
-                         unsigned long long* __restrict__ binsum)
+                         PointRec* __restrict__ recs)
 {
 	__shared__ int cur_inst, cur_chunk;
 	__shared__ BatchInst si;
@@ -179,14 +178,6 @@ batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int 
 		copy_to_shared(&so, t.io + cur_inst);
 		__syncthreads();
 		const int p = cur_chunk * kBinThreads + threadIdx.x;
-		if (forces) {
-			const unsigned mask = __ballot_sync(0xffffffffu, p < so.n);
-			if (p < so.n) {
-				float a[kMaxDims] = {0.0f, 0.0f, 0.0f};
-				instance_forces<DIMS>(si, so, forces, p, a);
-				bin_sum<DIMS>(mask, __ldg(&key_rank[so.pbase + p].x), a, binmax, binsum);
-			}
-		}
 		if (p < so.n) {
 			const int gp = so.pbase + p;
 			const int2 kr = __ldg(key_rank + gp);
@@ -202,9 +193,10 @@ batch_bin_scatter_kernel(const BatchInst* __restrict__ insts, BatchTable t, int 
 // Thread 0 takes the next work item of the active instances: instance and
 // item index within it, or instance -1 when the list is exhausted.
 __device__ __forceinline__ void next_item(int* next, int nitems, int nact, const int* __restrict__ pre,
-                                          const int* __restrict__ active, int* inst, int* local)
+                                          const int* __restrict__ active, int* inst, int* local, int* item = nullptr)
 {
 	const int k = atomicAdd(next, 1);
+	if (item) *item = k;
 	if (k >= nitems) { *inst = -1; *local = 0; return; }
 	const int j = find_instance(pre, nact, k);
 	*inst = __ldg(active + j);
@@ -217,16 +209,16 @@ template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
 batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
                     const PointRec* __restrict__ recs, const int* __restrict__ off, const unsigned* __restrict__ binmax,
-                    const unsigned long long* __restrict__ binsum, int step)
+                    int step, Deferral defer)
 {
-	__shared__ int cur_inst, cur_local;
+	__shared__ int cur_inst, cur_local, cur_item;
 	__shared__ BatchInst si;
 	__shared__ BatchIO so;
 	const int nitems = __ldg(&t.hdr->items_s), nact = __ldg(&t.hdr->num_active);
 	for (;;) {
-		if (threadIdx.x == 0) next_item(next, nitems, nact, t.spre, t.active, &cur_inst, &cur_local);
+		if (threadIdx.x == 0) next_item(next, nitems, nact, t.spre, t.active, &cur_inst, &cur_local, &cur_item);
 		__syncthreads();
-		const int inst = cur_inst, local = cur_local;
+		const int inst = cur_inst, local = cur_local, item = cur_item;
 		if (inst < 0) return;
 		copy_to_shared(&si, insts + inst);
 		copy_to_shared(&so, t.io + inst);
@@ -235,13 +227,47 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 #pragma unroll
 		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
 		if constexpr (PREC == IBK_PRECISION_FP32C) {
-			const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims, binsum + (size_t) si.bin_s * kMaxDims};
+			const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims};
+			// a dense tile is deferred by its work-item index
 			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
-			                           off + si.bin_s, bs, fe, local, -1);
+			                           off + si.bin_s, bs, fe, local, -1, defer, item);
 		} else {
 			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
-			                           off + si.bin_s, BinStatsView{nullptr, nullptr}, fe, local / DIMS, local % DIMS);
+			                           off + si.bin_s, BinStatsView{nullptr}, fe, local / DIMS, local % DIMS);
 		}
+		__syncthreads();
+	}
+}
+
+// The deferred dense tiles of an FP32C batch spread (see Deferral): work
+// items in the deferral list, folded.
+template <typename D, int DIMS>
+__global__ void __launch_bounds__(kTileThreads, 4)
+batch_spread_dense_kernel(const BatchInst* __restrict__ insts, BatchTable t, const PointRec* __restrict__ recs,
+                          const int* __restrict__ off, const unsigned* __restrict__ binmax, int step,
+                          const int* __restrict__ list, const int* __restrict__ count)
+{
+	__shared__ BatchInst si;
+	__shared__ BatchIO so;
+	__shared__ int cur_inst, cur_local;
+	const int m = *count, nact = __ldg(&t.hdr->num_active);
+	for (int q = blockIdx.x; q < m; q += gridDim.x) {
+		if (threadIdx.x == 0) {
+			const int k = __ldg(list + q);
+			const int j = find_instance(t.spre, nact, k);
+			cur_inst = __ldg(t.active + j);
+			cur_local = k - __ldg(t.spre + j);
+		}
+		__syncthreads();
+		copy_to_shared(&si, insts + cur_inst);
+		copy_to_shared(&so, t.io + cur_inst);
+		__syncthreads();
+		CompPtrs fe;
+#pragma unroll
+		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
+		const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims};
+		spread_tile<D, DIMS, IBK_PRECISION_FP32C, true>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl,
+		                                                recs, so.pbase, off + si.bin_s, bs, fe, cur_local, -1);
 		__syncthreads();
 	}
 }
@@ -331,8 +357,9 @@ struct Batch {
 	int* d_status = nullptr;
 	int2* d_kr = nullptr;
 	PointRec* d_recs = nullptr;
-	unsigned* d_binmax = nullptr;               // spread bins' force statistics (FP32C)
-	unsigned long long* d_binsum = nullptr;
+	unsigned* d_binmax = nullptr;               // spread bins' force maxima (FP32C)
+	int* d_defer = nullptr;                     // deferred dense spread items: count, then the list
+	size_t defer_cap = 0;
 	// step parameters and graphs
 	double dt = 0.0, k = 0.0;
 	cudaStream_t cap_stream = nullptr;
@@ -385,9 +412,6 @@ ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved, int forces
 	if (forces) {
 		ibk_status st = cuda_check(cudaMemsetAsync(b.d_binmax, 0, sizeof(unsigned) * kMaxDims * (size_t) nbins, s),
 		                           "cudaMemsetAsync");
-		if (st == IBK_OK)
-			st = cuda_check(cudaMemsetAsync(b.d_binsum, 0, sizeof(unsigned long long) * kMaxDims * (size_t) nbins, s),
-			                "cudaMemsetAsync");
 		if (st != IBK_OK) return st;
 	}
 	batch_bin_count_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, forces,
@@ -395,8 +419,8 @@ ibk_status batch_bin(Batch& b, cudaStream_t s, int spread, int moved, int forces
 	const int nchunks = (nbins + kScanChunk - 1) / kScanChunk;
 	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, nbins);
 	bin_scan_kernel<<<nchunks, kScanThreads, 0, s>>>(b.d_counts, b.d_chunk, b.d_off, nbins, nchunks);
-	batch_bin_scatter_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, forces, b.d_kr,
-	                                                                      b.d_off, b.d_recs, b.d_binmax, b.d_binsum);
+	batch_bin_scatter_kernel<M, DIMS><<<b.grid_bin, kBinThreads, 0, s>>>(b.d_inst, t, spread, moved, b.d_kr,
+	                                                                      b.d_off, b.d_recs);
 	b.launches += 4;
 	return check_launch("batch binning");
 }
@@ -423,9 +447,19 @@ ibk_status batch_run_impl(Batch& b, int op, cudaStream_t s)
 		return check_launch("batch_interp_kernel");
 	};
 	auto spread = [&]() -> ibk_status {
+		Deferral defer{b.d_defer + 4, b.d_defer};
+		if (PREC == IBK_PRECISION_FP32C) {
+			ibk_status ds = cuda_check(cudaMemsetAsync(b.d_defer, 0, sizeof(int), s), "cudaMemsetAsync");
+			if (ds != IBK_OK) return ds;
+		}
 		batch_spread_kernel<D, DIMS, PREC><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
-			b.d_inst, t, b.d_next, b.d_recs, b.d_off, b.d_binmax, b.d_binsum, step ? 1 : 0);
+			b.d_inst, t, b.d_next, b.d_recs, b.d_off, b.d_binmax, step ? 1 : 0, defer);
 		b.launches += 1;
+		if (PREC == IBK_PRECISION_FP32C) {
+			batch_spread_dense_kernel<D, DIMS><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
+				b.d_inst, t, b.d_recs, b.d_off, b.d_binmax, step ? 1 : 0, defer.list, defer.count);
+			b.launches += 1;
+		}
 		return check_launch("batch_spread_kernel");
 	};
 	// FP32C spreads take the bins' force statistics from the binning
@@ -454,6 +488,11 @@ ibk_status batch_prepare_impl(Batch& b)
 	auto ks = batch_spread_kernel<D, DIMS, PREC>;
 	auto ki = batch_interp_kernel<D, DIMS, PREC>;
 	ibk_status st;
+	if constexpr (PREC == IBK_PRECISION_FP32C) {
+		if ((st = cuda_check(cudaFuncSetAttribute(batch_spread_dense_kernel<D, DIMS>,
+		                                          cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b.smem_s),
+		                     "cudaFuncSetAttribute")) != IBK_OK) return st;
+	}
 	if ((st = cuda_check(cudaFuncSetAttribute(ks, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b.smem_s),
 	                     "cudaFuncSetAttribute")) != IBK_OK) return st;
 	if ((st = cuda_check(cudaFuncSetAttribute(ki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b.smem_i),
@@ -598,7 +637,7 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		items_i += nitem_i[i];
 		if (bins_s >= (1LL << 30) || bins_i >= (1LL << 30) || items_s >= (1LL << 30) || items_i >= (1LL << 30))
 			return set_error(IBK_ERR_INVALID_ARGUMENT, "batch has too many tiles");
-		smem_max = std::max(smem_max, spread_tile_bytes(bi.ts, b.dims, b.precision));
+		smem_max = std::max(smem_max, spread_tile_bytes(bi.g, bi.ts, b.M, b.precision));
 		region_max = std::max(region_max, interp_region_bytes(bi.g, bi.ti, b.M));
 	}
 	const size_t smem_s = smem_max;
@@ -610,19 +649,26 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		// bin arrays sized for the larger bin space (counts start zeroed and
 		// every scan leaves them zeroed)
 		void** bufs[] = {reinterpret_cast<void**>(&b.d_counts), reinterpret_cast<void**>(&b.d_off),
-		                 reinterpret_cast<void**>(&b.d_chunk), reinterpret_cast<void**>(&b.d_binmax),
-		                 reinterpret_cast<void**>(&b.d_binsum)};
+		                 reinterpret_cast<void**>(&b.d_chunk), reinterpret_cast<void**>(&b.d_binmax)};
 		const size_t bytes[] = {sizeof(int) * nb, sizeof(int) * (nb + 1), sizeof(int) * (nb / kScanChunk + 2),
-		                        sizeof(unsigned) * kMaxDims * nb, sizeof(unsigned long long) * kMaxDims * nb};
+		                        sizeof(unsigned) * kMaxDims * nb};
 		b.bins_cap = 0;
-		for (int j = 0; j < 5; ++j) {
+		for (int j = 0; j < 4; ++j) {
 			if (*bufs[j]) cudaFree(*bufs[j]);
 			*bufs[j] = nullptr;
 		}
-		for (int j = 0; j < 5; ++j)
+		for (int j = 0; j < 4; ++j)
 			if ((st = cuda_check(cudaMalloc(bufs[j], bytes[j]), "cudaMalloc")) != IBK_OK) return st;
 		if ((st = cuda_check(cudaMemset(b.d_counts, 0, bytes[0]), "cudaMemset")) != IBK_OK) return st;
 		b.bins_cap = nb;
+	}
+	if (!b.d_defer || b.defer_cap < (size_t) items_s + 4) {
+		if (b.d_defer) cudaFree(b.d_defer);
+		b.d_defer = nullptr;
+		b.defer_cap = 0;
+		if ((st = cuda_check(cudaMalloc(reinterpret_cast<void**>(&b.d_defer), sizeof(int) * ((size_t) items_s + 4)),
+		                     "cudaMalloc")) != IBK_OK) return st;
+		b.defer_cap = (size_t) items_s + 4;
 	}
 	size_t cap = 0;
 	BatchInst* d_inst = nullptr;
@@ -663,7 +709,7 @@ void destroy(Batch* b)
 		if (b->h_ring[r]) cudaFreeHost(b->h_ring[r]);
 	}
 	void* bufs[] = {b->d_inst, b->d_table, b->d_counts, b->d_off, b->d_chunk, b->d_recs,
-	                b->d_next, b->d_status, b->d_kr, b->d_binmax, b->d_binsum};
+	                b->d_next, b->d_status, b->d_kr, b->d_binmax, b->d_defer};
 	for (void* p : bufs)
 		if (p) cudaFree(p);
 	if (b->cap_stream) cudaStreamDestroy(b->cap_stream);

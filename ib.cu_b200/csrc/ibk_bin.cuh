@@ -137,19 +137,15 @@ __device__ __forceinline__ int point_bin(const GridGeom& g, const TileGeom& tg, 
 	return tile * tg.nclass + cls;
 }
 
-// Force statistics of the bins (spread only), from which the FP32C spread
-// takes its per-tile fixed-point scale without a pass over its points:
-// binmax[bin * 3 + c] = largest |f| of the bin's points as FP32 bits (f =
-// FP32 res * F_c, the value the spread multiplies), binsum[bin * 3 + c] =
-// sum over the bin's points of ceil(1024 |f| / binmax) + 1, so that
-// binmax * binsum / 1024 bounds the bin's sum of |f|.  Both are integer
-// reductions, independent of the order of the atomics (the binning order is
-// not deterministic; these are).
+// Force statistics of the bins (spread only): binmax[bin * 3 + c] = the
+// largest |f| of the bin's points as FP32 bits (f = FP32 res * F_c, the value
+// the FP32C spread multiplies), from which a tile takes the largest term its
+// fixed point must hold.  An integer maximum: independent of the order of
+// the atomics (the binning order is not deterministic; this is).
 struct BinStats {
 	const double* f;        // forces (dims * n), nullptr: no statistics
 	double res;             // product of the resolutions (1 / h^dims)
 	unsigned* binmax;
-	unsigned long long* binsum;
 };
 
 template <int DIMS>
@@ -195,25 +191,6 @@ bin_count_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
 	const unsigned mask = __ballot_sync(0xffffffffu, active);
 	if (!active) return;
 	bin_rank<DIMS>(mask, key, count, key_rank + p, st.f != nullptr ? a : nullptr, st.binmax);
-}
-
-// The bin sums of the statistics for one point (after the count kernel has
-// completed the bin maxima); every lane of `mask` must call it.
-template <int DIMS>
-__device__ __forceinline__ void bin_sum(unsigned mask, int key, const float* a, const unsigned* __restrict__ binmax,
-                                        unsigned long long* __restrict__ binsum)
-{
-	const int lane = threadIdx.x & 31;
-	const unsigned peers = __match_any_sync(mask, key);
-	const int leader = __ffs(peers) - 1;
-#pragma unroll
-	for (int c = 0; c < DIMS; ++c) {
-		const unsigned mb = __ldg(binmax + (size_t) key * kMaxDims + c);
-		const float inv = mb ? 1024.0f / __uint_as_float(mb) : 0.0f;
-		const unsigned q = (unsigned) ceilf(a[c] * inv) + 1u;
-		const unsigned s = __reduce_add_sync(peers, q);
-		if (lane == leader) atomicAdd(binsum + (size_t) key * kMaxDims + c, (unsigned long long) s);
-	}
 }
 
 // Exclusive scan of the bin counts in two launches.  Each CTA owns a chunk
@@ -309,18 +286,10 @@ template <int M, int DIMS>
 __global__ void __launch_bounds__(256)
 bin_scatter_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const int2* __restrict__ key_rank, const int* __restrict__ offset,
-                   PointRec* __restrict__ recs, BinStats st)
+                   PointRec* __restrict__ recs)
 {
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
-	const bool active = p < n;
-	if (st.f != nullptr) {
-		const unsigned mask = __ballot_sync(0xffffffffu, active);
-		if (!active) return;
-		float a[kMaxDims] = {0.0f, 0.0f, 0.0f};
-		force_abs<DIMS>(st, n, p, a);
-		bin_sum<DIMS>(mask, __ldg(&key_rank[p].x), a, st.binmax, st.binsum);
-	}
-	if (!active) return;
+	if (p >= n) return;
 	const int2 kr = __ldg(key_rank + p);
 	PointRec r;
 	point_bin<M, DIMS>(g, tg, x, n, p, &r);

@@ -53,6 +53,7 @@ struct Plan {
 	ibk_grid_info info{};
 	int delta_kind = 0, delta_order = 0, precision = 0, tag = 0;
 	int device = 0;
+	int num_sms = 0;
 	int reserved_points = 0;
 	OpTable ops{};
 	Scratch scratch[8];
@@ -81,7 +82,7 @@ ibk_status launch(Plan& plan, const char* name, cudaStream_t stream, F&& body)
 
 // Scratch slots of a plan.
 enum { kSlotCount = 0, kSlotOffset = 1, kSlotKeyRank = 2, kSlotRecs = 3, kSlotChunk = 4, kSlotBinMax = 5,
-       kSlotSums = 6, kSlotBinSum = 7 };
+       kSlotSums = 6, kSlotDefer = 7 };
 
 // Largest tile extent in cells per axis (point records keep tile-relative
 // origins in 8 bits).
@@ -89,7 +90,7 @@ constexpr int kMaxTileExtent = 64;
 
 // Shared memory of a spread CTA for tiles tg, and of an interpolation CTA's
 // staged region (largest component, stencil width M), in bytes.
-size_t spread_tile_bytes(const TileGeom& tg, int dims, int precision);
+size_t spread_tile_bytes(const GridGeom& g, const TileGeom& tg, int M, int precision);
 size_t interp_region_bytes(const GridGeom& g, const TileGeom& tg, int M);
 // Staged interpolation region of component c relative to a tile's first
 // cell: lower corner and extent per axis (the TMA box).

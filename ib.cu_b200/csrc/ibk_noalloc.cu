@@ -131,14 +131,14 @@ ibk_status run(const GridGeom& g, int tag, int n, const double* x, ConstCompPtrs
 	if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
 	const int nb = (n + 255) / 256;
 	const int nchunks = (tg.num_bins + kScanChunk - 1) / kScanChunk;
-	const BinStats no_stats{nullptr, g.res, nullptr, nullptr};   // interpolation: no force statistics
+	const BinStats no_stats{nullptr, g.res, nullptr};   // interpolation: no force statistics
 	bin_count_kernel<M, DIMS><<<nb, 256, 0, stream>>>(g, tg, n, x, count, kr, no_stats);
 	if ((s = check_launch("bin_count_kernel")) != IBK_OK) return s;
 	bin_chunk_sum_kernel<<<nchunks, kScanThreads, 0, stream>>>(count, chunk, tg.num_bins);
 	if ((s = check_launch("bin_chunk_sum_kernel")) != IBK_OK) return s;
 	bin_scan_kernel<<<nchunks, kScanThreads, 0, stream>>>(count, chunk, off, tg.num_bins, nchunks);
 	if ((s = check_launch("bin_scan_kernel")) != IBK_OK) return s;
-	bin_scatter_kernel<M, DIMS><<<nb, 256, 0, stream>>>(g, tg, n, x, kr, off, recs, no_stats);
+	bin_scatter_kernel<M, DIMS><<<nb, 256, 0, stream>>>(g, tg, n, x, kr, off, recs);
 	if ((s = check_launch("bin_scatter_kernel")) != IBK_OK) return s;
 	const size_t smem = interp_smem_bytes<M>(g, tg);
 	auto kern = interp_tile_kernel<D, DIMS, PREC>;

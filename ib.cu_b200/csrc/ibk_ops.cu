@@ -1,4 +1,5 @@
 // Operator implementations and the (delta, dims, precision) dispatch table.
+#include <algorithm>
 #include <cstdio>
 #include <cstdint>
 #include <cuda.h>
@@ -59,19 +60,15 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, const Poi
 	int* chunk = static_cast<int*>(plan.scratch[kSlotChunk].ptr);
 	const GridGeom& g = *a.g;
 	const int nb = blocks_for(a.n, 256);
-	BinStats st{nullptr, g.res, nullptr, nullptr};
+	BinStats st{nullptr, g.res, nullptr};
 	if (f) {
 		const size_t nm = sizeof(unsigned) * kMaxDims * (size_t) tg.num_bins;
-		const size_t ns = sizeof(unsigned long long) * kMaxDims * (size_t) tg.num_bins;
 		if ((s = ensure_scratch(plan, kSlotBinMax, nm, a.stream)) != IBK_OK) return s;
-		if ((s = ensure_scratch(plan, kSlotBinSum, ns, a.stream)) != IBK_OK) return s;
 		st.f = f;
 		st.binmax = static_cast<unsigned*>(plan.scratch[kSlotBinMax].ptr);
-		st.binsum = static_cast<unsigned long long*>(plan.scratch[kSlotBinSum].ptr);
 		cudaError_t e = cudaMemsetAsync(st.binmax, 0, nm, a.stream);
-		if (e == cudaSuccess) e = cudaMemsetAsync(st.binsum, 0, ns, a.stream);
 		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
-		*stats_out = BinStatsView{st.binmax, st.binsum};
+		*stats_out = BinStatsView{st.binmax};
 	}
 	if ((s = launch(plan, "bin_count_kernel", a.stream, [&] {
 		bin_count_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, count, kr, st);
@@ -83,7 +80,7 @@ ibk_status bin_points(Plan& plan, const OpArgs& a, const TileGeom& tg, const Poi
 		bin_scan_kernel<<<nchunks, kScanThreads, 0, a.stream>>>(count, chunk, off, tg.num_bins, nchunks);
 	})) != IBK_OK) return s;
 	if ((s = launch(plan, "bin_scatter_kernel", a.stream, [&] {
-		bin_scatter_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, kr, off, recs, st);
+		bin_scatter_kernel<M, DIMS><<<nb, 256, 0, a.stream>>>(g, tg, a.n, a.x, kr, off, recs);
 	})) != IBK_OK) return s;
 	*recs_out = recs;
 	*off_out = off;
@@ -104,15 +101,35 @@ template <typename D, int DIMS, int PREC>
 ibk_status launch_spread(Plan& plan, const OpArgs& a, const TileGeom& tg, const PointRec* recs, const int* off,
                          BinStatsView bs, const double* fl, CompPtrs fe)
 {
-	const size_t smem = spread_smem_bytes(tg, DIMS, PREC);
+	const size_t smem = spread_smem_bytes(*a.g, tg, D::M, PREC);
 	auto kern = spread_tile_kernel<D, DIMS, PREC>;
 	ibk_status s = set_smem(kern, smem);
 	if (s != IBK_OK) return s;
-	// FP32C: one CTA per tile for every component; FP64: per (tile, component)
+	// FP32C: one CTA per tile for every component, dense tiles deferred to
+	// the folded kernel; FP64: per (tile, component)
+	Deferral defer{nullptr, nullptr};
+	if constexpr (PREC == IBK_PRECISION_FP32C) {
+		if ((s = ensure_scratch(plan, kSlotDefer, sizeof(int) * ((size_t) tg.num_tiles + 4), a.stream)) != IBK_OK)
+			return s;
+		defer.count = static_cast<int*>(plan.scratch[kSlotDefer].ptr);
+		defer.list = defer.count + 4;
+		cudaError_t e = cudaMemsetAsync(defer.count, 0, sizeof(int), a.stream);
+		if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+	}
 	const dim3 grid(tg.num_tiles, PREC == IBK_PRECISION_FP32C ? 1 : DIMS);
-	return launch(plan, "spread_tile_kernel", a.stream, [&] {
-		kern<<<grid, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, bs, fe);
-	});
+	if ((s = launch(plan, "spread_tile_kernel", a.stream, [&] {
+		kern<<<grid, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, bs, fe, defer);
+	})) != IBK_OK) return s;
+	if constexpr (PREC == IBK_PRECISION_FP32C) {
+		auto dense = spread_dense_kernel<D, DIMS>;
+		if ((s = set_smem(dense, smem)) != IBK_OK) return s;
+		const int gd = std::max(1, std::min(tg.num_tiles, 4 * plan.num_sms));
+		return launch(plan, "spread_dense_kernel", a.stream, [&] {
+			dense<<<gd, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, bs, fe, defer.list,
+			                                            defer.count);
+		});
+	}
+	return IBK_OK;
 }
 
 template <int KIND, int ORDER, int DIMS, int PREC>
@@ -122,7 +139,7 @@ ibk_status spread_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs f
 	if (!plan.tiled) return spread_direct<D, DIMS>(plan, a, fl, fe);
 	const PointRec* recs = nullptr;
 	const int* off = nullptr;
-	BinStatsView bs{nullptr, nullptr};
+	BinStatsView bs{nullptr};
 	constexpr bool fix = PREC == IBK_PRECISION_FP32C;
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off, fix ? fl : nullptr, &bs);
 	if (s != IBK_OK) return s;
@@ -233,7 +250,7 @@ ibk_status both_impl(Plan& plan, const OpArgs& a, const double* fl, CompPtrs fe,
 	}
 	const PointRec* recs = nullptr;
 	const int* off = nullptr;
-	BinStatsView bs{nullptr, nullptr};
+	BinStatsView bs{nullptr};
 	constexpr bool fix = PREC == IBK_PRECISION_FP32C;
 	ibk_status s = bin_points<D::M, DIMS>(plan, a, plan.spread_tiles, &recs, &off, fix ? fl : nullptr, &bs);
 	if (s != IBK_OK) return s;
@@ -324,9 +341,9 @@ TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
 	return tg;
 }
 
-size_t spread_tile_bytes(const TileGeom& tg, int dims, int precision)
+size_t spread_tile_bytes(const GridGeom& g, const TileGeom& tg, int M, int precision)
 {
-	return spread_smem_bytes(tg, dims, precision);
+	return spread_smem_bytes(g, tg, M, precision);
 }
 
 void interp_region(const GridGeom& g, const TileGeom& tg, int M, int c, int* lower, int* extent)

@@ -92,26 +92,16 @@ struct RangeTable {
 	int count;
 };
 
-// Per-bin force statistics of a grid's bins for the FP32C scale (see
-// BinStats), or null pointers.
+// The bins' force maxima of a grid for the FP32C scale (see BinStats), or
+// null.
 struct BinStatsView {
 	const unsigned* binmax;
-	const unsigned long long* binsum;
 };
-
-// The scale of each component from the statistics of the candidate bins:
-// every bin contributes its largest |f| and the bound binmax * binsum / 1024
-// on its sum of |f|; the scale is the largest power of two that keeps
-// max|w| * (sum bound) * scale below 2^kFixSumLog2 and max|w| * max|f| *
-// scale below 2^kFixTermLog2 (0 when the component's forces are all 0).
-template <int DIMS>
-__device__ __forceinline__ void bin_scales(unsigned* fm, double* sb, float wmax, float* scale);
 
 template <int DIMS>
 __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& tg, const int* tc,
                                              const int* __restrict__ off, RangeTable& rt,
-                                             BinStatsView bs = BinStatsView{nullptr, nullptr},
-                                             float wmax = 1.0f, float* scale = nullptr)
+                                             BinStatsView bs = BinStatsView{nullptr}, unsigned* fmax = nullptr)
 {
 	constexpr int nent = DIMS == 3 ? 125 : 25;
 	const int tid = threadIdx.x;
@@ -158,17 +148,23 @@ __device__ __forceinline__ void build_ranges(const GridGeom& g, const TileGeom& 
 			sbin = bin;
 		}
 	}
-	if (scale != nullptr) {
+	if (fmax != nullptr) {
+		// the largest |f| per component over the candidate bins (threads
+		// 0..127 hold one bin each, or none)
+		__shared__ unsigned part_m[4][kMaxDims];
 		unsigned fm[kMaxDims] = {0u, 0u, 0u};
-		double sb[kMaxDims] = {0.0, 0.0, 0.0};
-		if (sbin >= 0) {
+		if (sbin >= 0)
 #pragma unroll
-			for (int c = 0; c < DIMS; ++c) {
-				fm[c] = __ldg(bs.binmax + (size_t) sbin * kMaxDims + c);
-				sb[c] = (double) __uint_as_float(fm[c]) * (double) __ldg(bs.binsum + (size_t) sbin * kMaxDims + c);
+			for (int c = 0; c < DIMS; ++c) fm[c] = __ldg(bs.binmax + (size_t) sbin * kMaxDims + c);
+		if (tid < 128)
+#pragma unroll
+			for (int c = 0; c < kMaxDims; ++c) {
+				const unsigned m = __reduce_max_sync(0xffffffffu, fm[c]);
+				if ((tid & 31) == 0) part_m[tid >> 5][c] = m;
 			}
-		}
-		bin_scales<DIMS>(fm, sb, wmax, scale);
+		__syncthreads();
+		if (tid < kMaxDims)
+			fmax[tid] = max(max(part_m[0][tid], part_m[1][tid]), max(part_m[2][tid], part_m[3][tid]));
 	}
 	// compaction: slot = number of non-empty entries before this one, pref =
 	// exclusive sum of the lengths (the first 128 threads, 4 warps)
@@ -227,23 +223,30 @@ template <> struct SpreadAcc<IBK_PRECISION_FP64> { using type = double; };
 template <> struct SpreadAcc<IBK_PRECISION_FP32C> { using type = int; };
 
 // Fixed point of the FP32C spread.  Per (tile, component) a power-of-two
-// scale is chosen so that the sum of |term| over every candidate point of
-// the tile, max|w| * sum |res * F|, is at most 2^30 and every single |term|
-// below 2^22 (the sum of |F| is bounded exactly and order-independently by
-// the binning's per-bin statistics: see BinStats and bin_scales).  Each FP32
-// product is scaled, rounded once to an integer with the float magic number
-// 1.5 * 2^23 (x + magic carries rint(x) in its low mantissa bits for |x| <=
-// 2^22: an FFMA and an integer subtract, no conversion instruction) and added
-// to the face's 32-bit word with one integer shared atomic.  A face's final
-// sum is at most 2^30 + (candidates)/2 in magnitude, below 2^31, so it is
-// exact (intermediate wrap-around of the two's-complement word cancels) and
-// independent of the order in which points are visited (the binning order is
-// not deterministic; the result is); the only rounding is each product's
-// quantisation to the scale's unit.
+// scale is chosen so that every single |term| stays below 2^22, the largest
+// term being max|w| * max|f| over the candidate bins (the binning's bin
+// maxima, BinStats).  Each FP32 product is scaled, rounded once to an integer
+// with the float magic number 1.5 * 2^23 (x + magic carries rint(x) in its
+// low mantissa bits for |x| <= 2^22: an FFMA and an integer subtract, no
+// conversion instruction) and added to the face's 32-bit word with one
+// integer shared atomic.  A word holds the sum of up to kFoldChunk = 256
+// such terms exactly (|sum| < 2^30 + 128 < 2^31).  When an occupancy bound
+// shows that no face can receive more than 2 kFoldChunk terms
+// (window_occupancy: the common case) every component is summed in one pass,
+// the scale halved where the bound exceeds kFoldChunk; otherwise (very dense
+// tiles) the components are summed one at a time and the words are folded
+// into exact FP64 totals every kFoldChunk candidates.  Either way the sum is
+// exact and independent of the order in which points are visited (the
+// binning order is not deterministic; the result is); the only rounding is
+// each product's quantisation to 2^-22 (at most 2^-21 where halved) of the
+// tile's largest term.
 constexpr float kMagic = 12582912.0f;           // 1.5 * 2^23
 constexpr int kMagicBits = 0x4B400000;
 constexpr int kFixSumLog2 = 30;                 // bound on sum |term| * scale
 constexpr int kFixTermLog2 = 22;                // bound on one |term| * scale
+// Candidates summed into a 32-bit word between folds in the folded form
+// (kFoldChunk * 2^kFixTermLog2 = 2^kFixSumLog2).
+constexpr int kFoldChunk = 256;
 
 // The fixed-point increments of a0 * b and a1 * b (each rounded once), from
 // one packed two-lane FP32 FMA.
@@ -265,43 +268,136 @@ __device__ __forceinline__ int fix_term(float a, float b)
 	return __float_as_int(__fmaf_rn(a, b, kMagic)) - kMagicBits;
 }
 
-template <int DIMS>
-__device__ __forceinline__ void bin_scales(unsigned* fm, double* sb, float wmax, float* scale)
+// Occupancy bound of a spread tile: an upper bound on the number of
+// candidate points whose stencil can reach one face.  A point reaches face j
+// (tile-local, along each axis) only if its half-staggered origin lies in a
+// window of width W_d = M + (own-axis shift range) starting at
+// j + sh - M + 1 - dhi_d.  The candidates' origins are counted on a grid of
+// 2 x 2 x 2-cell blocks covering every window of the tile; a window spans at
+// most ceil(W_d / 2) + 1 blocks per axis, and the largest box sum of that
+// many blocks bounds the points reaching any face.  cnt: shared scratch of at
+// least occupancy_words() ints (the accumulators, before they are zeroed).
+// Every thread of the CTA calls it; the result is the same in every thread.
+template <int M>
+__host__ __device__ inline void occupancy_axis(const GridGeom& g, const TileGeom& tg, int d, int* A, int* nb, int* wb)
 {
-	// threads 0..127 hold one bin each (or nothing); fixed-order reduction,
-	// so the result does not depend on anything but the bin statistics
-	__shared__ unsigned part_m[4][kMaxDims];
-	__shared__ double part_s[4][kMaxDims];
-	const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-	if (threadIdx.x < 128) {
+	constexpr int sh = (M - 1) >> 1;
+	int dlo, dhi;
+	own_shift_range(g, tg.tag_mac, d, d, &dlo, &dhi);
+	const int W = M + dhi - dlo;                // window width in cells
+	*A = sh - M + 1 - dhi;                      // window start for face 0
+	*nb = (tg.T[d] + W - 1 + 1) >> 1;           // blocks covering every window
+	*wb = (W + 1) / 2 + 1;                      // blocks one window can span
+}
+
+// Largest value of cnt[0 .. vol) over the CTA (every thread gets it).
+template <int NT>
+__device__ __forceinline__ int block_max(const int* cnt, int vol)
+{
+	__shared__ int warp_best[NT / 32];
+	int best = 0;
+	for (int i = threadIdx.x; i < vol; i += NT) best = max(best, cnt[i]);
+	best = __reduce_max_sync(0xffffffffu, best);
+	if ((threadIdx.x & 31) == 0) warp_best[threadIdx.x >> 5] = best;
+	__syncthreads();
+	best = 0;
 #pragma unroll
-		for (int c = 0; c < DIMS; ++c) {
-			const unsigned m = __reduce_max_sync(0xffffffffu, fm[c]);
-			double v = sb[c];
-#pragma unroll
-			for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
-			if (lane == 0) { part_m[warp][c] = m; part_s[warp][c] = v; }
-		}
+	for (int w = 0; w < NT / 32; ++w) best = max(best, warp_best[w]);
+	__syncthreads();
+	return best;
+}
+
+// Box sums along one axis: out[i] = sum of in[i + k * stride], k < w, while
+// the line index (i / stride) % n + k stays below n.
+template <int NT>
+__device__ __forceinline__ void box_axis(const int* in, int* out, int vol, int stride, int n, int w)
+{
+	for (int i = threadIdx.x; i < vol; i += NT) {
+		const int pos = (i / stride) % n;
+		int sum = 0;
+		for (int k = 0; k < w && pos + k < n; ++k) sum += in[i + k * stride];
+		out[i] = sum;
 	}
 	__syncthreads();
-	if (threadIdx.x < kMaxDims) {
-		const int c = threadIdx.x;
-		float s = 0.0f;
-		if (c < DIMS) {
-			unsigned m = 0u;
-			double sum = 0.0;
-			for (int w = 0; w < 4; ++w) { m = max(m, part_m[w][c]); sum += part_s[w][c]; }
-			if (m != 0u) {
-				const double wm = (double) wmax * 1.001;
-				int ex_sum, ex_term;
-				frexp(sum * (1.0 / 1024.0) * wm, &ex_sum);             // bound on sum |term| < 2^ex_sum
-				frexp((double) __uint_as_float(m) * wm, &ex_term);    // bound on one |term| < 2^ex_term
-				const int k = min(kFixSumLog2 - ex_sum, kFixTermLog2 - ex_term);
-				s = ldexpf(1.0f, max(-126, min(k, 126)));
-			}
-		}
-		scale[c] = s;
+}
+
+// cnt: shared scratch of at least 2 occupancy_words() ints.
+template <int M, int DIMS, int NT>
+__device__ __forceinline__ int window_occupancy(const GridGeom& g, const TileGeom& tg, const RangeTable& rt, int ncand,
+                                                const PointRec* __restrict__ recs, int* cnt)
+{
+	int A0, A1, A2 = 0, N0, N1, N2 = 1, W0, W1, W2 = 1;
+	occupancy_axis<M>(g, tg, 0, &A0, &N0, &W0);
+	occupancy_axis<M>(g, tg, 1, &A1, &N1, &W1);
+	if (DIMS == 3) occupancy_axis<M>(g, tg, 2, &A2, &N2, &W2);
+	const int vol = N0 * N1 * N2;
+	for (int i = threadIdx.x; i < vol; i += NT) cnt[i] = 0;
+	__syncthreads();
+	int r = 0;
+	for (int it = threadIdx.x; it < ncand; it += NT) {
+		const int org = __ldg(&recs[range_walk(rt, r, it)].org);
+		const int sft = rt.shift[r];
+		const int q0 = rec_origin(org, 0) + unpack8(sft, 0) - A0;
+		const int q1 = rec_origin(org, 1) + unpack8(sft, 1) - A1;
+		const int q2 = DIMS == 3 ? rec_origin(org, 2) + unpack8(sft, 2) - A2 : 0;
+		const int b0 = q0 >> 1, b1 = q1 >> 1, b2 = q2 >> 1;
+		if (q0 >= 0 && q1 >= 0 && q2 >= 0 && b0 < N0 && b1 < N1 && b2 < N2)
+			atomicAdd(cnt + (b2 * N1 + b1) * N0 + b0, 1);
 	}
+	__syncthreads();
+	// a window covers at most W0 W1 W2 blocks: when even the fullest block
+	// times that stays within twice a fold chunk, the box sums are not needed
+	const int densest = block_max<NT>(cnt, vol);
+	if (densest * W0 * W1 * W2 <= 2 * kFoldChunk) return densest * W0 * W1 * W2;
+	int* tmp = cnt + vol;
+	box_axis<NT>(cnt, tmp, vol, 1, N0, W0);
+	box_axis<NT>(tmp, cnt, vol, N0, N1, W1);
+	if (DIMS == 3) {
+		box_axis<NT>(cnt, tmp, vol, N0 * N1, N2, W2);
+		return block_max<NT>(tmp, vol);
+	}
+	return block_max<NT>(cnt, vol);
+}
+
+// Ints of shared scratch window_occupancy needs for tiles tg.
+template <int M>
+__host__ __device__ inline size_t occupancy_words(const GridGeom& g, const TileGeom& tg)
+{
+	size_t v = 1;
+	for (int d = 0; d < g.dims; ++d) {
+		int A, nb, wb;
+		occupancy_axis<M>(g, tg, d, &A, &nb, &wb);
+		v *= (size_t) nb;
+	}
+	return 2 * v;     // the count grid and one buffer of box sums
+}
+
+__host__ __device__ inline size_t occupancy_words_rt(const GridGeom& g, const TileGeom& tg, int M)
+{
+	switch (M) {
+	case 2: return occupancy_words<2>(g, tg);
+	case 3: return occupancy_words<3>(g, tg);
+	case 4: return occupancy_words<4>(g, tg);
+	case 5: return occupancy_words<5>(g, tg);
+	default: return occupancy_words<6>(g, tg);
+	}
+}
+
+// The fixed-point scale of one component: the largest power of two with
+// (largest term) * scale < 2^kFixTermLog2 and, for the one-pass form, nmax
+// (largest term) * scale < 2^kFixSumLog2, the largest term being max|w| *
+// max|f| (0 when the component's forces are all 0).  nmax <= kFoldChunk
+// leaves the first bound the only one; up to 2 kFoldChunk costs at most one
+// bit.
+__device__ __forceinline__ float fix_scale(unsigned fmax_bits, float wmax, int nmax)
+{
+	if (fmax_bits == 0u) return 0.0f;
+	const double term = (double) __uint_as_float(fmax_bits) * (double) wmax * 1.001;
+	int ex_term, ex_sum;
+	frexp(term, &ex_term);                       // largest term < 2^ex_term
+	frexp(term * (double) max(nmax, 1), &ex_sum); // largest face sum < 2^ex_sum
+	const int k = min(kFixTermLog2 - ex_term, kFixSumLog2 - ex_sum);
+	return ldexpf(1.0f, max(-126, min(k, 126)));
 }
 
 // Shared-memory reduction (no return value) at a 32-bit shared address.
@@ -499,15 +595,106 @@ __device__ __forceinline__ void write_tile(double* __restrict__ out, const CompG
 	}
 }
 
+// Words of the FP32C spread's shared region before the scratch rows: the
+// accumulators of every component, or one component's words and FP64
+// totals (the folded form), or the occupancy grid, whichever is largest.
+template <int M, int DIMS>
+__host__ __device__ inline int spread_region_words(const GridGeom& g, const TileGeom& tg)
+{
+	const int words = spread_strides(tg.T[0], tg.T[1], tg.T[2], DIMS).words;
+	const int occ = (int) occupancy_words<M>(g, tg);
+	const int acc = words * (DIMS > 3 ? DIMS : 3);   // 3 words per face: every component, or words + totals
+	return acc > occ ? acc : occ;
+}
+
+// The folded FP32C form of a spread tile (tiles where a face may receive
+// more terms than a 32-bit word holds): one component at a time, kFoldChunk
+// candidates per round, after each round the words added exactly into FP64
+// totals (integers below 2^53) and cleared.  Every thread of the CTA calls
+// it, after s_scale is set.
+template <typename D, int DIMS, int NT>
+__device__ __forceinline__ void spread_tile_folded(const GridGeom& g, const TileGeom& tg, int n,
+                                                const double* __restrict__ fl, const PointRec* __restrict__ recs,
+                                                int pbase, const RangeTable& rt, int ncand, const int* lo,
+                                                const int* cells, const bool* wrap, bool wrap_any,
+                                                unsigned acc_addr, unsigned trash, const CompPtrs& fe,
+                                                const float* s_scale)
+{
+	extern __shared__ __align__(16) unsigned char smem_raw[];
+	const SpreadStrides ss = spread_strides(tg.T[0], tg.T[1], DIMS == 3 ? tg.T[2] : 1, DIMS);
+	int* words = reinterpret_cast<int*>(smem_raw + 4 * kGuardWords);
+	double* total = reinterpret_cast<double*>(words + ss.words);     // ss.words is a multiple of 4
+	for (int c = 0; c < DIMS; ++c) {
+		const CompGeom& cg = g.comp[c];
+		int e[3] = {1, 1, 1};
+#pragma unroll
+		for (int d = 0; d < DIMS; ++d) e[d] = min(tg.T[d], cg.points[d] - lo[d]);
+		for (int i = threadIdx.x; i < ss.words; i += NT) { words[i] = 0; total[i] = 0.0; }
+		__syncthreads();
+		const float sc = s_scale[c];
+		if (sc != 0.0f) {
+			int r = 0;
+			for (int chunk = 0; chunk < ncand; chunk += kFoldChunk) {
+				for (int it = chunk + threadIdx.x; it < min(ncand, chunk + kFoldChunk); it += NT) {
+					const PointRec rec = load_rec(recs + range_walk(rt, r, it));
+					const int sft = rt.shift[r];
+					const int p = rec.p - pbase;
+					int l[DIMS];
+					float dl[DIMS];
+#pragma unroll
+					for (int d = 0; d < DIMS; ++d) {
+						const bool own = tg.tag_mac && d == c;
+						l[d] = rec_origin(rec.org, d) + unpack8(sft, d) + (own ? rec_own_shift(rec.org, d) : 0);
+						dl[d] = own ? rec.dn[d] : rec.dh[d];
+					}
+					const float f = (float) (g.res * __ldg(fl + (size_t) c * n + p)) * sc;
+					if (!wrap_any) {
+						spread_fix<D, DIMS>(acc_addr, trash, l, dl, f, e, ss.S1, ss.S2);
+					} else {
+						float w[DIMS][D::M];
+#pragma unroll
+						for (int d = 0; d < DIMS; ++d) weights32<D>(dl[d], w[d]);
+						spread_wrapped<D, DIMS>(l, e, cells, wrap, ss.S1, ss.S2,
+							[&](int li, int v) { red_shared(acc_addr + 4u * (unsigned) li, v); },
+							[&](int m0, int m1, int m2) {
+								const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
+								return fix_term(w[0][m0] * f, w12);
+							});
+					}
+				}
+				__syncthreads();
+				for (int i = threadIdx.x; i < ss.words; i += NT) {
+					total[i] += (double) words[i];
+					words[i] = 0;
+				}
+				__syncthreads();
+			}
+		}
+		const double inv = sc != 0.0f ? 1.0 / (double) sc : 0.0;
+		write_tile<DIMS, NT>(fe.p[c], cg, lo, e, ss.S1, ss.S2, [&](int li) { return total[li] * inv; });
+		__syncthreads();
+	}
+}
+
 // One spread tile; every thread of the CTA calls it.  comp < 0: every
 // component (FP32C); else that component only (FP64).  Records carry point
 // indices offset by pbase (a batch numbers the points of all its instances
 // consecutively); off is this grid's bin table.
-template <typename D, int DIMS, int PREC, int NT = kTileThreads>
+// Dense tiles (FP32C tiles where a face may receive more terms than a
+// 32-bit word holds) are not summed by the one-pass kernel: it appends
+// defer_id to the deferral list and leaves the tile to the folded kernel,
+// which keeps the folded form out of the one-pass kernel's code.
+struct Deferral {
+	int* list;
+	int* count;
+};
+
+template <typename D, int DIMS, int PREC, bool FOLDED = false, int NT = kTileThreads>
 __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& tg, int n, const double* __restrict__ x,
                                             const double* __restrict__ fl, const PointRec* __restrict__ recs, int pbase,
                                             const int* __restrict__ off, BinStatsView bs, const CompPtrs& fe,
-                                            int tile, int comp)
+                                            int tile, int comp, Deferral defer = Deferral{nullptr, nullptr},
+                                            int defer_id = 0)
 {
 	using acc_t = typename SpreadAcc<PREC>::type;
 	constexpr int M = D::M;
@@ -532,7 +719,8 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		wrap[d] = !g.solid[d] && tg.ntiles[d] == 1;
 		wrap_any = wrap_any || wrap[d];
 	}
-	if constexpr (PREC == IBK_PRECISION_FP32C) build_ranges<DIMS>(g, tg, tc, off, rt, bs, max_weight<D, DIMS>(), s_scale);
+	__shared__ unsigned s_fmax[kMaxDims];
+	if constexpr (PREC == IBK_PRECISION_FP32C) build_ranges<DIMS>(g, tg, tc, off, rt, bs, s_fmax);
 	else build_ranges<DIMS>(g, tg, tc, off, rt);
 	const int ncand = rt.pref[rt.count];
 	if (ncand == 0) {
@@ -545,6 +733,30 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		}
 		return;
 	}
+	// shared words of the accumulators (FP32C: every component, or one
+	// component and its FP64 totals in the folded form) and the lanes'
+	// scratch rows after them
+	const int region = PREC == IBK_PRECISION_FP32C ? spread_region_words<M, DIMS>(g, tg) : ss.words;
+	const unsigned acc_addr = smem_addr(acc);
+	const unsigned trash = acc_addr + 4u * (unsigned) (region + (threadIdx.x & 31) * kTrashStride);
+	if constexpr (PREC == IBK_PRECISION_FP32C && FOLDED) {
+		if (threadIdx.x < kMaxDims) s_scale[threadIdx.x] = fix_scale(s_fmax[threadIdx.x], max_weight<D, DIMS>(), kFoldChunk);
+		spread_tile_folded<D, DIMS, NT>(g, tg, n, fl, recs, pbase, rt, ncand, lo, cells, wrap, wrap_any, acc_addr,
+		                                trash, fe, s_scale);
+		return;
+	}
+	if constexpr (PREC == IBK_PRECISION_FP32C && !FOLDED) {
+		// one pass unless a face may receive more than 2 kFoldChunk terms (the
+		// occupancy bound uses the accumulator memory before it is zeroed; a
+		// tile that wraps a periodic axis counts every candidate)
+		const int nmax = (ncand <= kFoldChunk || wrap_any)
+			? ncand : window_occupancy<M, DIMS, NT>(g, tg, rt, ncand, recs, reinterpret_cast<int*>(acc));
+		if (nmax > 2 * kFoldChunk) {
+			if (threadIdx.x == 0) defer.list[atomicAdd(defer.count, 1)] = defer_id;
+			return;
+		}
+		if (threadIdx.x < kMaxDims) s_scale[threadIdx.x] = fix_scale(s_fmax[threadIdx.x], max_weight<D, DIMS>(), nmax);
+	}
 	const int nwords = ss.words * (c_hi - c_lo);
 	for (int i = threadIdx.x * 4; i < nwords; i += NT * 4) {
 		if constexpr (PREC == IBK_PRECISION_FP32C) *reinterpret_cast<int4*>(acc + i) = make_int4(0, 0, 0, 0);
@@ -555,9 +767,6 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	}
 	__syncthreads();
 
-	const unsigned acc_addr = smem_addr(acc);
-	// this lane's scratch row, past the accumulators (FP32C)
-	const unsigned trash = acc_addr + 4u * (unsigned) (nwords + (threadIdx.x & 31) * kTrashStride);
 	int r = 0;
 	for (int it = threadIdx.x; it < ncand; it += NT) {
 		const int slot = range_walk(rt, r, it);
@@ -643,13 +852,18 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 }
 
 // Shared memory of a spread CTA: the accumulator words of the components it
-// covers (FP32C: every component, 4 bytes per face, and the lanes' scratch
-// rows; FP64: one component, 8 bytes per face).
-__host__ __device__ inline size_t spread_smem_bytes(const TileGeom& tg, int dims, int precision)
+// covers (FP32C: every component, 4 bytes per face, or the occupancy grid if
+// larger, and the lanes' scratch rows; FP64: one component, 8 bytes per
+// face).
+__host__ __device__ inline size_t spread_smem_bytes(const GridGeom& g, const TileGeom& tg, int M, int precision)
 {
+	const int dims = g.dims;
 	const size_t words = (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], dims).words;
-	return precision == IBK_PRECISION_FP32C ? (words * (size_t) dims + kTrashWords + kGuardWords) * 4
-	                                        : words * 8 + 4 * kGuardWords;
+	if (precision != IBK_PRECISION_FP32C) return words * 8 + 4 * kGuardWords;
+	// the region (accumulators, folded words and totals, or the occupancy
+	// grid), the lanes' scratch rows, the guard words
+	const size_t occ = occupancy_words_rt(g, tg, M), acc = words * 3;
+	return ((acc > occ ? acc : occ) + kTrashWords + kGuardWords) * 4;
 }
 
 // FP32C: 256-thread CTAs capped at 64 registers so that four fit on an SM
@@ -659,11 +873,28 @@ template <typename D, int DIMS, int PREC>
 __global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
 spread_tile_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
                    const double* __restrict__ fl, const PointRec* __restrict__ recs,
-                   const int* __restrict__ off, BinStatsView bs, CompPtrs fe)
+                   const int* __restrict__ off, BinStatsView bs, CompPtrs fe, Deferral defer)
 {
 	// grid: tiles (FP32C) or (tile, component) (FP64)
 	spread_tile<D, DIMS, PREC>(g, tg, n, x, fl, recs, 0, off, bs, fe, blockIdx.x,
-	                           PREC == IBK_PRECISION_FP32C ? -1 : (int) blockIdx.y);
+	                           PREC == IBK_PRECISION_FP32C ? -1 : (int) blockIdx.y, defer, blockIdx.x);
+}
+
+// The deferred dense tiles of an FP32C spread, folded (see Deferral); the
+// grid strides over the list, whose length the one-pass kernel left on the
+// device.
+template <typename D, int DIMS>
+__global__ void __launch_bounds__(kTileThreads, 4)
+spread_dense_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x,
+                    const double* __restrict__ fl, const PointRec* __restrict__ recs,
+                    const int* __restrict__ off, BinStatsView bs, CompPtrs fe, const int* __restrict__ list,
+                    const int* __restrict__ count)
+{
+	const int m = *count;
+	for (int k = blockIdx.x; k < m; k += gridDim.x) {
+		spread_tile<D, DIMS, IBK_PRECISION_FP32C, true>(g, tg, n, x, fl, recs, 0, off, bs, fe, __ldg(list + k), -1);
+		__syncthreads();
+	}
 }
 
 // ------------------------------------------------------------ interp ---

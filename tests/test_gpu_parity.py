@@ -332,3 +332,32 @@ def test_every_delta_fp32c(ibk, oracle, cuda, dims, delta):
     for c in range(dims):
         assert normwise(ul[c * n:(c + 1) * n], want[c * n:(c + 1) * n]) <= FP32C_TOL
         assert normwise(fe[c], want_fe[c]) <= FP32C_TOL
+
+
+@pytest.mark.parametrize("seed", [0, 1])
+def test_dense_tiles_fp32c_and_fp64(ibk, oracle, cuda, seed):
+    """Tiles where one face receives more terms than a 32-bit fixed-point word
+    holds (here about five points per cell on a 32^3 periodic grid, the
+    density of the ensemble's smallest grids) take the folded FP32C form; both
+    forms against the oracle, and the FP32C spread bit-identical run to run."""
+    rng = np.random.default_rng(500 + seed)
+    L = [0.8, 0.8, 0.8]                    # 32^3 cells at fd::mac{32}
+    g = oracle.geometry(3, L, [0, 0, 0], oracle.TAG_MAC, 32)
+    n = 160000
+    # points crowded onto a few spherical shells, as cell surfaces are
+    centres = rng.uniform(0.1, 0.7, size=(12, 3))
+    which = rng.integers(0, len(centres), n)
+    v = rng.normal(size=(n, 3))
+    v /= np.linalg.norm(v, axis=1)[:, None]
+    pts = centres[which] + 0.12 * v
+    x = np.ascontiguousarray(pts.T.reshape(-1))
+    f = rng.normal(size=3 * n)
+    want_fe, fa = oracle.spread(g, x, f, with_abs=True)
+    p64 = plan_for(ibk, 3, L, [0, 0, 0], 0, 32, 0, 3, ibk.FP64)
+    check_spread(device_spread(p64, x, f, cuda), want_fe, fa)
+    p32 = plan_for(ibk, 3, L, [0, 0, 0], 0, 32, 0, 3, ibk.FP32C)
+    a = device_spread(p32, x, f, cuda)
+    b = device_spread(p32, x, f, cuda)
+    for c in range(3):
+        assert normwise(a[c], want_fe[c]) <= FP32C_TOL
+        assert np.array_equal(a[c], b[c])
