@@ -242,3 +242,54 @@ def test_bind_beyond_capacity_is_rejected(ibk, cuda):
     with pytest.raises(ibk.IbkError) as e:
         batch.bind([c.io() for c in cases])
     assert e.value.status == 5
+
+
+def test_ensemble_instances_against_oracle(ibk, oracle, cuda):
+    """Eight instances of the 256-instance ensemble (cube grids from 32^3 to
+    128^3, dense and sparse) in one batch against the oracle: FP64
+    interpolation bit for bit and spread within 1e-12 * sum |res w F| per face
+    (the oracle's spread of |F|: bspline<3> weights are non-negative); FP32C
+    to the normwise bar."""
+    import torch
+    from ib_cu_b200 import workloads as W
+    every = W.ensemble(seed=0, count=256)
+    sides = [int(round(w.lengths[0] / 0.025)) for w in every]
+    pick = []
+    for side in (32, 48, 64, 96, 128):
+        pick += [i for i, s in enumerate(sides) if s == side][:2 if side in (32, 64, 128) else 1]
+    ws = [every[i] for i in pick]
+    insts = [ibk.Instance(ibk.Mac(w.refinement), _domain(ibk, w)) for w in ws]
+    total = sum(w.n for w in ws)
+    for precision in (ibk.FP64, ibk.FP32C):
+        batch = ibk.Batch(insts, ibk.Bspline(3), precision, max_points=total)
+        rng = np.random.default_rng(3)
+        io, ue_h = [], []
+        for i, w in enumerate(ws):
+            sizes = batch.sizes(i)
+            ue_h.append([rng.normal(size=s) for s in sizes])
+            io.append({"n": w.n, "x": _dev(w.x, cuda), "fl": _dev(w.f, cuda),
+                       "fe": [torch.full((s,), np.nan, dtype=torch.float64, device=cuda) for s in sizes],
+                       "ue": [_dev(u, cuda) for u in ue_h[-1]],
+                       "ul": torch.full((3 * w.n,), np.nan, dtype=torch.float64, device=cuda)})
+        batch.bind(io)
+        batch.run(ibk.OP_SPREAD_INTERPOLATE)
+        torch.cuda.synchronize()
+        for i, w in enumerate(ws):
+            g = oracle.geometry(3, w.lengths, w.boundaries, oracle.TAG_MAC, w.refinement)
+            want_fe = oracle.spread(g, w.x, w.f, threads=oracle.max_threads())
+            want_ul = oracle.interpolate(g, w.x, ue_h[i], threads=oracle.max_threads())
+            got_ul = io[i]["ul"].cpu().numpy()
+            if precision == ibk.FP64:
+                absum = oracle.spread(g, w.x, np.abs(w.f), threads=oracle.max_threads())
+                assert np.array_equal(got_ul, want_ul), i
+                for c in range(3):
+                    err = np.abs(io[i]["fe"][c].cpu().numpy() - want_fe[c])
+                    assert np.all(err <= 1e-12 * absum[c] + 1e-300), (i, c)
+            else:
+                for c in range(3):
+                    got = io[i]["fe"][c].cpu().numpy()
+                    assert np.abs(got - want_fe[c]).max() <= FP32C_TOL * np.abs(want_fe[c]).max(), (i, c)
+                    n = w.n
+                    ref = want_ul[c * n:(c + 1) * n]
+                    assert np.abs(got_ul[c * n:(c + 1) * n] - ref).max() <= FP32C_TOL * np.abs(ref).max(), (i, c)
+        del batch, io

@@ -145,3 +145,52 @@ def test_translation_by_one_cell_permutes_fp64(ibk, cuda):
         b = fe1[c].reshape(p[2], p[1], p[0])
         shifted = torch.roll(a, shifts=1, dims=2)
         assert float((shifted - b).abs().max()) <= 1e-12 * float(a.abs().max())
+
+
+def test_large_channel_fp64_against_oracle(ibk, oracle, cuda):
+    """The benchmark's 512 x 256 x 512 channel (10,923,000 points, walls in y)
+    through the plain FP64 path against the oracle on every host core:
+    interpolation bit for bit, spread within 1e-12 * sum |res w F| per face
+    (summation order only).  bspline<3> weights are non-negative, so that sum
+    is the oracle's spread of |F|.  The chosen FP32C form is held to its
+    normwise bar on the same inputs, and its error per face relative to
+    sum |res w F| is reported."""
+    import torch
+    from ib_cu_b200 import workloads as W
+    w = W.large_channel()
+    g = oracle.geometry(3, w.lengths, w.boundaries, oracle.TAG_MAC, w.refinement)
+    threads = oracle.max_threads()
+    p64, p32 = _plan(ibk, w, ibk.FP64), _plan(ibk, w, ibk.FP32C)
+    x, f = _dev(w.x, cuda), _dev(w.f, cuda)
+    sizes = p64.sizes()
+    rng = np.random.default_rng(9)
+    ue_h = [rng.normal(size=s) for s in sizes]
+    ue = [_dev(u, cuda) for u in ue_h]
+    fe = [torch.empty(s, dtype=torch.float64, device=cuda) for s in sizes]
+    ul = torch.empty(3 * w.n, dtype=torch.float64, device=cuda)
+    p64.spread_interpolate(w.n, x, f, fe, ue, ul)
+    got_fe = [a.cpu().numpy() for a in fe]
+    got_ul = ul.cpu().numpy()
+    p32.spread_interpolate(w.n, x, f, fe, ue, ul)
+    got32_fe = [a.cpu().numpy() for a in fe]
+    got32_ul = ul.cpu().numpy()
+    del fe, ul, ue, x, f
+    want_ul = oracle.interpolate(g, w.x, ue_h, threads=threads)
+    assert np.array_equal(got_ul, want_ul)
+    for c in range(3):
+        n = w.n
+        ref = want_ul[c * n:(c + 1) * n]
+        assert np.abs(got32_ul[c * n:(c + 1) * n] - ref).max() <= FP32C_TOL * np.abs(ref).max()
+    del want_ul
+    want_fe = oracle.spread(g, w.x, w.f, threads=threads)
+    absum = oracle.spread(g, w.x, np.abs(w.f), threads=threads)
+    for c in range(3):
+        err = np.abs(got_fe[c] - want_fe[c])
+        assert np.all(err <= 1e-12 * absum[c] + 1e-300)
+        e32 = np.abs(got32_fe[c] - want_fe[c])
+        assert e32.max() <= FP32C_TOL * np.abs(want_fe[c]).max()
+        touched = absum[c] > 0
+        rel = e32[touched] / absum[c][touched]
+        print(f"FP32C spread component {c}: error / sum|res w F| per face: "
+              f"max {rel.max():.3e}, p99 {np.percentile(rel, 99):.3e}, p50 {np.percentile(rel, 50):.3e} "
+              f"({touched.sum()} faces touched)")
