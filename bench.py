@@ -6,16 +6,18 @@
                     [--precision fp32c|fp64] [--no-cpu] [--no-extras]
                     [--leg all|batched|serving]
 
-One step = ibk_spread + ibk_interpolate over every Lagrangian point of the
-workload (spread overwrites all grid faces, interpolate writes every point
-velocity).  Metric: points per second through spread+interp, in the chosen
+One step = ibk_spread_interpolate over every Lagrangian point of the
+workload: one spread and one interpolation at the same positions, which bin
+the points once (spread overwrites all grid faces, interpolate writes every
+point velocity).  Metric: points per second through spread+interp, in the chosen
 FP32C form, with the plain FP64 path, its accuracy, p50/p99 step times, the
 end-to-end rate through host buffers and the CPU baseline in the same line.
 
 The same line also carries two legs (skipped with --no-extras, or run alone
 with --leg): "batched" -- 256 independent instances (cube grids 32^3..128^3,
-1-50 cells each) in one persistent graph-captured launch per operator, FP32C
-against the FP64 batch and against a loop of single plans; "serving" -- the
+1-50 cells each) in graph-captured persistent launches (spread and
+interpolation, one binning), FP32C against the FP64 batch and against a loop
+of single plans; "serving" -- the
 256 instances as device-resident members stepped (interpolate, advect, spring
 force, spread) under Poisson request arrivals from 1k to 50k steps/s, with
 p50/p99 latency per offered rate.
@@ -161,20 +163,13 @@ def algorithmic_bytes(n_points, faces):
     return 48 * n_points + 8 * faces
 
 
-# ------------------------------------------------------------ CPU legs
-class CpuSampler:
-    """The oracle's multi-threaded restatement of the reference algorithm
-    (spread + interpolate) timed on a bounded sample of workload `w`: the
-    first eighth of its points (whole cells) on the full grid.  The spread's
-    grid-sized passes (plane buffers, combine) do not shrink with the sample:
-    they are timed once with a one-point spread (median of three) and the
-    per-point remainder of the sampled spread is scaled to the full point
-    count; the interpolation has no grid-sized pass and scales directly.
-    Checked against a full run of the 512 x 256 x 512 channel on 16 host
-    threads (15.5 s spread + 13.1 s interpolation): the estimate lands
-    within about 15 %."""
+class CpuStep:
+    """One full spread + interpolate of the workload through the oracle's
+    multi-threaded restatement of the reference algorithm (every point, the
+    full grid), timed on the host cores: the CPU baseline and the reference
+    arm.  Nothing is sampled or scaled."""
 
-    def __init__(self, w, threads=0, frac=0.125):
+    def __init__(self, w, threads=0):
         from oracle import oracle as O
         from ib_cu_b200 import workloads as W
         O.build()
@@ -183,53 +178,35 @@ class CpuSampler:
         # every host CPU this process may run on: torchrun sets OMP_NUM_THREADS=1
         # per rank, which the oracle's explicit thread count overrides
         self.threads = threads or max(len(os.sched_getaffinity(0)), O.max_threads())
-        n = w.n
-        xs = w.x.reshape(w.dims, n)
-        fs = w.f.reshape(w.dims, n)
         sizes = [int(self.g.size[c]) for c in range(w.dims)]
         rng = np.random.default_rng(w.seed + 1)
         self.ue = [rng.normal(size=s_) * W.UM_PER_S for s_ in sizes]
-        self.ns = max(1, min(n, int(n * frac)))
-        self.x = np.ascontiguousarray(xs[:, :self.ns]).reshape(-1)
-        self.f = np.ascontiguousarray(fs[:, :self.ns]).reshape(-1)
         self.fe = [np.zeros(s_) for s_ in sizes]
-        x1 = np.ascontiguousarray(xs[:, :1]).reshape(-1)
-        f1 = np.ascontiguousarray(fs[:, :1]).reshape(-1)
-        grid = []
-        for _ in range(3):
-            t0 = time.perf_counter()
-            O.spread(self.g, x1, f1, fe=self.fe, threads=self.threads)
-            grid.append(time.perf_counter() - t0)
-        self.t_grid = statistics.median(grid)
 
     def step(self):
-        """Estimated seconds of one full-workload spread + interpolate."""
+        """Seconds of one full spread + interpolate."""
         O, w = self.O, self.w
         t0 = time.perf_counter()
-        O.spread(self.g, self.x, self.f, fe=self.fe, threads=self.threads)
-        t1 = time.perf_counter()
-        O.interpolate(self.g, self.x, self.ue, threads=self.threads)
-        t2 = time.perf_counter()
-        scale = w.n / self.ns
-        return self.t_grid + max(t1 - t0 - self.t_grid, 0.0) * scale + (t2 - t1) * scale
+        O.spread(self.g, w.x, w.f, fe=self.fe, threads=self.threads)
+        O.interpolate(self.g, w.x, self.ue, threads=self.threads)
+        return time.perf_counter() - t0
 
     def describe(self, steps):
-        return (f"oracle spread+interp (reference algorithm, {self.threads} threads) on the first "
-                f"{self.ns} of {self.w.n} points on the full grid; grid passes {self.t_grid:.3f} s "
-                f"(one-point spread, median of 3), per-point time scaled to {self.w.n} points; "
-                f"median of {steps}")
+        return (f"oracle spread+interp (reference algorithm, {self.threads} threads), the full workload "
+                f"({self.w.n} points, full grid), {steps} whole step(s) timed, median")
 
 
-def cpu_measure(w, seconds_budget=20.0, threads=0):
-    """CPU baseline of the main line: CpuSampler steps until seconds_budget
-    (at least two)."""
-    cs = CpuSampler(w, threads)
-    times, t_start = [], time.perf_counter()
-    while len(times) < 2 or (time.perf_counter() - t_start < seconds_budget and len(times) < 5):
-        times.append(cs.step())
-    t_full = statistics.median(times)
-    return {"value": w.n / t_full, "unit": "points/s", "cores": cs.threads, "kind": "port",
-            "sample": cs.describe(len(times)), "t_full_s": t_full, "t_grid_s": cs.t_grid}
+def cpu_measure(w, threads=0):
+    """CPU baseline of the main line: one whole oracle step of the workload."""
+    cs = CpuStep(w, threads)
+    t = cs.step()
+    return {"value": w.n / t, "unit": "points/s", "cores": cs.threads, "kind": "port",
+            "sample": cs.describe(1), "t_full_s": t}
+
+
+# Whole reference steps take about half a minute on the host cores: the arm
+# runs at most this many timed steps (and at most one warm-up step).
+REFERENCE_MAX_STEPS = 3
 
 
 def run_reference(args):
@@ -237,24 +214,26 @@ def run_reference(args):
     if rank != 0:
         return
     w = make_workload(args.workload)
-    cs = CpuSampler(w)
-    # warm-up + K timed steps, each one bounded sample of the workload
-    for _ in range(args.warmup):
+    cs = CpuStep(w)
+    for _ in range(min(args.warmup, 1)):
         cs.step()
-    times = [cs.step() for _ in range(args.steps)]
+    steps = max(1, min(args.steps, REFERENCE_MAX_STEPS))
+    times = [cs.step() for _ in range(steps)]
     t_full = statistics.median(times)
     v = w.n / t_full
     line = {
         "impl": "reference", "metric": METRIC, "value": v, "unit": "points/s",
-        "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1000.0 * t_full,
+        "n_gpus": args.gpus, "steps": steps, "steps_requested": args.steps, "warmup": min(args.warmup, 1),
+        "ms_per_step": 1000.0 * t_full,
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
         "data": "synthetic", "config": workload_config(w, "fp64"),
         "cpu_baseline": {"value": v, "unit": "points/s", "cores": cs.threads, "kind": "port",
-                         "sample": cs.describe(len(times))},
+                         "sample": cs.describe(steps)},
         "e2e": {"value": v, "unit": "points/s", "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
-        "note": ("the reference's GPU build does not compile with nvcc 12.9 (device lambdas in "
-                 "private members, legacy cuSPARSE API); this arm times the oracle's multi-threaded "
-                 "restatement of the reference algorithm on the host cores"),
+        "note": (f"whole steps of the full workload, capped at {REFERENCE_MAX_STEPS} timed steps and one "
+                 "warm-up (about half a minute each); the reference's GPU build does not compile with "
+                 "nvcc 12.9 (device lambdas in private members, legacy cuSPARSE API), so this arm times "
+                 "the oracle's multi-threaded restatement of the reference algorithm on the host cores"),
     }
     print(json.dumps(line), flush=True)
 
@@ -486,6 +465,24 @@ def run_ours(args):
         step()
         barrier()
         err = {"spread_max": 0.0, "spread_rms": 0.0, "interp_max": 0.0, "interp_rms": 0.0}
+        # per face: |err| / sum over the face's terms of |res w F| (the FP64
+        # spread of |F|: bspline<3> weights are non-negative)
+        fa64 = [torch.empty(s_, dtype=torch.float64, device=dev) for s_ in sizes]
+        plan64.spread(n, x, f.abs(), fa64, stream)
+        face = {}
+        for c in range(3):
+            touched = fa64[c] > 0
+            rel = ((fe[c] - fe64[c]).abs()[touched] / fa64[c][touched]).sort().values
+            big = fa64[c] >= 1e-6 * float(fa64[c].max())
+            rel_big = ((fe[c] - fe64[c]).abs()[big] / fa64[c][big]).sort().values
+            for key, r in (("all", rel), ("significant", rel_big)):
+                m = r.numel()
+                stats = {q: float(r[min(m - 1, int(q * m))]) for q in (0.5, 0.9, 0.99, 0.999)}
+                stats["max"] = float(r[-1])
+                prev = face.get(key)
+                face[key] = stats if prev is None else {k: max(prev[k], v) for k, v in stats.items()}
+            del rel, rel_big, touched, big
+        del fa64
         for c in range(3):
             ref_f = fe64[c]
             scale = float(ref_f.abs().max())
@@ -508,7 +505,13 @@ def run_ours(args):
         plain = {"value": world * n / (ms64 / 1000.0), "unit": "points/s", "ms_per_step": ms64,
                  "steps": k64, "speedup": ms64 / ms_step,
                  "accuracy_vs_fp64": {k: v for k, v in err.items()},
-                 "accuracy_note": "normwise: max|err|/max|ref| and rms(err)/rms(ref), worst component"}
+                 "accuracy_note": "normwise: max|err|/max|ref| and rms(err)/rms(ref), worst component",
+                 "spread_error_per_face": {
+                     "all_touched_faces": face["all"],
+                     "faces_with_sum_above_1e-6_of_max": face["significant"],
+                     "note": ("|err| / sum over the face's terms of |res w F|, quantiles over faces, worst "
+                              "component; a face reached only by far stencil tails sums to less than the "
+                              "fixed-point unit of its tile (2^-22 of the tile's largest term) and reads 0")}}
         # the reference's algorithm restated on the GPU, on the same inputs
         if world == 1:
             r = run_reference_gpu(ibk, w, plan64.info, x, f, ue)
@@ -532,7 +535,7 @@ def run_ours(args):
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
-        cpu = cpu_measure(w, seconds_budget=args.cpu_seconds)
+        cpu = cpu_measure(w)
         cpu = {k: cpu[k] for k in ("value", "unit", "cores", "kind", "sample")}
 
     if world > 1:
@@ -835,7 +838,6 @@ def main():
                     choices=["large-channel", "medium-channel", "channel", "single-rbc"])
     ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--cpu-seconds", type=float, default=20.0)
     ap.add_argument("--leg", choices=["all", "batched", "serving"], default="all",
                     help="batched / serving: run that leg alone (its own JSON line)")
     ap.add_argument("--no-extras", action="store_true",

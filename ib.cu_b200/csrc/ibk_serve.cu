@@ -463,7 +463,16 @@ ibk_status ibk_server_admit_from(ibk_server handle, int member, const char* path
 	for (int c = 0; c < s->dims && st == IBK_OK; ++c)
 		st = cuda_ok(cudaMemcpy(m.fe[c], grids[s->dims + c].data(), sizeof(double) * grids[s->dims + c].size(),
 		                        cudaMemcpyHostToDevice), "cudaMemcpy");
-	return st;
+	if (st != IBK_OK) {
+		// a member restored only in part is not left admitted: release it as
+		// retire does (nothing of it is in flight yet) and report the error
+		const std::string msg = ibk_last_error();
+		s->admitted_bytes -= m.bytes;
+		s->admitted_points -= m.n;
+		free_member(m);
+		return set_error(st, msg);
+	}
+	return IBK_OK;
 }
 
 ibk_status ibk_server_get_stats(ibk_server handle, ibk_server_stats* stats)

@@ -72,9 +72,17 @@ def build(force: bool = False) -> None:
         subprocess.run(["make", "-s", "-C", HERE, "libibk_oracle.so"], check=True)
 
 
-def build_ref() -> bool:
-    ref_root = os.environ.get("IBK_REFERENCE_ROOT", "/root/reference")
-    if not os.path.isdir(os.path.join(ref_root, "include", "ib")):
+def reference_root():
+    """Location of the sonwell/ib.cu tree: the IBK_REFERENCE_ROOT environment
+    variable, or None (no default location)."""
+    return os.environ.get("IBK_REFERENCE_ROOT") or None
+
+
+def build_ref(ref_root=None) -> bool:
+    """Compile the bridge from the reference tree at ref_root (default:
+    reference_root()); without a tree, report whether a bridge is built."""
+    ref_root = ref_root or reference_root()
+    if not ref_root or not os.path.isdir(os.path.join(ref_root, "include", "ib")):
         return os.path.exists(REF_PATH)
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={ref_root}"], check=True)
     return os.path.exists(REF_PATH)

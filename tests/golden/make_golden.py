@@ -2,7 +2,7 @@
 
 Run from the repository root where the sonwell/ib.cu tree is available:
 
-    python tests/golden/make_golden.py [--reference /root/reference]
+    python tests/golden/make_golden.py --reference <path of the sonwell/ib.cu tree>
 
 Stencil data (sort keys, stencil origins, fractional offsets, weights, spread
 and interpolation node indices) come from ``oracle/_ref/libibref.so``: the
@@ -69,12 +69,11 @@ def stencil_case(store, prefix, dims, L, solid, tag, ref, delta, order, x):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--reference", default="/root/reference")
+    ap.add_argument("--reference", required=True, help="path of the sonwell/ib.cu tree")
     ap.add_argument("--out", default=os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden.npz"))
     args = ap.parse_args()
-    os.environ["IBK_REFERENCE_ROOT"] = args.reference
     O.build()
-    if not O.build_ref() or O.ref() is None:
+    if not O.build_ref(args.reference) or O.ref() is None:
         sys.exit("reference bridge could not be built; fixtures need the reference tree")
     rng = np.random.default_rng(20261203)
     store = {}

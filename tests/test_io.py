@@ -51,10 +51,12 @@ def test_reads_fp32_containers_and_rejects_garbage(ibk, tmp_path):
         ibk.io_read(short)
 
 
-REF_DATA = "/root/reference/data"
+# the reference's data tables, where its tree is available (IBK_REFERENCE_ROOT)
+REF_DATA = os.path.join(os.environ.get("IBK_REFERENCE_ROOT", ""), "data")
 
 
-@pytest.mark.skipif(not os.path.isdir(REF_DATA), reason="reference data tables not present")
+@pytest.mark.skipif(not os.environ.get("IBK_REFERENCE_ROOT") or not os.path.isdir(REF_DATA),
+                    reason="reference data tables not present (set IBK_REFERENCE_ROOT)")
 @pytest.mark.parametrize("name,n", [("rbc.864.bin", 864), ("plt.386.bin", 386)])
 def test_reads_the_reference_data_tables(ibk, name, n):
     """The reference's sample-site tables (data/*.bin: n x 2 matrices of
