@@ -273,15 +273,10 @@ ibk_status ibk_plan_create(const ibk_domain* domain, int tag, int refinement, ib
 	if (gs != IBK_OK) { delete plan; return gs; }
 	const GridGeom& g = plan->g;
 	const ibk_grid_info& info = plan->info;
+	// both operators on the default tiles (16^3 cells, smaller on small
+	// grids), so one binning serves a spread and an interpolation
 	plan->tiles = make_tiles(g, tag, info.meshwidths);
-	{
-		// spread: 16^3 cells per tile (FP32C: 12 bytes of shared memory per
-		// face, 48 KB, four 256-thread CTAs per SM; FP64: 8 bytes per face).
-		// Measured on the 512 x 256 x 512 channel, 16^3 beats 32 x 16 x 8,
-		// 32 x 16 x 16 (512 threads) and 64 x 16 x 8.
-		const int spread_pref[3] = {16, 16, 16};
-		plan->spread_tiles = make_tiles(g, tag, info.meshwidths, spread_pref);
-	}
+	plan->spread_tiles = plan->tiles;
 	plan->tag = tag;
 	for (int d = 0; d < dims; ++d)
 		if (g.comp[0].cells[d] < info.meshwidths) plan->tiled = false;

@@ -252,11 +252,14 @@ batch_spread_dense_kernel(const BatchInst* __restrict__ insts, BatchTable t, con
 	__shared__ int cur_inst, cur_local;
 	const int m = *count, nact = __ldg(&t.hdr->num_active);
 	for (int q = blockIdx.x; q < m; q += gridDim.x) {
+		__shared__ int cur_comp;
 		if (threadIdx.x == 0) {
-			const int k = __ldg(list + q);
+			const int v = __ldg(list + q);
+			const int k = v >> 2;
 			const int j = find_instance(t.spre, nact, k);
 			cur_inst = __ldg(t.active + j);
 			cur_local = k - __ldg(t.spre + j);
+			cur_comp = v & 3;
 		}
 		__syncthreads();
 		copy_to_shared(&si, insts + cur_inst);
@@ -267,7 +270,7 @@ batch_spread_dense_kernel(const BatchInst* __restrict__ insts, BatchTable t, con
 		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
 		const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims};
 		spread_tile<D, DIMS, IBK_PRECISION_FP32C, true>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl,
-		                                                recs, so.pbase, off + si.bin_s, bs, fe, cur_local, -1);
+		                                                recs, so.pbase, off + si.bin_s, bs, fe, cur_local, cur_comp);
 		__syncthreads();
 	}
 }
@@ -625,8 +628,18 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 	for (int i = 0; i < b.count; ++i) {
 		BatchInst& bi = inst[i];
 		bi.g = b.geo[i];
-		bi.ts = make_tiles(bi.g, b.tag[i], b.M, cfg.spread_tile);
-		bi.ti = make_tiles(bi.g, b.tag[i], b.M, cfg.interp_tile);
+		// small grids take smaller tiles (at least four per axis, extents of
+		// at least 8 cells): the ensemble's small grids are its dense ones,
+		// and their work then spreads over more CTAs
+		int ext_s[3], ext_i[3];
+		for (int d = 0; d < 3; ++d) {
+			const int cells = d < b.dims ? bi.g.comp[0].cells[d] : 1;
+			const int cap = std::max(8, cells / 4);
+			ext_s[d] = std::min(cfg.spread_tile[d], cap);
+			ext_i[d] = std::min(cfg.interp_tile[d], cap);
+		}
+		bi.ts = make_tiles(bi.g, b.tag[i], b.M, ext_s);
+		bi.ti = make_tiles(bi.g, b.tag[i], b.M, ext_i);
 		bi.bin_s = (int) bins_s;
 		bi.bin_i = (int) bins_i;
 		bins_s += bi.ts.num_bins;
@@ -662,13 +675,15 @@ ibk_status configure(Batch& b, const ibk_batch_config& cfg)
 		if ((st = cuda_check(cudaMemset(b.d_counts, 0, bytes[0]), "cudaMemset")) != IBK_OK) return st;
 		b.bins_cap = nb;
 	}
-	if (!b.d_defer || b.defer_cap < (size_t) items_s + 4) {
+	// deferred dense items: one per (tile, component)
+	const size_t defer_want = (size_t) items_s * kMaxDims + 4;
+	if (!b.d_defer || b.defer_cap < defer_want) {
 		if (b.d_defer) cudaFree(b.d_defer);
 		b.d_defer = nullptr;
 		b.defer_cap = 0;
-		if ((st = cuda_check(cudaMalloc(reinterpret_cast<void**>(&b.d_defer), sizeof(int) * ((size_t) items_s + 4)),
+		if ((st = cuda_check(cudaMalloc(reinterpret_cast<void**>(&b.d_defer), sizeof(int) * defer_want),
 		                     "cudaMalloc")) != IBK_OK) return st;
-		b.defer_cap = (size_t) items_s + 4;
+		b.defer_cap = defer_want;
 	}
 	size_t cap = 0;
 	BatchInst* d_inst = nullptr;

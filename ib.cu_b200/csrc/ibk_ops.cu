@@ -109,7 +109,7 @@ ibk_status launch_spread(Plan& plan, const OpArgs& a, const TileGeom& tg, const 
 	// the folded kernel; FP64: per (tile, component)
 	Deferral defer{nullptr, nullptr};
 	if constexpr (PREC == IBK_PRECISION_FP32C) {
-		if ((s = ensure_scratch(plan, kSlotDefer, sizeof(int) * ((size_t) tg.num_tiles + 4), a.stream)) != IBK_OK)
+		if ((s = ensure_scratch(plan, kSlotDefer, sizeof(int) * ((size_t) tg.num_tiles * DIMS + 4), a.stream)) != IBK_OK)
 			return s;
 		defer.count = static_cast<int*>(plan.scratch[kSlotDefer].ptr);
 		defer.list = defer.count + 4;
@@ -123,7 +123,7 @@ ibk_status launch_spread(Plan& plan, const OpArgs& a, const TileGeom& tg, const 
 	if constexpr (PREC == IBK_PRECISION_FP32C) {
 		auto dense = spread_dense_kernel<D, DIMS>;
 		if ((s = set_smem(dense, smem)) != IBK_OK) return s;
-		const int gd = std::max(1, std::min(tg.num_tiles, 4 * plan.num_sms));
+		const int gd = std::max(1, std::min(tg.num_tiles * DIMS, 4 * plan.num_sms));
 		return launch(plan, "spread_dense_kernel", a.stream, [&] {
 			dense<<<gd, kTileThreads, smem, a.stream>>>(*a.g, tg, a.n, a.x, fl, recs, off, bs, fe, defer.list,
 			                                            defer.count);
@@ -296,8 +296,9 @@ const Entry kTable[] = {
 
 } // namespace
 
-// Tile extent per axis: the preferred extent (16 cells by default) where the
-// last tile keeps at least M cells (a stencil can then reach at most one
+// Tile extent per axis: the preferred extent (by default 16 cells, or a
+// quarter of a small axis, at least 8) where the last tile keeps at least M
+// cells (a stencil can then reach at most one
 // neighbour per side), otherwise the nearest size that does; an axis no
 // longer than the preferred extent is one tile.
 TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
@@ -310,7 +311,9 @@ TileGeom make_tiles(const GridGeom& g, int tag, int M, const int* pref_extent)
 		if (d >= g.dims) { tg.T[d] = 1; tg.ntiles[d] = 1; tg.cells[d] = 1; continue; }
 		const int cells = g.comp[0].cells[d];
 		tg.cells[d] = cells;
-		const int want = pref_extent ? pref_extent[d] : 16;
+		// default: 16 cells, but at least four tiles per axis on small grids
+		// (extents of at least 8), so their work spreads over more CTAs
+		const int want = pref_extent ? pref_extent[d] : std::min(16, std::max(8, cells / 4));
 		int T = cells;
 		if (cells > want) {
 			static const int prefs[] = {16, 14, 18, 12, 20, 10, 8, 9, 11, 13, 15, 17, 19};

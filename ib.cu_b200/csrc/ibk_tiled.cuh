@@ -608,7 +608,8 @@ __host__ __device__ inline int spread_region_words(const GridGeom& g, const Tile
 }
 
 // The folded FP32C form of a spread tile (tiles where a face may receive
-// more terms than a 32-bit word holds): one component at a time, kFoldChunk
+// more terms than a 32-bit word holds): components c_lo .. c_hi - 1 one at a
+// time (the folded kernel takes one component per item), kFoldChunk
 // candidates per round, after each round the words added exactly into FP64
 // totals (integers below 2^53) and cleared.  Every thread of the CTA calls
 // it, after s_scale is set.
@@ -618,13 +619,13 @@ __device__ __forceinline__ void spread_tile_folded(const GridGeom& g, const Tile
                                                 int pbase, const RangeTable& rt, int ncand, const int* lo,
                                                 const int* cells, const bool* wrap, bool wrap_any,
                                                 unsigned acc_addr, unsigned trash, const CompPtrs& fe,
-                                                const float* s_scale)
+                                                const float* s_scale, int c_lo, int c_hi)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
 	const SpreadStrides ss = spread_strides(tg.T[0], tg.T[1], DIMS == 3 ? tg.T[2] : 1, DIMS);
 	int* words = reinterpret_cast<int*>(smem_raw + 4 * kGuardWords);
 	double* total = reinterpret_cast<double*>(words + ss.words);     // ss.words is a multiple of 4
-	for (int c = 0; c < DIMS; ++c) {
+	for (int c = c_lo; c < c_hi; ++c) {
 		const CompGeom& cg = g.comp[c];
 		int e[3] = {1, 1, 1};
 #pragma unroll
@@ -682,8 +683,9 @@ __device__ __forceinline__ void spread_tile_folded(const GridGeom& g, const Tile
 // consecutively); off is this grid's bin table.
 // Dense tiles (FP32C tiles where a face may receive more terms than a
 // 32-bit word holds) are not summed by the one-pass kernel: it appends
-// defer_id to the deferral list and leaves the tile to the folded kernel,
-// which keeps the folded form out of the one-pass kernel's code.
+// (defer_id << 2) | c for each component c to the deferral list and leaves
+// the tile to the folded kernel, one component per item, which keeps the
+// folded form out of the one-pass kernel's code.
 struct Deferral {
 	int* list;
 	int* count;
@@ -742,7 +744,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 	if constexpr (PREC == IBK_PRECISION_FP32C && FOLDED) {
 		if (threadIdx.x < kMaxDims) s_scale[threadIdx.x] = fix_scale(s_fmax[threadIdx.x], max_weight<D, DIMS>(), kFoldChunk);
 		spread_tile_folded<D, DIMS, NT>(g, tg, n, fl, recs, pbase, rt, ncand, lo, cells, wrap, wrap_any, acc_addr,
-		                                trash, fe, s_scale);
+		                                trash, fe, s_scale, c_lo, c_hi);
 		return;
 	}
 	if constexpr (PREC == IBK_PRECISION_FP32C && !FOLDED) {
@@ -752,7 +754,8 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		const int nmax = (ncand <= kFoldChunk || wrap_any)
 			? ncand : window_occupancy<M, DIMS, NT>(g, tg, rt, ncand, recs, reinterpret_cast<int*>(acc));
 		if (nmax > 2 * kFoldChunk) {
-			if (threadIdx.x == 0) defer.list[atomicAdd(defer.count, 1)] = defer_id;
+			// one deferred item per component: (defer_id << 2) | component
+			if (threadIdx.x < DIMS) defer.list[atomicAdd(defer.count, 1)] = (defer_id << 2) | (int) threadIdx.x;
 			return;
 		}
 		if (threadIdx.x < kMaxDims) s_scale[threadIdx.x] = fix_scale(s_fmax[threadIdx.x], max_weight<D, DIMS>(), nmax);
@@ -892,7 +895,8 @@ spread_dense_kernel(GridGeom g, TileGeom tg, int n, const double* __restrict__ x
 {
 	const int m = *count;
 	for (int k = blockIdx.x; k < m; k += gridDim.x) {
-		spread_tile<D, DIMS, IBK_PRECISION_FP32C, true>(g, tg, n, x, fl, recs, 0, off, bs, fe, __ldg(list + k), -1);
+		const int v = __ldg(list + k);
+		spread_tile<D, DIMS, IBK_PRECISION_FP32C, true>(g, tg, n, x, fl, recs, 0, off, bs, fe, v >> 2, v & 3);
 		__syncthreads();
 	}
 }

@@ -293,6 +293,7 @@ def test_tile_decompositions(ibk, oracle, cuda, precision, lengths, solid, ref):
     rng = np.random.default_rng(21)
     g = oracle.geometry(3, lengths, solid, oracle.TAG_MAC, ref)
     plan = plan_for(ibk, 3, lengths, solid, 0, ref, 0, 3, precision)
+    plan.set_tiles([16, 16, 16], [16, 16, 16])    # the decompositions listed above
     assert [plan.info.cells[0][d] for d in range(3)] == [g.cells[0][d] for d in range(3)]
     n = 3000
     x = np.concatenate([rng.uniform(-0.1, l + 0.1, n) for l in lengths])
