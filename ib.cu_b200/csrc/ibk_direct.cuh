@@ -60,7 +60,6 @@ interp_direct_kernel(GridGeom g, int n, const double* __restrict__ x, ConstCompP
                      double* __restrict__ ul)
 {
 	using P = Pattern<D::M, DIMS, D::every_other>;
-	constexpr int M = D::M;
 	const int p = blockIdx.x * blockDim.x + threadIdx.x;
 	if (p >= n) return;
 	double z[DIMS];

@@ -417,14 +417,9 @@ __device__ __forceinline__ void red_row4(unsigned row, int t0, int t1, int t2, i
 	             :: "r"(row), "r"(t0), "r"(t1), "r"(t2), "r"(t3) : "memory");
 }
 
-// Per-lane scratch row that takes the reductions of stencil rows lying
-// outside the tile (cheaper than a branch around them): lane l's row starts
-// at word l * kTrashStride, an odd stride, so the lanes of one instruction
-// hit distinct banks.  The accumulators start kGuardWords after the dynamic
-// shared memory: a row's out-of-tile columns (zero terms) may fall up to
-// M - 1 words before the first row of the first component.
-constexpr int kTrashStride = 7;
-constexpr int kTrashWords = 32 * kTrashStride;
+// The accumulators start kGuardWords after the dynamic shared memory: a
+// row's out-of-tile columns (zero terms) may fall up to M - 1 words before
+// the first row of the first component.
 constexpr int kGuardWords = 8;
 
 // In-tile node mask of one axis: bit m set when node (j0 + m) lies in [0, e).
@@ -439,9 +434,10 @@ __device__ __forceinline__ unsigned axis_mask(int j0, int e)
 // component.  l: tile-local stencil origin per axis; dl: fractional offsets;
 // f: res * F * scale; e: faces of the tile per axis; acc: shared byte address
 // of the component's accumulator words (row stride S1, plane stride S2);
-// trash: this lane's scratch row.
+// Rows outside the tile are predicated off: their lanes issue no shared
+// access, so they add no bank traffic to the row's reductions.
 template <typename D, int DIMS>
-__device__ __forceinline__ void spread_fix(unsigned acc, unsigned trash, const int* l, const float* dl, float f,
+__device__ __forceinline__ void spread_fix(unsigned acc, const int* l, const float* dl, float f,
                                            const int* e, int S1, int S2)
 {
 	constexpr int M = D::M, sh = (M - 1) >> 1;
@@ -468,20 +464,21 @@ __device__ __forceinline__ void spread_fix(unsigned acc, unsigned trash, const i
 		const int m1 = r % M, m2 = r / M;
 		const unsigned rm = DIMS == 3 ? (mk[1] >> m1) & (mk[2] >> m2) & 1u : (mk[1] >> m1) & 1u;
 		const float w12 = DIMS == 3 ? w[1][m1] * w[2][m2] : w[1][m1];
-		// rows outside the tile go to this lane's scratch row
-		const unsigned row = rm ? base + 4u * (unsigned) (m1 * S1 + (DIMS == 3 ? m2 * S2 : 0)) : trash;
+		const unsigned row = base + 4u * (unsigned) (m1 * S1 + (DIMS == 3 ? m2 * S2 : 0));
 		if constexpr (M == 4) {
 			const int2 a = fix_terms2(w[0][0], w[0][1], w12);
 			const int2 b = fix_terms2(w[0][2], w[0][3], w12);
-			red_row4(row, a.x, a.y, b.x, b.y);
+			if (rm) red_row4(row, a.x, a.y, b.x, b.y);
 		} else {
 #pragma unroll
 			for (int m0 = 0; m0 + 1 < M; m0 += 2) {
 				const int2 t = fix_terms2(w[0][m0], w[0][m0 + 1], w12);
-				red_shared(row + 4u * m0, t.x);
-				red_shared(row + 4u * (m0 + 1), t.y);
+				if (rm) {
+					red_shared(row + 4u * m0, t.x);
+					red_shared(row + 4u * (m0 + 1), t.y);
+				}
 			}
-			if (M & 1) red_shared(row + 4u * (M - 1), fix_term(w[0][M - 1], w12));
+			if ((M & 1) && rm) red_shared(row + 4u * (M - 1), fix_term(w[0][M - 1], w12));
 		}
 	}
 }
@@ -595,18 +592,6 @@ __device__ __forceinline__ void write_tile(double* __restrict__ out, const CompG
 	}
 }
 
-// Words of the FP32C spread's shared region before the scratch rows: the
-// accumulators of every component, or one component's words and FP64
-// totals (the folded form), or the occupancy grid, whichever is largest.
-template <int M, int DIMS>
-__host__ __device__ inline int spread_region_words(const GridGeom& g, const TileGeom& tg)
-{
-	const int words = spread_strides(tg.T[0], tg.T[1], tg.T[2], DIMS).words;
-	const int occ = (int) occupancy_words<M>(g, tg);
-	const int acc = words * (DIMS > 3 ? DIMS : 3);   // 3 words per face: every component, or words + totals
-	return acc > occ ? acc : occ;
-}
-
 // The folded FP32C form of a spread tile (tiles where a face may receive
 // more terms than a 32-bit word holds): components c_lo .. c_hi - 1 one at a
 // time (the folded kernel takes one component per item), kFoldChunk
@@ -618,7 +603,7 @@ __device__ __forceinline__ void spread_tile_folded(const GridGeom& g, const Tile
                                                 const double* __restrict__ fl, const PointRec* __restrict__ recs,
                                                 int pbase, const RangeTable& rt, int ncand, const int* lo,
                                                 const int* cells, const bool* wrap, bool wrap_any,
-                                                unsigned acc_addr, unsigned trash, const CompPtrs& fe,
+                                                unsigned acc_addr, const CompPtrs& fe,
                                                 const float* s_scale, int c_lo, int c_hi)
 {
 	extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -650,7 +635,7 @@ __device__ __forceinline__ void spread_tile_folded(const GridGeom& g, const Tile
 					}
 					const float f = (float) (g.res * __ldg(fl + (size_t) c * n + p)) * sc;
 					if (!wrap_any) {
-						spread_fix<D, DIMS>(acc_addr, trash, l, dl, f, e, ss.S1, ss.S2);
+						spread_fix<D, DIMS>(acc_addr, l, dl, f, e, ss.S1, ss.S2);
 					} else {
 						float w[DIMS][D::M];
 #pragma unroll
@@ -735,16 +720,11 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 		}
 		return;
 	}
-	// shared words of the accumulators (FP32C: every component, or one
-	// component and its FP64 totals in the folded form) and the lanes'
-	// scratch rows after them
-	const int region = PREC == IBK_PRECISION_FP32C ? spread_region_words<M, DIMS>(g, tg) : ss.words;
 	const unsigned acc_addr = smem_addr(acc);
-	const unsigned trash = acc_addr + 4u * (unsigned) (region + (threadIdx.x & 31) * kTrashStride);
 	if constexpr (PREC == IBK_PRECISION_FP32C && FOLDED) {
 		if (threadIdx.x < kMaxDims) s_scale[threadIdx.x] = fix_scale(s_fmax[threadIdx.x], max_weight<D, DIMS>(), kFoldChunk);
 		spread_tile_folded<D, DIMS, NT>(g, tg, n, fl, recs, pbase, rt, ncand, lo, cells, wrap, wrap_any, acc_addr,
-		                                trash, fe, s_scale, c_lo, c_hi);
+		                                fe, s_scale, c_lo, c_hi);
 		return;
 	}
 	if constexpr (PREC == IBK_PRECISION_FP32C && !FOLDED) {
@@ -798,7 +778,7 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 				for (int d = 0; d < DIMS; ++d) dl[d] = (tg.tag_mac && d == c) ? rec.dn[d] : rec.dh[d];
 				const unsigned a = acc_addr + 4u * (unsigned) (ss.words * (c - c_lo));
 				if (!wrap_any) {
-					spread_fix<D, DIMS>(a, trash, l, dl, f, e, ss.S1, ss.S2);
+					spread_fix<D, DIMS>(a, l, dl, f, e, ss.S1, ss.S2);
 				} else {
 					float w[DIMS][M];
 #pragma unroll
@@ -856,17 +836,16 @@ __device__ __forceinline__ void spread_tile(const GridGeom& g, const TileGeom& t
 
 // Shared memory of a spread CTA: the accumulator words of the components it
 // covers (FP32C: every component, 4 bytes per face, or the occupancy grid if
-// larger, and the lanes' scratch rows; FP64: one component, 8 bytes per
-// face).
+// larger; FP64: one component, 8 bytes per face), after the guard words.
 __host__ __device__ inline size_t spread_smem_bytes(const GridGeom& g, const TileGeom& tg, int M, int precision)
 {
 	const int dims = g.dims;
 	const size_t words = (size_t) spread_strides(tg.T[0], tg.T[1], tg.T[2], dims).words;
 	if (precision != IBK_PRECISION_FP32C) return words * 8 + 4 * kGuardWords;
 	// the region (accumulators, folded words and totals, or the occupancy
-	// grid), the lanes' scratch rows, the guard words
+	// grid) and the guard words
 	const size_t occ = occupancy_words_rt(g, tg, M), acc = words * 3;
-	return ((acc > occ ? acc : occ) + kTrashWords + kGuardWords) * 4;
+	return ((acc > occ ? acc : occ) + kGuardWords) * 4;
 }
 
 // FP32C: 256-thread CTAs capped at 64 registers so that four fit on an SM
