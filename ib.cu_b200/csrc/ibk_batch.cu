@@ -46,8 +46,8 @@ struct BatchIO {
 	int n, pbase;           // points; index of the first point in the batch numbering
 	const double* x;
 	const double* fl;
-	double* fe[kMaxDims];
-	const double* ue[kMaxDims];
+	CompPtrs fe;            // kernels pass the shared copy by reference, so the
+	ConstCompPtrs ue;       // component index never addresses a local array
 	double* ul;
 	double* xn;
 	const double* xref;
@@ -223,9 +223,7 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		copy_to_shared(&si, insts + inst);
 		copy_to_shared(&so, t.io + inst);
 		__syncthreads();
-		CompPtrs fe;
-#pragma unroll
-		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
+		const CompPtrs& fe = so.fe;
 		if constexpr (PREC == IBK_PRECISION_FP32C) {
 			const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims};
 			// a dense tile is deferred by its work-item index
@@ -265,9 +263,7 @@ batch_spread_dense_kernel(const BatchInst* __restrict__ insts, BatchTable t, con
 		copy_to_shared(&si, insts + cur_inst);
 		copy_to_shared(&so, t.io + cur_inst);
 		__syncthreads();
-		CompPtrs fe;
-#pragma unroll
-		for (int c = 0; c < kMaxDims; ++c) fe.p[c] = so.fe[c];
+		const CompPtrs& fe = so.fe;
 		const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims};
 		spread_tile<D, DIMS, IBK_PRECISION_FP32C, true>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl,
 		                                                recs, so.pbase, off + si.bin_s, bs, fe, cur_local, cur_comp);
@@ -300,9 +296,7 @@ batch_interp_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		__syncthreads();
 		if (step && threadIdx.x == 0) epi = StepEpilogue{so.xn, so.fs, so.xref, dt, k};
 		__syncthreads();
-		ConstCompPtrs ue;
-#pragma unroll
-		for (int c = 0; c < kMaxDims; ++c) ue.p[c] = so.ue[c];
+		const ConstCompPtrs& ue = so.ue;
 		const bool ok = interp_tile<D, DIMS, PREC>(si.g, si.ti, so.n, so.x, recs, so.pbase, off + si.bin_i, ue,
 		                                           so.ul, t.maps + (size_t) inst * kMaxDims,
 		                                           __ldg(t.use_tma + inst), true, status,
@@ -567,11 +561,11 @@ bool instance_maps(Batch& b, int i, const BatchIO& o)
 	bool ok = true;
 	for (int c = 0; c < b.dims; ++c) {
 		const size_t k = (size_t) i * kMaxDims + c;
-		if (b.map_ptr[k] != o.ue[c]) {
+		if (b.map_ptr[k] != o.ue.p[c]) {
 			int lower[3], box[3];
 			interp_region(bi.g, bi.ti, b.M, c, lower, box);
-			b.map_ok[k] = o.ue[c] && grid_tensor_map(&b.map_cache[k], o.ue[c], bi.g.comp[c], b.dims, box);
-			b.map_ptr[k] = o.ue[c];
+			b.map_ok[k] = o.ue.p[c] && grid_tensor_map(&b.map_cache[k], o.ue.p[c], bi.g.comp[c], b.dims, box);
+			b.map_ptr[k] = o.ue.p[c];
 		}
 		ok = ok && b.map_ok[k];
 	}
@@ -740,12 +734,12 @@ ibk_status check_bound(const Batch& b, int op)
 		if (o.n == 0) continue;
 		bool ok = o.x != nullptr;
 		if (op == IBK_OP_SPREAD || op == IBK_OP_STEP)
-			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe[c] != nullptr;
+			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe.p[c] != nullptr;
 		if (op == IBK_OP_SPREAD_INTERPOLATE)
-			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe[c] != nullptr;
+			for (int c = 0; c < b.dims; ++c) ok = ok && o.fe.p[c] != nullptr;
 		if (op == IBK_OP_SPREAD || op == IBK_OP_SPREAD_INTERPOLATE) ok = ok && o.fl != nullptr;
 		if (op == IBK_OP_INTERPOLATE || op == IBK_OP_STEP || op == IBK_OP_SPREAD_INTERPOLATE)
-			for (int c = 0; c < b.dims; ++c) ok = ok && o.ue[c] != nullptr;
+			for (int c = 0; c < b.dims; ++c) ok = ok && o.ue.p[c] != nullptr;
 		if (op == IBK_OP_INTERPOLATE || op == IBK_OP_SPREAD_INTERPOLATE) ok = ok && o.ul != nullptr;
 		if (op == IBK_OP_STEP) ok = ok && o.xn && o.xref && o.fs;
 		if (!ok)
@@ -877,7 +871,7 @@ ibk_status ibk_batch_bind(ibk_batch handle, const ibk_instance_io* io, void* str
 		t.pbase = (int) total;
 		t.x = s.x;
 		t.fl = s.fl;
-		for (int c = 0; c < kMaxDims; ++c) { t.fe[c] = s.fe[c]; t.ue[c] = s.ue[c]; }
+		for (int c = 0; c < kMaxDims; ++c) { t.fe.p[c] = s.fe[c]; t.ue.p[c] = s.ue[c]; }
 		t.ul = s.ul;
 		t.xn = s.xn;
 		t.xref = s.xref;

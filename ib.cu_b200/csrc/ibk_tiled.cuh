@@ -902,11 +902,16 @@ __host__ __device__ inline void region_axis(int T, int dlo, int dhi, bool x_axis
 template <int M>
 __host__ __device__ inline void region_of(const GridGeom& g, const TileGeom& tg, int c, int* lower, int* extent)
 {
-	for (int d = 0; d < kMaxDims; ++d) { lower[d] = 0; extent[d] = 1; }
-	for (int d = 0; d < g.dims; ++d) {
-		int dlo, dhi;
-		own_shift_range(g, tg.tag_mac, c, d, &dlo, &dhi);
-		region_axis<M>(tg.T[d], dlo, dhi, d == 0, &lower[d], &extent[d]);
+	// axes at compile-time indices (the arrays stay in registers)
+#pragma unroll
+	for (int d = 0; d < kMaxDims; ++d) {
+		lower[d] = 0;
+		extent[d] = 1;
+		if (d < g.dims) {
+			int dlo, dhi;
+			own_shift_range(g, tg.tag_mac, c, d, &dlo, &dhi);
+			region_axis<M>(tg.T[d], dlo, dhi, d == 0, &lower[d], &extent[d]);
+		}
 	}
 }
 
@@ -1061,8 +1066,9 @@ __device__ __forceinline__ bool interp_tile(const GridGeom& g, const TileGeom& t
 		if (!tma_ok) return false;
 		if (threadIdx.x == 0) mbar_inval(&bar);   // every thread is past the wait
 		if (!interior) {
-			// out-of-range slabs: wrap periodic, clamp solid (interpolate.h:16-22)
-#pragma unroll 1
+			// out-of-range slabs: wrap periodic, clamp solid (interpolate.h:16-22);
+			// the axis loop is unrolled so that the extents stay in registers
+#pragma unroll
 			for (int d = 0; d < DIMS; ++d) {
 				const int below = max(0, -rlo[d]);
 				const int above_from = min(E[d], cg.points[d] - rlo[d]);
