@@ -187,7 +187,7 @@ ibk_status ibk_plan_check(ibk_plan plan);
  * does not own the device's memory pool, a real-time loop where an
  * allocation would synchronise the device, a host that keeps no plan.  Same
  * arguments and result as ibk_interpolate, with the grid described directly
- * instead of by a plan.  Its scratch is one fixed array of about 8 MB that
+ * instead of by a plan.  Its scratch is one fixed array of about 22 MB that
  * every GPU loading this library holds until exit; calls beyond 524288
  * points, or grids needing more than 262144 bins (tiles x 3^dims), return
  * IBK_ERR_CAPACITY.  All calls share that array, so calls that overlap on the
