@@ -4,7 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload large-channel|medium-channel|channel|single-rbc]
                     [--precision fp32c|fp64] [--no-cpu] [--no-extras]
-                    [--leg all|batched|serving]
+                    [--leg all|batched|serving|membrane]
 
 One step = ibk_spread_interpolate over every Lagrangian point of the
 workload: one spread and one interpolation at the same positions, which bin
@@ -13,14 +13,17 @@ point velocity).  Metric: points per second through spread+interp, in the chosen
 FP32C form, with the plain FP64 path, its accuracy, p50/p99 step times, the
 end-to-end rate through host buffers and the CPU baseline in the same line.
 
-The same line also carries two legs (skipped with --no-extras, or run alone
-with --leg): "batched" -- 256 independent instances (cube grids 32^3..128^3,
+The same line also carries three legs (skipped with --no-extras, or run
+alone with --leg): "batched" -- 256 independent instances (cube grids 32^3..128^3,
 1-50 cells each) in graph-captured persistent launches (spread and
 interpolation, one binning), FP32C against the FP64 batch and against a loop
 of single plans; "serving" -- the
 256 instances as device-resident members stepped (interpolate, advect, spring
 force, spread) under Poisson request arrivals from 1k to 50k steps/s, with
-p50/p99 latency per offered rate.
+p50/p99 latency per offered rate; "membrane" -- the producers of the point
+forces, for 64 shapes of the reference's RBC discretisation (2500 data sites,
+10000 samples): surface geometry (FP64 operator products, normals, patch
+areas) and the Skalak tension, per step.
 
 Default workload: the large channel, 128 x 64 x 128 um, MAC grid 512 x 256 x
 512 (h = 0.25 um), 3300 RBCs x 2210 points + 6000 platelets x 605 points =
@@ -264,10 +267,12 @@ def run_ours(args):
     ibk.lib()
     from ib_cu_b200 import workloads as W
 
-    if args.leg in ("batched", "serving"):
+    if args.leg in ("batched", "serving", "membrane"):
         # one leg alone (profiling runs): its own JSON object
         if args.leg == "batched":
             res = run_batched(ibk, W, dev, seed=0, steps=max(5, args.steps), rank=rank, world=world)
+        elif args.leg == "membrane":
+            res = run_membrane(ibk, dev, steps=max(5, args.steps))
         else:
             res = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
         if rank == 0:
@@ -533,6 +538,7 @@ def run_ours(args):
         torch.cuda.empty_cache()
         extras["batched"] = run_batched(ibk, W, dev, seed=0, steps=max(5, args.steps // 2), rank=rank, world=world)
         extras["serving"] = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
+        extras["membrane"] = run_membrane(ibk, dev, steps=max(5, args.steps // 2))
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -795,6 +801,61 @@ def run_batched(ibk, W, dev, seed, steps, rank=0, world=1):
     return out
 
 
+def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
+    """Membrane forces of nc shapes with the reference's RBC discretisation
+    (rbc{2500, 10000}: 2500 data sites, 10000 sample sites,
+    test/ib-whole.cc:233): per step the current geometry (six FP64 operator
+    products of ns x nd operators with the 3*nc position columns, then the
+    per-sample normal and patch area) and the Skalak tension from it and the
+    rest geometry (computed once), then the bending force (the curvature field
+    at the data sites through the data-site operators, its derivatives at the
+    samples).  Random operators and positions of the reference's shapes: the
+    timing does not depend on their values."""
+    import torch
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(11)
+    ops = [torch.randn(ns, nd, generator=gen, dtype=torch.float64, device=dev) / nd for _ in range(6)]
+    wts = torch.rand(ns, generator=gen, dtype=torch.float64, device=dev) + 0.5
+    plan = ibk.SurfacePlan(ops, wts)
+    dops = [None] + [torch.randn(nd, nd, generator=gen, dtype=torch.float64, device=dev) / nd for _ in range(5)]
+    dplan = ibk.SurfacePlan(dops, torch.rand(nd, generator=gen, dtype=torch.float64, device=dev) + 0.5)
+    del ops, dops
+    x0 = torch.randn(3 * nd * nc, generator=gen, dtype=torch.float64, device=dev)
+    x1 = x0 + 0.01 * torch.randn(3 * nd * nc, generator=gen, dtype=torch.float64, device=dev)
+    rest = plan.geometry(x0, nc)
+    stream = torch.cuda.current_stream()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
+    geo_ms, ten_ms, ben_ms = [], [], []
+    for it in range(warmup + steps):
+        ev[0].record(stream)
+        cur = plan.geometry(x1, nc)
+        ev[1].record(stream)
+        f = ibk.membrane_tension(ibk.SKALAK, 0.25, 25.0, rest, cur)
+        ev[2].record(stream)
+        fb = ibk.membrane_bending(dplan, plan, 1.0, False, None, x1, None, cur, nc)
+        ev[3].record(stream)
+        torch.cuda.synchronize()
+        if it >= warmup:
+            geo_ms.append(ev[0].elapsed_time(ev[1]))
+            ten_ms.append(ev[1].elapsed_time(ev[2]))
+            ben_ms.append(ev[2].elapsed_time(ev[3]))
+        del cur, f, fb
+    g, t, b = float(np.median(geo_ms)), float(np.median(ten_ms)), float(np.median(ben_ms))
+    bflops = (5 * 2.0 * nd * nd * 3 * nc) + (5 * 2.0 * ns * nd * nc)
+    flops = 6 * 2.0 * ns * nd * 3 * nc
+    tbytes = (2 * 15 + 1 + 3) * 8.0 * ns * nc     # rest t, tt and area + current t, tt read; f written
+    peak, _ = measured_peaks()
+    del plan, dplan, rest
+    torch.cuda.empty_cache()
+    return {"shapes": nc, "data_sites": nd, "samples": ns, "law": "skalak", "steps": steps,
+            "ms_per_step": g + t + b, "geometry_ms": g, "tension_ms": t, "bending_ms": b,
+            "bending_gemm_tflops": bflops / (b * 1e-3) / 1e12,
+            "geometry_tflops": flops / (g * 1e-3) / 1e12,
+            "tension_gbs": tbytes / (t * 1e-3) / 1e9, "tension_frac_of_hbm": tbytes / (t * 1e-3) / 1e9 / peak,
+            "note": "FP64: operator products as library DGEMMs, normal / area and tension as hand-written "
+                    "kernels; median of the timed steps, CUDA events"}
+
+
 def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=4):
     """Serving sweep: 256 ensemble members resident on the device, Poisson
     step requests (interpolate, advect dt = 1 us, spring k = 1 pN/um,
@@ -839,8 +900,8 @@ def main():
                     choices=["large-channel", "medium-channel", "channel", "single-rbc"])
     ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--leg", choices=["all", "batched", "serving"], default="all",
-                    help="batched / serving: run that leg alone (its own JSON line)")
+    ap.add_argument("--leg", choices=["all", "batched", "serving", "membrane"], default="all",
+                    help="batched / serving / membrane: run that leg alone (its own JSON line)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched (256 instances) and serving legs")
     args = ap.parse_args()

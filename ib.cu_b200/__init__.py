@@ -37,6 +37,7 @@ PERIODIC, SOLID = 0, 1
 TAG_MAC, TAG_CENTERED = 0, 1
 BSPLINE, PESKIN, ROMA, COSINE, HAT = 0, 1, 2, 3, 4
 FP64, FP32C = 0, 1
+SKALAK, NEOHOOKEAN = 0, 1          # ibk_tension_law
 
 # Every symbol include/ibk.h declares (checked by the CPU test suite).
 ABI_SYMBOLS = (
@@ -52,6 +53,8 @@ ABI_SYMBOLS = (
     "ibk_server_read", "ibk_server_get_stats", "ibk_server_reset_stats", "ibk_server_run_poisson",
     "ibk_server_save", "ibk_server_admit_from",
     "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
+    "ibk_surface_plan_create", "ibk_surface_plan_destroy", "ibk_surface_geometry", "ibk_membrane_tension",
+    "ibk_membrane_bending",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
 OP_SPREAD, OP_INTERPOLATE, OP_STEP, OP_SPREAD_INTERPOLATE = 1, 2, 3, 4
@@ -126,6 +129,11 @@ class ServerStats(ctypes.Structure):
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}
+
+
+class _Surface(ctypes.Structure):
+    _fields_ = [("position", ctypes.c_void_p), ("t", ctypes.c_void_p * 2), ("tt", ctypes.c_void_p * 3),
+                ("normal", ctypes.c_void_p), ("sigma", ctypes.c_void_p)]
 
 
 _lib = None
@@ -209,8 +217,16 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
         L.ibk_io_read_scalar.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_longlong)]
+        L.ibk_surface_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp), _vp, ctypes.POINTER(_vp)]
+        L.ibk_surface_plan_destroy.argtypes = [_vp]
+        L.ibk_surface_geometry.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_Surface), _vp]
+        L.ibk_membrane_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                           ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
+        L.ibk_membrane_bending.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _vp,
+                                           ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
         for name in ABI_SYMBOLS:
-            if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_")) and name != "ibk_server_clock":
+            if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_", "ibk_surface_", "ibk_membrane_")) \
+                    and name != "ibk_server_clock":
                 getattr(L, name).restype = ctypes.c_int
         L.ibk_last_error.restype = ctypes.c_char_p
         L.ibk_status_string.restype = ctypes.c_char_p
@@ -678,6 +694,89 @@ class Server:
         st = ServerStats()
         check(lib().ibk_server_run_poisson(self._h, float(rate), int(requests), int(seed), ctypes.byref(st)))
         return st.as_dict()
+
+
+# ------------------------------------------- membrane forces on RBF surfaces
+_SURFACE_FIELDS = ("position", "tu", "tv", "tuu", "tuv", "tvv", "normal", "sigma")
+
+
+def _surface_struct(g):
+    """ibk_surface from a dict of device tensors (missing keys: NULL)."""
+    s = _Surface()
+    s.position = _ptr(g.get("position"))
+    s.t[0], s.t[1] = _ptr(g.get("tu")), _ptr(g.get("tv"))
+    s.tt[0], s.tt[1], s.tt[2] = _ptr(g.get("tuu")), _ptr(g.get("tuv")), _ptr(g.get("tvv"))
+    s.normal = _ptr(g.get("normal"))
+    s.sigma = _ptr(g.get("sigma"))
+    return s
+
+
+class SurfacePlan:
+    """Geometry of a family of shapes sharing one set of RBF operators
+    (bases::geometry<2>, include/bases/geometry.h:74-124).  ops: six CUDA
+    float64 ns x nd tensors (evaluation -- or None when the samples are the
+    data sites -- d/du, d/dv, d2/du2, d2/dudv, d2/dv2); weights: ns quadrature
+    weights.  The tensors are kept alive by the plan."""
+
+    def __init__(self, ops, weights):
+        import torch
+        self.ns = int(weights.numel())
+        self.nd = int(ops[1].shape[1])
+        # column-major ns x nd: the transpose of a row-major (ns, nd) tensor
+        self._ops = [None if o is None else o.t().contiguous().t() for o in ops]
+        self._weights = weights.contiguous()
+        arr = (_vp * 6)(*[None if o is None else o.data_ptr() for o in self._ops])
+        h = _vp()
+        check(lib().ibk_surface_plan_create(self.ns, self.nd, arr, self._weights.data_ptr(), ctypes.byref(h)))
+        self.handle = h
+        self._torch = torch
+
+    def geometry(self, x, nc, stream=None):
+        """x: 3*nd*nc positions [component][shape][site]; returns a dict of
+        position, tu, tv, tuu, tuv, tvv, normal (3*ns*nc) and sigma (ns*nc)."""
+        torch = self._torch
+        m = self.ns * nc
+        g = {k: torch.empty(m if k == "sigma" else 3 * m, dtype=torch.float64, device=x.device)
+             for k in _SURFACE_FIELDS}
+        s = _surface_struct(g)
+        check(lib().ibk_surface_geometry(self.handle, nc, x.data_ptr(), ctypes.byref(s), _stream_handle(stream)))
+        return g
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().ibk_surface_plan_destroy(self.handle)
+            self.handle = None
+
+
+def membrane_tension(law, shear, bulk, rest, current, stream=None):
+    """Tension force at every sample site (forces::tension with the Skalak or
+    neo-Hookean law, include/forces/tension.h:55-116) from the rest and
+    current geometry dicts; returns 3*npoints forces [component][site]."""
+    import torch
+    n = int(rest["sigma"].numel())
+    f = torch.empty(3 * n, dtype=torch.float64, device=rest["sigma"].device)
+    r, c = _surface_struct(rest), _surface_struct(current)
+    check(lib().ibk_membrane_tension(law, shear, bulk, n, ctypes.byref(r), ctypes.byref(c), f.data_ptr(),
+                                     _stream_handle(stream)))
+    return f
+
+
+def membrane_bending(data_plan, sample_plan, modulus, preferred, x_rest, x_current, rest, current, nc,
+                     stream=None):
+    """Bending force at every sample (forces::bending,
+    include/forces/bending.h:145-229): data_plan holds the shape family's
+    operators at its data sites, sample_plan those at its samples; rest /
+    current are sample geometry dicts (SurfacePlan.geometry), x_rest /
+    x_current the data-site positions.  Returns 3*ns*nc forces."""
+    import torch
+    n = sample_plan.ns * nc
+    f = torch.empty(3 * n, dtype=torch.float64, device=x_current.device)
+    r = _surface_struct(rest) if rest is not None else None
+    c = _surface_struct(current)
+    check(lib().ibk_membrane_bending(data_plan.handle, sample_plan.handle, modulus, int(bool(preferred)), nc,
+                                     _ptr(x_rest), x_current.data_ptr(), ctypes.byref(r) if r is not None else None,
+                                     ctypes.byref(c), f.data_ptr(), _stream_handle(stream)))
+    return f
 
 
 # ------------------------------------------------------- linalg::io files

@@ -110,8 +110,9 @@ ibk_status ibk_plan_info(ibk_plan plan, ibk_grid_info* info);
 /* Preferred tile extents in cells per axis, in [M, 64], for the spread
  * (owner-computes accumulator tiles) and interpolation (staged halo regions)
  * kernels; either may be NULL to keep the current shape.  Each axis is
- * shrunk so its last tile keeps at least M cells.  Defaults: 16^3 for both
- * (equal shapes let ibk_spread_interpolate bin the points once).  Results do
+ * shrunk so its last tile keeps at least M cells.  Default for both: 16
+ * cells per axis, but at least four tiles per axis on small grids (equal
+ * shapes let ibk_spread_interpolate bin the points once).  Results do
  * not depend on the shape except through the FP32C fixed-point scale, which
  * is per tile. */
 ibk_status ibk_plan_set_tiles(ibk_plan plan, const int* spread_tile, const int* interp_tile);
@@ -385,6 +386,79 @@ ibk_status ibk_io_write_scalar(const char* path, int append, double value);
 ibk_status ibk_io_read_dense(const char* path, long long offset, ibk_io_header* header, double* values,
                              long long capacity, long long* next_offset);
 ibk_status ibk_io_read_scalar(const char* path, long long offset, double* value, long long* next_offset);
+
+/* ---- Membrane forces on RBF surfaces ------------------------------------
+ * The producers of the point forces that a spread takes: the surface geometry
+ * of a family of shapes that share one set of RBF operators
+ * (bases::geometry<2>::compute, include/bases/geometry.h:74-124) and the
+ * in-plane tension of a hyperelastic membrane (forces::tension,
+ * include/forces/tension.h:9-118) under the Skalak law
+ * (include/forces/skalak.h:11-37) or the neo-Hookean law
+ * (include/forces/neohookean.h:10-37).  FP64 throughout.
+ *
+ * Layout, as the reference's shape matrices: nc shapes of ns sample sites
+ * (or nd data sites); a per-site vector quantity is 3 blocks of ns*nc values,
+ * [component][shape][site] (the reference's column-major ns x 3nc matrix),
+ * a scalar quantity one block of ns*nc values [shape][site]. */
+typedef struct ibk_surface_plan_s* ibk_surface_plan;
+
+/* Geometry at the sample sites (every pointer a caller-owned device array;
+ * outputs may be NULL where noted). */
+typedef struct {
+	double* position;       /* 3*ns*nc; NULL: not computed */
+	double* t[2];           /* tangents d/du, d/dv: 3*ns*nc each */
+	double* tt[3];          /* second derivatives uu, uv, vv: 3*ns*nc each */
+	double* normal;         /* t_u x t_v / |t_u x t_v|: 3*ns*nc; NULL: not computed */
+	double* sigma;          /* patch areas weight * |t_u x t_v|: ns*nc */
+} ibk_surface;
+
+/* One shape family's operators (bases::operators<2>,
+ * include/bases/operators.h:128-234): ops[0] evaluation, ops[1..2] first
+ * derivatives (u, v), ops[3..5] second derivatives (uu, uv, vv), each a
+ * column-major ns x nd device matrix; ops[0] may be NULL when the samples
+ * are the data sites (ns == nd; the reference then copies the positions).
+ * weights: ns quadrature weights.  The arrays are kept by pointer and must
+ * outlive the plan.  Binds the current CUDA device. */
+ibk_status ibk_surface_plan_create(int ns, int nd, const double* const* ops, const double* weights,
+                                   ibk_surface_plan* out);
+ibk_status ibk_surface_plan_destroy(ibk_surface_plan plan);
+
+/* Geometry of nc shapes from their data-site positions x (3*nd*nc,
+ * [component][shape][site]): position and derivatives are the operators
+ * times x (FP64 library GEMMs), then per sample the normal and the patch area
+ * (geometry.h:95-119).  Overwrites every non-NULL output of *out. */
+ibk_status ibk_surface_geometry(ibk_surface_plan plan, int nc, const double* x, const ibk_surface* out,
+                                void* stream);
+
+/* Tension laws: w(I1, I2) and its second derivatives. */
+typedef enum { IBK_LAW_SKALAK = 0, IBK_LAW_NEOHOOKEAN = 1 } ibk_tension_law;
+
+/* Tension force at npoints sample sites (forces::tension::operator(),
+ * tension.h:55-116): from the rest geometry (t, tt, sigma read) and the
+ * current geometry (t, tt read), the strain invariants, the law's
+ * derivatives and the divergence of the tension, times the rest patch area.
+ * shear and bulk are energies per area in internal units (the reference's
+ * skalak{shear, bulk} / neohookean{shear, bulk}).  Overwrites f (3*npoints,
+ * [component][site]).  npoints <= 0 returns at once. */
+ibk_status ibk_membrane_tension(int law, double shear, double bulk, int npoints, const ibk_surface* rest,
+                                const ibk_surface* current, double* f, void* stream);
+
+/* Bending force (forces::bending, include/forces/bending.h:10-229):
+ * f = -4 kappa sigma (Lap H + 2 (H - H0)(H^2 - K + H H0)) n at every sample,
+ * with H0 the rest shape's mean curvature when `preferred` is set (else 0).
+ * The mean curvature is taken at the data sites from data_plan (that shape
+ * family's operators at its own data sites: ns == nd, evaluation may be
+ * NULL) and the positions x_rest / x_current (3*nd*nc; x_rest read only
+ * with `preferred`), its surface Laplacian at the samples through
+ * sample_plan's derivative operators and the current sample geometry
+ * (t, tt, normal, sigma read); K and H at the samples from that geometry,
+ * H0 there from the rest sample geometry (t, tt, normal read, with
+ * `preferred`).  modulus: bending energy in internal units.  Overwrites f
+ * (3*ns*nc).  Device scratch of about (21 nd + 5 ns) * nc doubles is kept by
+ * sample_plan and grown on first use (not during stream capture). */
+ibk_status ibk_membrane_bending(ibk_surface_plan data_plan, ibk_surface_plan sample_plan, double modulus,
+                                int preferred, int nc, const double* x_rest, const double* x_current,
+                                const ibk_surface* rest, const ibk_surface* current, double* f, void* stream);
 
 /* Human-readable text of the last error on the calling host thread. */
 const char* ibk_last_error(void);

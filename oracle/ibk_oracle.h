@@ -86,6 +86,25 @@ void ibo_interpolate_mt(const ibo_geom* g, int n, const double* x,
                         const double* const* ue, double* ul, int nthreads);
 int ibo_max_threads(void);
 
+/* Membrane forces (ibk_membrane_oracle.c).  Surface geometry of nc shapes:
+ * ops[0..5] column-major ns x nd operators (ops[0] NULL: samples are the
+ * data sites), x 3*nd*nc positions [component][shape][site]; out[0..7] =
+ * position, tu, tv, tuu, tuv, tvv (3*ns*nc each), normal (3*ns*nc) and
+ * sigma (ns*nc), NULL to skip (tu, tv and sigma required). */
+void ibo_surface_geometry(int ns, int nd, int nc, const double* const* ops, const double* weights,
+                          const double* x, double* const* out);
+/* Tension force (law 0 Skalak, 1 neo-Hookean): rest[0..5] = tu, tv, tuu,
+ * tuv, tvv, sigma; cur[0..4] = tu, tv, tuu, tuv, tvv; f 3*npoints. */
+void ibo_membrane_tension(int law, double e, double kappa, int npoints, const double* const* rest,
+                          const double* const* cur, double* f);
+/* Bending force: data_ops (nd x nd, evaluation NULL) with data_weights give
+ * the curvature field at the data sites, sample_ops[1..5] (ns x nd) its
+ * derivatives at the samples; rest[0..5] = tu, tv, tuu, tuv, tvv, normal
+ * (read with preferred); cur[0..6] the same and sigma; f 3*ns*nc. */
+void ibo_membrane_bending(int ns, int nd, int nc, const double* const* data_ops, const double* data_weights,
+                          const double* const* sample_ops, double modulus, int preferred, const double* x_rest,
+                          const double* x_cur, const double* const* rest, const double* const* cur, double* f);
+
 #ifdef __cplusplus
 }
 #endif

@@ -113,6 +113,13 @@ def lib():
             L.ibo_interpolate_mt.argtypes = [ctypes.POINTER(Geom), ctypes.c_int, _dp,
                                              ctypes.POINTER(_dp), _dp, ctypes.c_int]
             L.ibo_max_threads.restype = ctypes.c_int
+            L.ibo_surface_geometry.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
+                                               _dp, _dp, ctypes.POINTER(_dp)]
+            L.ibo_membrane_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                               ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
+            L.ibo_membrane_bending.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp), _dp,
+                                               ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int, _dp, _dp,
+                                               ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
             _lib = L
     return _lib
 
@@ -231,6 +238,62 @@ def interpolate(g: Geom, x, ue, with_abs=False, threads=1):
 
 def max_threads() -> int:
     return int(lib().ibo_max_threads())
+
+
+SURFACE_FIELDS = ("position", "tu", "tv", "tuu", "tuv", "tvv", "normal", "sigma")
+
+
+def surface_geometry(ops, weights, x, nc):
+    """Surface geometry of nc shapes (include/bases/geometry.h:30-49, 95-119):
+    ops = six (ns, nd) arrays (ops[0] None: samples are the data sites),
+    weights (ns,), x 3*nd*nc positions [component][shape][site]; returns a
+    dict of the SURFACE_FIELDS arrays."""
+    weights = np.ascontiguousarray(weights, dtype=np.float64)
+    ns = weights.size
+    cm = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in ops]   # column-major
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    m = ns * nc
+    out = {k: np.zeros(m if k == "sigma" else 3 * m) for k in SURFACE_FIELDS}
+    opp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cm])
+    outp = (_dp * 8)(*[_d(out[k]) for k in SURFACE_FIELDS])
+    nd = cm[1].shape[1]
+    lib().ibo_surface_geometry(ns, nd, nc, opp, _d(weights), _d(x), outp)
+    return out
+
+
+def membrane_tension(law, shear, bulk, rest, cur):
+    """Tension force at every sample (include/forces/tension.h:71-112;
+    law 0 Skalak, 1 neo-Hookean) from rest and current geometry dicts."""
+    keep = [np.ascontiguousarray(rest[k], dtype=np.float64) for k in ("tu", "tv", "tuu", "tuv", "tvv", "sigma")]
+    keep += [np.ascontiguousarray(cur[k], dtype=np.float64) for k in ("tu", "tv", "tuu", "tuv", "tvv")]
+    n = keep[5].size
+    f = np.zeros(3 * n)
+    rp = (_dp * 6)(*[_d(a) for a in keep[:6]])
+    cp = (_dp * 5)(*[_d(a) for a in keep[6:]])
+    lib().ibo_membrane_tension(int(law), float(shear), float(bulk), n, rp, cp, _d(f))
+    return f
+
+
+def membrane_bending(data_ops, data_weights, sample_ops, modulus, preferred, x_rest, x_cur, rest, cur, nc):
+    """Bending force at every sample (include/forces/bending.h:145-229):
+    data_ops / sample_ops as for surface_geometry (the shape family's
+    operators at its data sites and at its samples), rest / cur sample
+    geometry dicts, positions 3*nd*nc; returns 3*ns*nc forces."""
+    cmd = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in data_ops]
+    cms = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in sample_ops]
+    dw = np.ascontiguousarray(data_weights, dtype=np.float64)
+    ns, nd = cms[1].shape
+    keys = ("tu", "tv", "tuu", "tuv", "tvv", "normal")
+    r = [np.ascontiguousarray(rest[k], dtype=np.float64) for k in keys]
+    c = [np.ascontiguousarray(cur[k], dtype=np.float64) for k in keys + ("sigma",)]
+    xr = np.ascontiguousarray(x_rest, dtype=np.float64)
+    xc = np.ascontiguousarray(x_cur, dtype=np.float64)
+    f = np.zeros(3 * ns * nc)
+    dp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cmd])
+    sp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cms])
+    lib().ibo_membrane_bending(ns, nd, nc, dp, _d(dw), sp, float(modulus), int(bool(preferred)), _d(xr), _d(xc),
+                               (_dp * 6)(*[_d(a) for a in r]), (_dp * 7)(*[_d(a) for a in c]), _d(f))
+    return f
 
 
 def ref_stencil(g: Geom, comp: int, x):
