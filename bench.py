@@ -856,38 +856,53 @@ def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
                     "kernels; median of the timed steps, CUDA events"}
 
 
-def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=4):
+def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=4, slot_sweep=(1, 2, 8), sweep_rate=50000):
     """Serving sweep: 256 ensemble members resident on the device, Poisson
     step requests (interpolate, advect dt = 1 us, spring k = 1 pN/um,
-    spread) at each offered rate, continuous batching on `slots` streams."""
+    spread) at each offered rate, continuous batching on `slots` streams;
+    then the saturating rate again with other slot counts.  Each launch's
+    host time (packing the ready members, binding, launching) is reported."""
     insts_w = W.ensemble(seed=seed, count=256)
-    insts = [ibk.Instance(ibk.Mac(w.refinement),
-                          ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)]))
-             for w in insts_w]
+    doms = [ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)]) for w in insts_w]
+    insts = [ibk.Instance(ibk.Mac(w.refinement), d) for w, d in zip(insts_w, doms)]
     dt = 1e-6 * 1e3            # 1 us in the internal time unit (1 ms)
     k = W.PN / W.UM            # 1 pN/um
-    srv = ibk.Server(insts, ibk.Bspline(3), ibk.FP32C, slots=slots, dt=dt, k=k,
-                     hbm_budget=150 * 10**9, max_points=sum(w.n for w in insts_w))
     rng = np.random.default_rng(3000 + seed)
-    for i, w in enumerate(insts_w):
-        info = ibk.Plan(ibk.Mac(w.refinement),
-                        ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)]),
-                        ibk.Bspline(3), ibk.FP32C).sizes()
-        srv.admit(i, w.x, [rng.normal(size=s_) * W.UM_PER_S for s_ in info])
-    srv.run_poisson(rate=500.0, requests=100, seed=1)          # warm-up
+    velocities = [[rng.normal(size=s_) * W.UM_PER_S
+                   for s_ in ibk.Plan(ibk.Mac(w.refinement), d, ibk.Bspline(3), ibk.FP32C).sizes()]
+                  for w, d in zip(insts_w, doms)]
+
+    def server(nslots):
+        srv = ibk.Server(insts, ibk.Bspline(3), ibk.FP32C, slots=nslots, dt=dt, k=k,
+                         hbm_budget=150 * 10**9, max_points=sum(w.n for w in insts_w))
+        for i, w in enumerate(insts_w):
+            srv.admit(i, w.x, velocities[i])
+        srv.run_poisson(rate=500.0, requests=100, seed=1)          # warm-up
+        return srv
+
+    def entry(r, st):
+        return {"offered_per_s": r, "requests": st["requests"], "p50_ms": st["p50_ms"],
+                "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
+                "served_per_s": st["requests"] / max(st["wall_s"], 1e-9),
+                "points_per_s": st["points"] / max(st["wall_s"], 1e-9),
+                "launches": st["launches"], "host_ms_per_launch": st["host_ms_per_launch"]}
+
+    srv = server(slots)
     sweep = []
     for r in rates:
         nreq = int(max(200, min(20000, r * seconds_per_rate)))
-        st = srv.run_poisson(rate=float(r), requests=nreq, seed=int(r))
-        sweep.append({"offered_per_s": r, "requests": st["requests"], "p50_ms": st["p50_ms"],
-                      "p99_ms": st["p99_ms"], "mean_ms": st["mean_ms"],
-                      "served_per_s": st["requests"] / max(st["wall_s"], 1e-9),
-                      "points_per_s": st["points"] / max(st["wall_s"], 1e-9),
-                      "launches": st["launches"]})
+        sweep.append(entry(r, srv.run_poisson(rate=float(r), requests=nreq, seed=int(r))))
     admitted = srv.stats()["admitted_bytes"]
     srv.close()
+    slots_sweep = []
+    for ns_ in slot_sweep:
+        srv = server(ns_)
+        e = entry(sweep_rate, srv.run_poisson(rate=float(sweep_rate), requests=10000, seed=7))
+        e["slots"] = ns_
+        slots_sweep.append(e)
+        srv.close()
     return {"members": len(insts_w), "slots": slots, "admitted_bytes": admitted,
-            "hbm_budget_bytes": 150 * 10**9, "sweep": sweep}
+            "hbm_budget_bytes": 150 * 10**9, "sweep": sweep, "slot_sweep": slots_sweep}
 
 
 def main():

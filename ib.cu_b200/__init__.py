@@ -125,7 +125,7 @@ class ServerStats(ctypes.Structure):
     _fields_ = [("requests", ctypes.c_longlong), ("launches", ctypes.c_longlong),
                 ("points", ctypes.c_longlong), ("p50_ms", ctypes.c_double), ("p99_ms", ctypes.c_double),
                 ("mean_ms", ctypes.c_double), ("max_ms", ctypes.c_double), ("wall_s", ctypes.c_double),
-                ("admitted_bytes", ctypes.c_longlong)]
+                ("admitted_bytes", ctypes.c_longlong), ("host_ms_per_launch", ctypes.c_double)]
 
     def as_dict(self):
         return {name: getattr(self, name) for name, _ in self._fields_}

@@ -74,6 +74,7 @@ struct Server {
 	std::vector<double> latency_ms;
 	long long launches = 0, points = 0;
 	double first_arrival = -1.0, last_done = 0.0;
+	double launch_host_s = 0.0;           // host time spent in launches
 };
 
 namespace {
@@ -124,6 +125,7 @@ ibk_status reap(Server& s)
 // Launches the queued requests of idle members on one free slot.
 ibk_status launch(Server& s, Slot& sl)
 {
+	const double t_start = now_s(s);
 	std::fill(s.chosen.begin(), s.chosen.end(), 0);
 	sl.reqs.clear();
 	sl.points = 0;
@@ -164,6 +166,7 @@ ibk_status launch(Server& s, Slot& sl)
 	}
 	sl.busy = true;
 	++s.launches;
+	s.launch_host_s += now_s(s) - t_start;
 	return IBK_OK;
 }
 
@@ -204,6 +207,7 @@ void fill_stats(const Server& s, ibk_server_stats* out)
 	out->launches = s.launches;
 	out->points = s.points;
 	out->admitted_bytes = s.admitted_bytes;
+	out->host_ms_per_launch = s.launches ? 1e3 * s.launch_host_s / (double) s.launches : 0.0;
 	if (s.latency_ms.empty()) return;
 	std::vector<double> v(s.latency_ms);
 	std::sort(v.begin(), v.end());
@@ -492,6 +496,7 @@ ibk_status ibk_server_reset_stats(ibk_server handle)
 	s->points = 0;
 	s->first_arrival = -1.0;
 	s->last_done = 0.0;
+	s->launch_host_s = 0.0;
 	return IBK_OK;
 }
 

@@ -320,6 +320,7 @@ typedef struct {
 	double p50_ms, p99_ms, mean_ms, max_ms;   /* arrival -> completion seen */
 	double wall_s;              /* first arrival -> last completion */
 	long long admitted_bytes;
+	double host_ms_per_launch;  /* host time to pack, bind and launch one step batch */
 } ibk_server_stats;
 
 ibk_status ibk_server_create(int members, const ibk_instance_desc* desc, const ibk_server_config* config,
