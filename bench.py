@@ -4,7 +4,7 @@
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
                     [--workload large-channel|medium-channel|channel|single-rbc]
                     [--precision fp32c|fp64] [--no-cpu] [--no-extras]
-                    [--leg all|batched|serving|membrane]
+                    [--leg all|batched|serving|membrane|fluid]
 
 One step = ibk_spread_interpolate over every Lagrangian point of the
 workload: one spread and one interpolation at the same positions, which bin
@@ -13,14 +13,15 @@ point velocity).  Metric: points per second through spread+interp, in the chosen
 FP32C form, with the plain FP64 path, its accuracy, p50/p99 step times, the
 end-to-end rate through host buffers and the CPU baseline in the same line.
 
-The same line also carries three legs (skipped with --no-extras, or run
+The same line also carries four legs (skipped with --no-extras, or run
 alone with --leg): "batched" -- 256 independent instances (cube grids 32^3..128^3,
 1-50 cells each) in graph-captured persistent launches (spread and
 interpolation, one binning), FP32C against the FP64 batch and against a loop
 of single plans; "serving" -- the
 256 instances as device-resident members stepped (interpolate, advect, spring
 force, spread) under Poisson request arrivals from 1k to 50k steps/s, with
-p50/p99 latency per offered rate; "membrane" -- the producers of the point
+p50/p99 latency per offered rate; "fluid" -- one implicit diffusion step of
+a velocity component on the large channel's grid; "membrane" -- the producers of the point
 forces, for 64 shapes of the reference's RBC discretisation (2500 data sites,
 10000 samples): surface geometry (FP64 operator products, normals, patch
 areas) and the Skalak tension, per step.
@@ -267,12 +268,14 @@ def run_ours(args):
     ibk.lib()
     from ib_cu_b200 import workloads as W
 
-    if args.leg in ("batched", "serving", "membrane"):
+    if args.leg in ("batched", "serving", "membrane", "fluid"):
         # one leg alone (profiling runs): its own JSON object
         if args.leg == "batched":
             res = run_batched(ibk, W, dev, seed=0, steps=max(5, args.steps), rank=rank, world=world)
         elif args.leg == "membrane":
             res = run_membrane(ibk, dev, steps=max(5, args.steps))
+        elif args.leg == "fluid":
+            res = run_fluid(ibk, W, dev, steps=max(3, args.steps // 2))
         else:
             res = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
         if rank == 0:
@@ -539,6 +542,7 @@ def run_ours(args):
         extras["batched"] = run_batched(ibk, W, dev, seed=0, steps=max(5, args.steps // 2), rank=rank, world=world)
         extras["serving"] = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
         extras["membrane"] = run_membrane(ibk, dev, steps=max(5, args.steps // 2))
+        extras["fluid"] = run_fluid(ibk, W, dev, steps=3)
 
     cpu = None
     if rank == 0 and world == 1 and not args.no_cpu:
@@ -856,6 +860,47 @@ def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
                     "kernels; median of the timed steps, CUDA events"}
 
 
+def run_fluid(ibk, W, dev, steps, warmup=1):
+    """The fluid step that consumes the spread's force density: one implicit
+    diffusion step (Crank-Nicolson, gamma = 1) of the x-velocity grid of the
+    large channel (512 x 256 x 512 cells, walls in y: Dirichlet), mu = 1,
+    timestep 1e-3 (internal units: mu k / h^2 = 1.6), solver tolerance 1e-11
+    as the reference's drivers set it.  Random velocity, force and rhs."""
+    import torch
+    w = make_workload("large-channel")
+    dom = ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)])
+    plan = ibk.Plan(ibk.Mac(w.refinement), dom, ibk.Bspline(3), ibk.FP64)
+    d = ibk.Diffusion(plan, 0, 1e-3, 1.0, tolerance=1e-11, max_iterations=5000)
+    gen = torch.Generator(device=dev)
+    gen.manual_seed(17)
+    u, f, rhs = (torch.randn(d.size, generator=gen, dtype=torch.float64, device=dev) for _ in range(3))
+    times, its = [], []
+    for it in range(warmup + steps):
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record()
+        out = d.step(u, rhs, f, gamma=1.0)
+        e1.record()
+        torch.cuda.synchronize()
+        if it >= warmup:
+            times.append(e0.elapsed_time(e1))
+            its.append(d.iterations)
+        del out
+    ms = float(np.median(times))
+    iters = int(np.median(its))
+    per_iter_bytes = 13 * 8.0 * d.size     # operator (2 vectors), update (8), direction (3)
+    peak, _ = measured_peaks()
+    res = {"faces": d.size, "grid": "512x256x512 (x faces)", "steps": steps, "ms_per_step": ms,
+           "iterations": iters, "ms_per_iteration": ms / max(iters, 1),
+           "iteration_gbs": per_iter_bytes * iters / (ms * 1e-3) / 1e9,
+           "iteration_frac_of_hbm": per_iter_bytes * iters / (ms * 1e-3) / 1e9 / peak,
+           "note": "FP64 matrix-free operator and PCG (Jacobi), the convergence test read back once per "
+                   "iteration; median of the timed steps, CUDA events"}
+    del d, plan, u, f, rhs
+    torch.cuda.empty_cache()
+    return res
+
+
 def run_serving(ibk, W, dev, seed, rates, seconds_per_rate=1.0, slots=4, slot_sweep=(1, 2, 8), sweep_rate=50000):
     """Serving sweep: 256 ensemble members resident on the device, Poisson
     step requests (interpolate, advect dt = 1 us, spring k = 1 pN/um,
@@ -915,8 +960,8 @@ def main():
                     choices=["large-channel", "medium-channel", "channel", "single-rbc"])
     ap.add_argument("--precision", choices=["fp32c", "fp64"], default="fp32c")
     ap.add_argument("--no-cpu", action="store_true", help="skip the CPU baseline leg")
-    ap.add_argument("--leg", choices=["all", "batched", "serving", "membrane"], default="all",
-                    help="batched / serving / membrane: run that leg alone (its own JSON line)")
+    ap.add_argument("--leg", choices=["all", "batched", "serving", "membrane", "fluid"], default="all",
+                    help="batched / serving / membrane / fluid: run that leg alone (its own JSON line)")
     ap.add_argument("--no-extras", action="store_true",
                     help="skip the batched (256 instances) and serving legs")
     args = ap.parse_args()

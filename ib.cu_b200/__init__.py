@@ -55,6 +55,7 @@ ABI_SYMBOLS = (
     "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
     "ibk_surface_plan_create", "ibk_surface_plan_destroy", "ibk_surface_geometry", "ibk_membrane_tension",
     "ibk_membrane_bending",
+    "ibk_diffusion_create", "ibk_diffusion_destroy", "ibk_diffusion_apply", "ibk_diffusion_step",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
 OP_SPREAD, OP_INTERPOLATE, OP_STEP, OP_SPREAD_INTERPOLATE = 1, 2, 3, 4
@@ -222,10 +223,16 @@ def lib() -> ctypes.CDLL:
         L.ibk_surface_geometry.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_Surface), _vp]
         L.ibk_membrane_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                            ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
+        L.ibk_diffusion_create.argtypes = [_vp, ctypes.c_int, _vp, ctypes.c_double, ctypes.c_double,
+                                           ctypes.c_double, ctypes.c_int, ctypes.POINTER(_vp)]
+        L.ibk_diffusion_destroy.argtypes = [_vp]
+        L.ibk_diffusion_apply.argtypes = [_vp, ctypes.c_int, _vp, _vp, _vp]
+        L.ibk_diffusion_step.argtypes = [_vp, ctypes.c_double, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int), _vp]
         L.ibk_membrane_bending.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                            ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
         for name in ABI_SYMBOLS:
-            if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_", "ibk_surface_", "ibk_membrane_")) \
+            if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_", "ibk_surface_", "ibk_membrane_",
+                                "ibk_diffusion_")) \
                     and name != "ibk_server_clock":
                 getattr(L, name).restype = ctypes.c_int
         L.ibk_last_error.restype = ctypes.c_char_p
@@ -777,6 +784,50 @@ def membrane_bending(data_plan, sample_plan, modulus, preferred, x_rest, x_curre
                                      _ptr(x_rest), x_current.data_ptr(), ctypes.byref(r) if r is not None else None,
                                      ctypes.byref(c), f.data_ptr(), _stream_handle(stream)))
     return f
+
+
+# ------------------------------------------- the fluid step: implicit diffusion
+DIRICHLET, NEUMANN = (1.0, 0.0), (0.0, 1.0)    # Robin (a, b) of a wall: a u + b du/dn
+
+
+class Diffusion:
+    """ins::diffusion (include/ins/diffusion.h:12-78) on one component grid
+    of a plan: step(u, rhs, f, gamma) = u + (I~ - lambda L)^-1 (k I~ f +
+    k mu (L u + rhs)), k = gamma * timestep, lambda = timestep * mu / 2.
+    robin[axis] = ((a, b) lower wall, (a, b) upper wall), ignored on periodic
+    axes; default Dirichlet walls."""
+
+    def __init__(self, plan, component, timestep, mu, tolerance=1e-11, max_iterations=10000, robin=None):
+        if robin is None:
+            robin = [(DIRICHLET, DIRICHLET)] * 3
+        flat = (ctypes.c_double * 12)(*[float(v) for axis in robin for side in axis for v in side])
+        h = _vp()
+        check(lib().ibk_diffusion_create(plan.handle, int(component), flat, float(timestep), float(mu),
+                                         float(tolerance), int(max_iterations), ctypes.byref(h)))
+        self.handle = h
+        self.size = int(plan.info.size[component])
+        self.iterations = 0
+
+    def apply(self, op, u, stream=None):
+        """op 0: L u, 1: I~ u, 2: (I~ - lambda L) u."""
+        import torch
+        out = torch.empty(self.size, dtype=torch.float64, device=u.device)
+        check(lib().ibk_diffusion_apply(self.handle, int(op), u.data_ptr(), out.data_ptr(), _stream_handle(stream)))
+        return out
+
+    def step(self, u, rhs, f, gamma=1.0, stream=None):
+        import torch
+        out = torch.empty(self.size, dtype=torch.float64, device=u.device)
+        it = ctypes.c_int()
+        check(lib().ibk_diffusion_step(self.handle, float(gamma), u.data_ptr(), rhs.data_ptr(), f.data_ptr(),
+                                       out.data_ptr(), ctypes.byref(it), _stream_handle(stream)))
+        self.iterations = it.value
+        return out
+
+    def __del__(self):
+        if getattr(self, "handle", None):
+            lib().ibk_diffusion_destroy(self.handle)
+            self.handle = None
 
 
 # ------------------------------------------------------- linalg::io files

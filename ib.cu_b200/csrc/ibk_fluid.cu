@@ -1,0 +1,437 @@
+// The fluid step that consumes the spread's force density: one implicit
+// diffusion step of a component grid (ins::diffusion,
+// include/ins/diffusion.h:12-78),
+//     out = u + (I~ - lambda L)^-1 (k I~ f + k mu (L u + rhs)),
+// with L the second-order finite-difference Laplacian and I~ the
+// boundary-corrected identity (fd::laplacian, fd::identity with
+// correction::second_order).  Both are Kronecker sums / products of 1-D
+// operators (include/fd/combine.h:24-30): along an axis L_d is the 3-point
+// Laplacian res^2 (1, -2, 1) with a wrap entry per corner on a periodic axis,
+// or on a solid axis the ghost-point weight of each wall added to its corner
+// diagonal, and I~_d is the identity plus each wall's second-order error
+// coefficient on its corner (include/fd/laplacian.h:18-46,
+// include/fd/identity.h:22-47, include/fd/discretization.h:47-80).  So
+//     (L u)_ijk = Iz Iy (Lx u) + Iz (Ly u) Ix + (Lz u) Iy Ix,   I~ = Iz Iy Ix,
+// a 7-point stencil whose coefficients differ from the interior only at the
+// walls: applied matrix-free here, one thread per face.  The solve is the
+// reference's preconditioned CG loop (include/solvers/pcg.h:12-45: stop when
+// |d|_2 <= tolerance for the search direction d, bail out when <d, H d> is
+// below tolerance^2) with a Jacobi preconditioner in place of the
+// reference's Chebyshev one, which changes the iteration count, not the
+// solution it converges to.  FP64, compiled without contraction.
+#include <cmath>
+#include <string>
+#include <vector>
+#include "ibk_internal.h"
+
+namespace ibk {
+namespace {
+
+constexpr int kFluidThreads = 256;
+constexpr int kFluidBlocks = 1184;          // 8 CTAs per SM on 148 SMs: fixed, so sums have one order
+
+// 1-D operators of one axis: L (lo, diag, hi; lo[0] / hi[P-1] wrap on a
+// periodic axis, else 0) and the corrected identity id.
+struct AxisOps {
+	const double* lo;
+	const double* diag;
+	const double* hi;
+	const double* id;
+	int P;
+	int periodic;
+};
+
+struct FluidOps {
+	AxisOps ax[3];
+	int dims;
+	long long size;
+	double lambda;
+};
+
+__device__ __forceinline__ double axis_apply(const AxisOps& a, const double* __restrict__ u, long long idx, int i,
+                                             long long stride)
+{
+	// tridiagonal row i along this axis (wrapping on a periodic axis)
+	const double um = i > 0 ? u[idx - stride] : (a.periodic ? u[idx + (long long) (a.P - 1) * stride] : 0.0);
+	const double up = i + 1 < a.P ? u[idx + stride] : (a.periodic ? u[idx - (long long) (a.P - 1) * stride] : 0.0);
+	return a.lo[i] * um + a.diag[i] * u[idx] + a.hi[i] * up;
+}
+
+// op 0: L u, 1: I~ u, 2: (I~ - lambda L) u.  With dot != nullptr also the
+// per-block partial sums of u . out (fixed grid and block order).
+__global__ void __launch_bounds__(kFluidThreads)
+apply_kernel(FluidOps o, int op, const double* __restrict__ u, double* __restrict__ out, double* __restrict__ dot)
+{
+	__shared__ double red[kFluidThreads / 32];
+	double acc = 0.0;
+	const int P0 = o.ax[0].P, P1 = o.ax[1].P;
+	for (long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x; idx < o.size;
+	     idx += (long long) gridDim.x * blockDim.x) {
+		const int i = (int) (idx % P0);
+		const long long r = idx / P0;
+		const int j = (int) (r % P1);
+		const int k = (int) (r / P1);
+		const double ix = o.ax[0].id[i], iy = o.dims > 1 ? o.ax[1].id[j] : 1.0;
+		const double iz = o.dims > 2 ? o.ax[2].id[k] : 1.0;
+		double v = 0.0;
+		if (op != 1) {
+			double l = iz * iy * axis_apply(o.ax[0], u, idx, i, 1);
+			if (o.dims > 1) l += iz * axis_apply(o.ax[1], u, idx, j, P0) * ix;
+			if (o.dims > 2) l += axis_apply(o.ax[2], u, idx, k, (long long) P0 * P1) * iy * ix;
+			v = l;
+		}
+		if (op == 1) v = iz * iy * ix * u[idx];
+		if (op == 2) v = iz * iy * ix * u[idx] - o.lambda * v;
+		out[idx] = v;
+		if (dot) acc += u[idx] * v;
+	}
+	if (!dot) return;
+	for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < kFluidThreads / 32; ++w) t += red[w];
+		dot[blockIdx.x] = t;
+	}
+}
+
+// Diagonal of I~ - lambda L (the Jacobi preconditioner).
+__global__ void __launch_bounds__(kFluidThreads)
+diagonal_kernel(FluidOps o, double* __restrict__ diag)
+{
+	const int P0 = o.ax[0].P, P1 = o.ax[1].P;
+	for (long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x; idx < o.size;
+	     idx += (long long) gridDim.x * blockDim.x) {
+		const int i = (int) (idx % P0);
+		const long long r = idx / P0;
+		const int j = (int) (r % P1);
+		const int k = (int) (r / P1);
+		const double ix = o.ax[0].id[i], iy = o.dims > 1 ? o.ax[1].id[j] : 1.0;
+		const double iz = o.dims > 2 ? o.ax[2].id[k] : 1.0;
+		double l = iz * iy * o.ax[0].diag[i];
+		if (o.dims > 1) l += iz * o.ax[1].diag[j] * ix;
+		if (o.dims > 2) l += o.ax[2].diag[k] * iy * ix;
+		diag[idx] = iz * iy * ix - o.lambda * l;
+	}
+}
+
+__device__ __forceinline__ void block_partial(double acc, double* __restrict__ out)
+{
+	__shared__ double red[kFluidThreads / 32];
+	for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
+	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+	__syncthreads();
+	if (threadIdx.x == 0) {
+		double t = 0.0;
+		for (int w = 0; w < kFluidThreads / 32; ++w) t += red[w];
+		out[blockIdx.x] = t;
+	}
+}
+
+// Sum of the per-block partials into *out (one thread, fixed order).
+__global__ void sum_kernel(const double* __restrict__ partial, int n, double* __restrict__ out)
+{
+	double t = 0.0;
+	for (int b = 0; b < n; ++b) t += partial[b];
+	*out = t;
+}
+
+// rhs = k I~ f + k mu (L u + rhs0): the right-hand side of the solve
+// (diffusion.h:51-53: gemv(1, L, u, 1, rhs), then gemv(k, I~, f, k mu, rhs)).
+__global__ void __launch_bounds__(kFluidThreads)
+rhs_kernel(long long n, double k, double kmu, const double* __restrict__ lu, const double* __restrict__ rhs0,
+           const double* __restrict__ idf, double* __restrict__ b)
+{
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x)
+		b[i] = k * idf[i] + kmu * (lu[i] + rhs0[i]);
+}
+
+// Start of the loop: x = 0, d = M^-1 r, partials of r . d and d . d.
+__global__ void __launch_bounds__(kFluidThreads)
+start_kernel(long long n, const double* __restrict__ r, const double* __restrict__ diag, double* __restrict__ x,
+             double* __restrict__ d, double* __restrict__ rd, double* __restrict__ dd)
+{
+	double a = 0.0, b = 0.0;
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+		const double z = r[i] / diag[i];
+		x[i] = 0.0;
+		d[i] = z;
+		a += r[i] * z;
+		b += z * z;
+	}
+	block_partial(a, rd);
+	__syncthreads();
+	block_partial(b, dd);
+}
+
+// x += alpha d, r -= alpha q, q = M^-1 r; partial sums of r . q.
+__global__ void __launch_bounds__(kFluidThreads)
+update_kernel(long long n, double alpha, const double* __restrict__ d, double* __restrict__ q, double* __restrict__ x,
+              double* __restrict__ r, const double* __restrict__ diag, double* __restrict__ rq)
+{
+	double a = 0.0;
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+		x[i] += alpha * d[i];
+		const double ri = r[i] - alpha * q[i];
+		r[i] = ri;
+		const double z = ri / diag[i];
+		q[i] = z;
+		a += ri * z;
+	}
+	block_partial(a, rq);
+}
+
+// d = q + beta d; partial sums of d . d.
+__global__ void __launch_bounds__(kFluidThreads)
+direction_kernel(long long n, double beta, const double* __restrict__ q, double* __restrict__ d, double* __restrict__ dd)
+{
+	double a = 0.0;
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+		const double v = q[i] + beta * d[i];
+		d[i] = v;
+		a += v * v;
+	}
+	block_partial(a, dd);
+}
+
+// out = u + x
+__global__ void __launch_bounds__(kFluidThreads)
+finish_kernel(long long n, const double* __restrict__ u, const double* __restrict__ x, double* __restrict__ out)
+{
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x)
+		out[i] = x[i] + u[i];
+}
+
+// util::math::modulo for the non-negative arguments met here
+double modulo1(double x) { return x - std::floor(x); }
+
+// Ghost-point weights of one wall (fd::__1::coefficients,
+// include/fd/discretization.h:47-80): Robin condition a u + b du/dn, signed
+// mesh width h, alignment s of the grid against the wall.
+struct WallWeights { double interior, laplacian; };
+
+WallWeights wall_weights(const double* p, double h, double s_in)
+{
+	const double s = 1 - modulo1(1 - s_in);
+	const double denom = p[1] - p[0] * s * h;
+	return {(p[1] + p[0] * h * (1 - s)) / denom, (-(p[1] * (1 - 2 * s) - p[0] * s * h * (1 - s))) / (2 * denom)};
+}
+
+ibk_status cuda_fail(cudaError_t e, const char* what)
+{
+	return set_error(IBK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+}
+
+} // namespace
+} // namespace ibk
+
+using namespace ibk;
+
+struct ibk_diffusion_s {
+	int device = 0;
+	FluidOps ops{};
+	double mu = 0.0, timestep = 0.0, tolerance = 0.0;
+	int max_iterations = 0;
+	double* coef = nullptr;        // per axis: lo, diag, hi, id (4 P_d doubles)
+	double* work = nullptr;        // b, r, d, q, x, diag, tmp (7 size doubles)
+	double* partial = nullptr;     // 2 * kFluidBlocks partial sums
+	double* scalars = nullptr;     // device scalars: [0] r.d / r.q, [1] d.q, [2] d.d
+};
+
+extern "C" {
+
+ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin[3][2][2], double timestep,
+                                double mu, double tolerance, int max_iterations, ibk_diffusion* out)
+{
+	if (!out) return set_error(IBK_ERR_INVALID_ARGUMENT, "null output handle");
+	*out = nullptr;
+	Plan* p = reinterpret_cast<Plan*>(plan);
+	if (!p || !robin) return set_error(IBK_ERR_INVALID_ARGUMENT, "null plan or boundary conditions");
+	const GridGeom& g = p->g;
+	if (component < 0 || component >= g.dims) return set_error(IBK_ERR_INVALID_ARGUMENT, "component out of range");
+	if (!(timestep > 0.0) || !(mu >= 0.0) || !(tolerance > 0.0) || max_iterations < 1)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "timestep and tolerance must be positive, mu non-negative");
+	const CompGeom& cg = g.comp[component];
+	auto* d = new ibk_diffusion_s;
+	cudaGetDevice(&d->device);
+	d->mu = mu;
+	d->timestep = timestep;
+	d->tolerance = tolerance;
+	d->max_iterations = max_iterations;
+	d->ops.dims = g.dims;
+	d->ops.lambda = timestep * mu / 2;       // diffusion.h:21-25
+	long long size = 1;
+	int total = 0;
+	for (int a = 0; a < 3; ++a) {
+		d->ops.ax[a].P = a < g.dims ? cg.points[a] : 1;
+		size *= d->ops.ax[a].P;
+		total += 4 * d->ops.ax[a].P;
+	}
+	d->ops.size = size;
+	std::vector<double> host((size_t) total, 0.0);
+	int off = 0;
+	for (int a = 0; a < g.dims; ++a) {
+		const int P = cg.points[a];
+		if (P < 3) {
+			delete d;
+			return set_error(IBK_ERR_INVALID_ARGUMENT, "each axis needs at least 3 points");
+		}
+		double* lo = host.data() + off;
+		double* dg = lo + P;
+		double* hi = dg + P;
+		double* id = hi + P;
+		const double scale = g.r * g.r;          // laplacian.h:25-26
+		for (int i = 0; i < P; ++i) {
+			lo[i] = i > 0 ? scale : 0.0;
+			dg[i] = -2 * scale;
+			hi[i] = i + 1 < P ? scale : 0.0;
+			id[i] = 1.0;
+		}
+		const int periodic = !g.solid[a];
+		if (periodic) {
+			// wrap entries (discretization.h:94-100: {!lower, lower, 1})
+			lo[0] = scale * 1.0;
+			hi[P - 1] = scale * 1.0;
+		} else {
+			// ghost-point weights of each wall on the corner diagonals, and the
+			// second-order error coefficients on the identity's corners
+			const double h = 1 / g.r;
+			const double al = modulo1(cg.shift[a]);
+			const WallWeights wl = wall_weights(robin[a][0], h, al);
+			const WallWeights wu = wall_weights(robin[a][1], -h, 1 - al);
+			dg[0] += scale * wl.interior;
+			dg[P - 1] += scale * wu.interior;
+			id[0] += wl.laplacian;
+			id[P - 1] += wu.laplacian;
+		}
+		d->ops.ax[a].periodic = periodic;
+		off += 4 * P;
+	}
+	cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d->coef), sizeof(double) * (size_t) total);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->work), sizeof(double) * 7 * (size_t) size);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->partial), sizeof(double) * 2 * kFluidBlocks);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->scalars), sizeof(double) * 4);
+	if (e == cudaSuccess) e = cudaMemcpy(d->coef, host.data(), sizeof(double) * (size_t) total, cudaMemcpyHostToDevice);
+	if (e != cudaSuccess) {
+		cudaGetLastError();
+		ibk_diffusion_destroy(d);
+		return set_error(IBK_ERR_OUT_OF_MEMORY, std::string("diffusion set-up: ") + cudaGetErrorString(e));
+	}
+	off = 0;
+	for (int a = 0; a < 3; ++a) {
+		AxisOps& ax = d->ops.ax[a];
+		if (a < g.dims) {
+			ax.lo = d->coef + off;
+			ax.diag = ax.lo + ax.P;
+			ax.hi = ax.diag + ax.P;
+			ax.id = ax.hi + ax.P;
+			off += 4 * ax.P;
+		} else {
+			ax.lo = ax.diag = ax.hi = ax.id = d->coef;    // never read (dims < 3)
+			ax.periodic = 0;
+		}
+	}
+	// the preconditioner's diagonal, kept in work slot 5
+	diagonal_kernel<<<kFluidBlocks, kFluidThreads>>>(d->ops, d->work + 5 * size);
+	ibk_status st = check_launch("diagonal_kernel");
+	if (st == IBK_OK && (e = cudaDeviceSynchronize()) != cudaSuccess) st = cuda_fail(e, "diffusion set-up");
+	if (st != IBK_OK) {
+		ibk_diffusion_destroy(d);
+		return st;
+	}
+	*out = d;
+	return IBK_OK;
+}
+
+ibk_status ibk_diffusion_destroy(ibk_diffusion d)
+{
+	if (!d) return IBK_OK;
+	int dev = 0;
+	cudaGetDevice(&dev);
+	cudaSetDevice(d->device);
+	cudaFree(d->coef);
+	cudaFree(d->work);
+	cudaFree(d->partial);
+	cudaFree(d->scalars);
+	cudaSetDevice(dev);
+	delete d;
+	return IBK_OK;
+}
+
+ibk_status ibk_diffusion_apply(ibk_diffusion d, int op, const double* u, double* out, void* stream)
+{
+	if (!d || !u || !out || op < 0 || op > 2) return set_error(IBK_ERR_INVALID_ARGUMENT, "null arrays or unknown operator");
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, op, u, out, nullptr);
+	return check_launch("apply_kernel");
+}
+
+ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, const double* rhs, const double* f,
+                              double* out, int* iterations, void* stream)
+{
+	if (!d || !u || !rhs || !f || !out) return set_error(IBK_ERR_INVALID_ARGUMENT, "null arrays");
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	const long long n = d->ops.size;
+	double* b = d->work;
+	double* r = b + n;
+	double* dv = r + n;
+	double* q = dv + n;
+	double* x = q + n;
+	double* diag = x + n;
+	double* tmp = diag + n;
+	double* pa = d->partial;
+	double* pb = d->partial + kFluidBlocks;
+	double* sc = d->scalars;
+	const double k = gamma * d->timestep;
+	// rhs of the solve: k I~ f + k mu (L u + rhs)
+	apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 0, u, tmp, nullptr);
+	apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 1, f, q, nullptr);
+	rhs_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, k, k * d->mu, tmp, rhs, q, b);
+	cudaError_t e = cudaMemcpyAsync(r, b, sizeof(double) * (size_t) n, cudaMemcpyDeviceToDevice, s);
+	if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+	start_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, r, diag, x, dv, pa, pb);
+	sum_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc + 0);
+	sum_kernel<<<1, 1, 0, s>>>(pb, kFluidBlocks, sc + 2);
+	ibk_status st = check_launch("diffusion set-up kernels");
+	if (st != IBK_OK) return st;
+	double hs[3];
+	const double tol = d->tolerance;
+	int it = 0;
+	for (;;) {
+		// pcg.h:21-42, the scalars read back once per iteration
+		e = cudaMemcpyAsync(hs, sc, sizeof(double) * 3, cudaMemcpyDeviceToHost, s);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+		if (e != cudaSuccess) return cuda_fail(e, "diffusion residual read");
+		if (!(std::sqrt(hs[2]) > tol)) break;
+		if (it >= d->max_iterations) {
+			if (iterations) *iterations = it;
+			return set_error(IBK_ERR_DEVICE_CHECK, "diffusion solve did not converge within max_iterations");
+		}
+		apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 2, dv, q, pa);
+		sum_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc + 1);
+		e = cudaMemcpyAsync(hs + 1, sc + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+		if (e != cudaSuccess) return cuda_fail(e, "diffusion curvature read");
+		const double nu = hs[1];
+		if (std::abs(nu) < tol * tol) break;   // pcg.h:26-31: no further progress possible
+		const double alpha = hs[0] / nu;
+		update_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, alpha, dv, q, x, r, diag, pa);
+		sum_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc + 3);
+		e = cudaMemcpyAsync(hs + 2, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, s);
+		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+		if (e != cudaSuccess) return cuda_fail(e, "diffusion residual read");
+		const double beta = hs[2] / hs[0];
+		e = cudaMemcpyAsync(sc, sc + 3, sizeof(double), cudaMemcpyDeviceToDevice, s);
+		if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
+		direction_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, beta, q, dv, pb);
+		sum_kernel<<<1, 1, 0, s>>>(pb, kFluidBlocks, sc + 2);
+		if ((st = check_launch("diffusion iteration kernels")) != IBK_OK) return st;
+		++it;
+	}
+	finish_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, u, x, out);
+	if (iterations) *iterations = it;
+	return check_launch("finish_kernel");
+}
+
+} // extern "C"

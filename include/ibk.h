@@ -461,6 +461,41 @@ ibk_status ibk_membrane_bending(ibk_surface_plan data_plan, ibk_surface_plan sam
                                 int preferred, int nc, const double* x_rest, const double* x_current,
                                 const ibk_surface* rest, const ibk_surface* current, double* f, void* stream);
 
+/* ---- The fluid step that consumes the spread: implicit diffusion --------
+ * ins::diffusion (include/ins/diffusion.h:12-78) on one component grid of a
+ * plan: with L the second-order finite-difference Laplacian and I~ the
+ * boundary-corrected identity of that grid (fd::laplacian, fd::identity with
+ * correction::second_order; include/fd/laplacian.h, identity.h,
+ * discretization.h:47-80), each a Kronecker sum / product of 1-D operators,
+ * a step with weight gamma (0.5 backward Euler, 1 Crank-Nicolson) is
+ *     out = u + (I~ - lambda L)^-1 (k I~ f + k mu (L u + rhs)),
+ *     k = gamma * timestep, lambda = timestep * mu / 2,
+ * solved by preconditioned conjugate gradients on the device with the
+ * reference's stopping rule: |d|_2 <= tolerance for the search direction d
+ * (include/solvers/pcg.h:12-45).  Periodic axes wrap; on a solid axis each
+ * side takes a Robin condition a u + b du/dn (Dirichlet {1, 0}, Neumann
+ * {0, 1}; include/fd/boundary.h:31-42); the boundary data enter through rhs. */
+typedef struct ibk_diffusion_s* ibk_diffusion;
+
+/* robin[d][side][0..1]: (a, b) of the lower (side 0) and upper (side 1) wall
+ * of axis d (ignored on periodic axes).  mu: diffusivity (viscosity /
+ * density) in internal units; timestep in internal units; max_iterations
+ * bounds each solve.  Allocates the component's working vectors. */
+ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin[3][2][2], double timestep,
+                                double mu, double tolerance, int max_iterations, ibk_diffusion* out);
+ibk_status ibk_diffusion_destroy(ibk_diffusion d);
+
+/* out = op(u) over the component grid: op 0 = L, 1 = I~, 2 = I~ - lambda L. */
+ibk_status ibk_diffusion_apply(ibk_diffusion d, int op, const double* u, double* out, void* stream);
+
+/* One step (ins::diffusion::operator(), diffusion.h:47-56): u, rhs, f and
+ * out are component-grid vectors (ibk_grid_info.size[component] doubles;
+ * out may alias u).  Synchronises the stream once per solver iteration to
+ * test convergence; *iterations (optional) receives the iteration count.
+ * IBK_ERR_DEVICE_CHECK when max_iterations pass without convergence. */
+ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, const double* rhs, const double* f,
+                              double* out, int* iterations, void* stream);
+
 /* Human-readable text of the last error on the calling host thread. */
 const char* ibk_last_error(void);
 const char* ibk_status_string(ibk_status status);

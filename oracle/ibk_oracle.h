@@ -105,6 +105,17 @@ void ibo_membrane_bending(int ns, int nd, int nc, const double* const* data_ops,
                           const double* const* sample_ops, double modulus, int preferred, const double* x_rest,
                           const double* x_cur, const double* const* rest, const double* const* cur, double* f);
 
+/* Implicit diffusion step on one component grid (ibk_fluid_oracle.c):
+ * points / periodic / shift per axis (dims of them), res the resolution,
+ * robin[axis][side][2] the wall conditions (a, b).  ibo_wall_weights: out =
+ * {interior, laplacian, boundary} weights of one wall (signed h). */
+void ibo_wall_weights(const double* p, double h, double s_in, double* out);
+void ibo_diffusion_apply(int dims, const int* points, const int* periodic, const double* shift, double res,
+                         const double* robin, double lambda, int op, const double* u, double* out);
+int ibo_diffusion_step(int dims, const int* points, const int* periodic, const double* shift, double res,
+                       const double* robin, double timestep, double mu, double tolerance, int max_iterations,
+                       double gamma, const double* u, const double* rhs, const double* f, double* out);
+
 #ifdef __cplusplus
 }
 #endif

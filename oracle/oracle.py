@@ -117,6 +117,13 @@ def lib():
                                                _dp, _dp, ctypes.POINTER(_dp)]
             L.ibo_membrane_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
+            L.ibo_wall_weights.argtypes = [_dp, ctypes.c_double, ctypes.c_double, _dp]
+            L.ibo_diffusion_apply.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, _dp, ctypes.c_double,
+                                              ctypes.c_int, _dp, _dp]
+            L.ibo_diffusion_step.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, _dp, ctypes.c_double,
+                                             ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
+                                             _dp, _dp, _dp, _dp]
+            L.ibo_diffusion_step.restype = ctypes.c_int
             L.ibo_membrane_bending.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp), _dp,
                                                ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int, _dp, _dp,
                                                ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
@@ -144,6 +151,7 @@ def ref():
             R.ibref_phi.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_double]
             R.ibref_phi.restype = ctypes.c_double
             R.ibref_domain_unit.argtypes = [ctypes.c_int, _dp]
+            R.ibref_wall_weights.argtypes = [ctypes.c_double] * 7 + [_dp]
             R.ibref_domain_unit.restype = ctypes.c_double
             _ref = R
     return _ref
@@ -317,3 +325,55 @@ def ref_stencil(g: Geom, comp: int, x):
     if rc != 0:
         raise ValueError("reference bridge does not cover this configuration")
     return keys, base, delta, w, sidx, iidx, geo
+
+
+class FluidGrid:
+    """One component grid for the diffusion oracle: points, periodicity and
+    shift per axis (from a Geom), the resolution, and the wall conditions
+    robin[axis][side] = (a, b)."""
+
+    def __init__(self, g, comp, robin):
+        self.dims = g.dims
+        self.points = np.array(g.comp_points(comp) + [1] * (3 - g.dims), dtype=np.int32)
+        self.periodic = np.array([0 if g.solid[d] else 1 for d in range(g.dims)] + [1] * (3 - g.dims), dtype=np.int32)
+        self.shift = np.array([g.shift[comp][d] for d in range(g.dims)] + [0.0] * (3 - g.dims))
+        self.res = float(g.resolution)
+        self.robin = np.ascontiguousarray(np.asarray(robin, dtype=np.float64).reshape(3, 2, 2))
+        self.size = int(np.prod(self.points))
+
+
+def wall_weights(p, h, s):
+    """{interior, laplacian, boundary} ghost-point weights of one wall
+    (include/fd/discretization.h:47-80)."""
+    out = np.zeros(3)
+    lib().ibo_wall_weights(_d(np.ascontiguousarray(p, dtype=np.float64)), float(h), float(s), _d(out))
+    return out
+
+
+def diffusion_apply(fg: FluidGrid, op, u, lam=0.0):
+    u = np.ascontiguousarray(u, dtype=np.float64)
+    out = np.zeros(fg.size)
+    lib().ibo_diffusion_apply(fg.dims, _i(fg.points), _i(fg.periodic), _d(fg.shift), fg.res, _d(fg.robin),
+                              float(lam), int(op), _d(u), _d(out))
+    return out
+
+
+def diffusion_step(fg: FluidGrid, timestep, mu, tolerance, max_iterations, gamma, u, rhs, f):
+    """out = u + (I~ - lambda L)^-1 (k I~ f + k mu (L u + rhs)) and the
+    iteration count (include/ins/diffusion.h:47-56)."""
+    u, rhs, f = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, rhs, f))
+    out = np.zeros(fg.size)
+    it = lib().ibo_diffusion_step(fg.dims, _i(fg.points), _i(fg.periodic), _d(fg.shift), fg.res, _d(fg.robin),
+                                  float(timestep), float(mu), float(tolerance), int(max_iterations), float(gamma),
+                                  _d(u), _d(rhs), _d(f), _d(out))
+    return out, it
+
+
+def ref_wall_weights(length, resolution, shift, lower, upper):
+    """The reference's own wall weights (bridge): {interior, laplacian,
+    boundary} of the lower and of the upper wall."""
+    out = np.zeros(6)
+    ref().ibref_wall_weights(float(length), float(resolution), float(shift), float(lower[0]), float(lower[1]),
+                             float(upper[0]), float(upper[1]), _d(out))
+    return out[:3], out[3:]
+

@@ -284,6 +284,24 @@ ibref_phi(int kind, int order, double r)
 	return 0;
 }
 
+/* Wall weights of the reference's fd::discretization over Robin walls
+ * (include/fd/discretization.h:47-80, 159-164): out = {lower interior, lower
+ * laplacian (second-order correction), lower boundary, the same for the
+ * upper wall}. */
+void
+ibref_wall_weights(double length, double resolution, double shift, double la, double lb, double ua, double ub,
+                   double* out)
+{
+	using robin_t = fd::boundary::robin;
+	fd::dimension<robin_t, robin_t> dim{length, robin_t(la, lb), robin_t(ua, ub)};
+	fd::discretization<fd::dimension<robin_t, robin_t>> disc{dim, fd::alignment{shift}, resolution};
+	const auto in = disc.interior();
+	const auto bd = disc.boundary();
+	const auto lp = disc.coefficient(fd::correction::second_order);
+	out[0] = in.lower; out[1] = lp.lower; out[2] = bd.lower;
+	out[3] = in.upper; out[4] = lp.upper; out[5] = bd.upper;
+}
+
 /* fd::domain::unit(): GCD of the dimension lengths (include/fd/domain.h:30-32) */
 double
 ibref_domain_unit(int dims, const double* length)
