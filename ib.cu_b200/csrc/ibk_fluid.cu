@@ -48,6 +48,22 @@ struct FluidOps {
 	double lambda;
 };
 
+// Axis coordinates of face idx (x fastest); 32-bit arithmetic below 2^31 faces.
+__device__ __forceinline__ void face_coords(long long idx, int P0, int P1, int& i, int& j, int& k)
+{
+	if (idx < 0x7fffffffLL) {
+		const unsigned u = (unsigned) idx, r = u / (unsigned) P0;
+		i = (int) (u - r * (unsigned) P0);
+		j = (int) (r % (unsigned) P1);
+		k = (int) (r / (unsigned) P1);
+	} else {
+		i = (int) (idx % P0);
+		const long long r = idx / P0;
+		j = (int) (r % P1);
+		k = (int) (r / P1);
+	}
+}
+
 __device__ __forceinline__ double axis_apply(const AxisOps& a, const double* __restrict__ u, long long idx, int i,
                                              long long stride)
 {
@@ -67,10 +83,8 @@ apply_kernel(FluidOps o, int op, const double* __restrict__ u, double* __restric
 	const int P0 = o.ax[0].P, P1 = o.ax[1].P;
 	for (long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x; idx < o.size;
 	     idx += (long long) gridDim.x * blockDim.x) {
-		const int i = (int) (idx % P0);
-		const long long r = idx / P0;
-		const int j = (int) (r % P1);
-		const int k = (int) (r / P1);
+		int i, j, k;
+		face_coords(idx, P0, P1, i, j, k);
 		const double ix = o.ax[0].id[i], iy = o.dims > 1 ? o.ax[1].id[j] : 1.0;
 		const double iz = o.dims > 2 ? o.ax[2].id[k] : 1.0;
 		double v = 0.0;
@@ -96,23 +110,21 @@ apply_kernel(FluidOps o, int op, const double* __restrict__ u, double* __restric
 	}
 }
 
-// Diagonal of I~ - lambda L (the Jacobi preconditioner).
+// Reciprocal of the diagonal of I~ - lambda L (the Jacobi preconditioner).
 __global__ void __launch_bounds__(kFluidThreads)
 diagonal_kernel(FluidOps o, double* __restrict__ diag)
 {
 	const int P0 = o.ax[0].P, P1 = o.ax[1].P;
 	for (long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x; idx < o.size;
 	     idx += (long long) gridDim.x * blockDim.x) {
-		const int i = (int) (idx % P0);
-		const long long r = idx / P0;
-		const int j = (int) (r % P1);
-		const int k = (int) (r / P1);
+		int i, j, k;
+		face_coords(idx, P0, P1, i, j, k);
 		const double ix = o.ax[0].id[i], iy = o.dims > 1 ? o.ax[1].id[j] : 1.0;
 		const double iz = o.dims > 2 ? o.ax[2].id[k] : 1.0;
 		double l = iz * iy * o.ax[0].diag[i];
 		if (o.dims > 1) l += iz * o.ax[1].diag[j] * ix;
 		if (o.dims > 2) l += o.ax[2].diag[k] * iy * ix;
-		diag[idx] = iz * iy * ix - o.lambda * l;
+		diag[idx] = 1.0 / (iz * iy * ix - o.lambda * l);   // the preconditioner's reciprocal
 	}
 }
 
@@ -147,14 +159,15 @@ rhs_kernel(long long n, double k, double kmu, const double* __restrict__ lu, con
 		b[i] = k * idf[i] + kmu * (lu[i] + rhs0[i]);
 }
 
-// Start of the loop: x = 0, d = M^-1 r, partials of r . d and d . d.
+// Start of the loop: x = 0, d = M^-1 r (dinv: the reciprocal diagonal),
+// partials of r . d and d . d.
 __global__ void __launch_bounds__(kFluidThreads)
 start_kernel(long long n, const double* __restrict__ r, const double* __restrict__ diag, double* __restrict__ x,
              double* __restrict__ d, double* __restrict__ rd, double* __restrict__ dd)
 {
 	double a = 0.0, b = 0.0;
 	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
-		const double z = r[i] / diag[i];
+		const double z = r[i] * diag[i];
 		x[i] = 0.0;
 		d[i] = z;
 		a += r[i] * z;
@@ -165,17 +178,43 @@ start_kernel(long long n, const double* __restrict__ r, const double* __restrict
 	block_partial(b, dd);
 }
 
-// x += alpha d, r -= alpha q, q = M^-1 r; partial sums of r . q.
-__global__ void __launch_bounds__(kFluidThreads)
-update_kernel(long long n, double alpha, const double* __restrict__ d, double* __restrict__ q, double* __restrict__ x,
-              double* __restrict__ r, const double* __restrict__ diag, double* __restrict__ rq)
+// Device scalars of the loop (sc): [0] delta = r . M^-1 r, [1] nu = d . H d,
+// [2] |d|^2, [3] alpha, [4] beta, [5] stop (1 when nu fell below tol^2).
+
+// nu from its partials; alpha = delta / nu, or stop (pcg.h:23-31).
+__global__ void alpha_kernel(const double* __restrict__ partial, int n, double tol2, double* __restrict__ sc)
 {
+	double t = 0.0;
+	for (int b = 0; b < n; ++b) t += partial[b];
+	sc[1] = t;
+	if (fabs(t) < tol2) { sc[5] = 1.0; sc[3] = 0.0; return; }
+	sc[3] = sc[0] / t;
+}
+
+// delta_new from its partials; beta = delta_new / delta (pcg.h:36-39).
+__global__ void beta_kernel(const double* __restrict__ partial, int n, double* __restrict__ sc)
+{
+	if (sc[5] != 0.0) return;
+	double t = 0.0;
+	for (int b = 0; b < n; ++b) t += partial[b];
+	sc[4] = t / sc[0];
+	sc[0] = t;
+}
+
+// x += alpha d, r -= alpha q, q = M^-1 r; partial sums of r . q.  Does
+// nothing once the loop has stopped.
+__global__ void __launch_bounds__(kFluidThreads)
+update_kernel(long long n, const double* __restrict__ sc, const double* __restrict__ d, double* __restrict__ q,
+              double* __restrict__ x, double* __restrict__ r, const double* __restrict__ dinv, double* __restrict__ rq)
+{
+	if (sc[5] != 0.0) return;
+	const double alpha = sc[3];
 	double a = 0.0;
 	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
 		x[i] += alpha * d[i];
 		const double ri = r[i] - alpha * q[i];
 		r[i] = ri;
-		const double z = ri / diag[i];
+		const double z = ri * dinv[i];
 		q[i] = z;
 		a += ri * z;
 	}
@@ -184,8 +223,11 @@ update_kernel(long long n, double alpha, const double* __restrict__ d, double* _
 
 // d = q + beta d; partial sums of d . d.
 __global__ void __launch_bounds__(kFluidThreads)
-direction_kernel(long long n, double beta, const double* __restrict__ q, double* __restrict__ d, double* __restrict__ dd)
+direction_kernel(long long n, const double* __restrict__ sc, const double* __restrict__ q, double* __restrict__ d,
+                 double* __restrict__ dd)
 {
+	if (sc[5] != 0.0) return;
+	const double beta = sc[4];
 	double a = 0.0;
 	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
 		const double v = q[i] + beta * d[i];
@@ -236,7 +278,7 @@ struct ibk_diffusion_s {
 	double* coef = nullptr;        // per axis: lo, diag, hi, id (4 P_d doubles)
 	double* work = nullptr;        // b, r, d, q, x, diag, tmp (7 size doubles)
 	double* partial = nullptr;     // 2 * kFluidBlocks partial sums
-	double* scalars = nullptr;     // device scalars: [0] r.d / r.q, [1] d.q, [2] d.d
+	double* scalars = nullptr;     // device scalars of the loop (see alpha_kernel)
 };
 
 extern "C" {
@@ -311,7 +353,7 @@ ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin
 	cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d->coef), sizeof(double) * (size_t) total);
 	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->work), sizeof(double) * 7 * (size_t) size);
 	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->partial), sizeof(double) * 2 * kFluidBlocks);
-	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->scalars), sizeof(double) * 4);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->scalars), sizeof(double) * 8);
 	if (e == cudaSuccess) e = cudaMemcpy(d->coef, host.data(), sizeof(double) * (size_t) total, cudaMemcpyHostToDevice);
 	if (e != cudaSuccess) {
 		cudaGetLastError();
@@ -332,7 +374,7 @@ ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin
 			ax.periodic = 0;
 		}
 	}
-	// the preconditioner's diagonal, kept in work slot 5
+	// the preconditioner's reciprocal diagonal, kept in work slot 5
 	diagonal_kernel<<<kFluidBlocks, kFluidThreads>>>(d->ops, d->work + 5 * size);
 	ibk_status st = check_launch("diagonal_kernel");
 	if (st == IBK_OK && (e = cudaDeviceSynchronize()) != cudaSuccess) st = cuda_fail(e, "diffusion set-up");
@@ -395,40 +437,33 @@ ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, co
 	sum_kernel<<<1, 1, 0, s>>>(pb, kFluidBlocks, sc + 2);
 	ibk_status st = check_launch("diffusion set-up kernels");
 	if (st != IBK_OK) return st;
-	double hs[3];
+	e = cudaMemsetAsync(sc + 5, 0, sizeof(double), s);
+	if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
 	const double tol = d->tolerance;
 	int it = 0;
+	double hs[6];
 	for (;;) {
-		// pcg.h:21-42, the scalars read back once per iteration
-		e = cudaMemcpyAsync(hs, sc, sizeof(double) * 3, cudaMemcpyDeviceToHost, s);
+		// the loop test of pcg.h:21 (|d| > tol) and its bail-out, read back once
+		// per iteration; alpha and beta stay on the device
+		e = cudaMemcpyAsync(hs, sc, sizeof(double) * 6, cudaMemcpyDeviceToHost, s);
 		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
 		if (e != cudaSuccess) return cuda_fail(e, "diffusion residual read");
-		if (!(std::sqrt(hs[2]) > tol)) break;
+		if (hs[5] != 0.0 || !(std::sqrt(hs[2]) > tol)) break;
 		if (it >= d->max_iterations) {
 			if (iterations) *iterations = it;
 			return set_error(IBK_ERR_DEVICE_CHECK, "diffusion solve did not converge within max_iterations");
 		}
 		apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 2, dv, q, pa);
-		sum_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc + 1);
-		e = cudaMemcpyAsync(hs + 1, sc + 1, sizeof(double), cudaMemcpyDeviceToHost, s);
-		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-		if (e != cudaSuccess) return cuda_fail(e, "diffusion curvature read");
-		const double nu = hs[1];
-		if (std::abs(nu) < tol * tol) break;   // pcg.h:26-31: no further progress possible
-		const double alpha = hs[0] / nu;
-		update_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, alpha, dv, q, x, r, diag, pa);
-		sum_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc + 3);
-		e = cudaMemcpyAsync(hs + 2, sc + 3, sizeof(double), cudaMemcpyDeviceToHost, s);
-		if (e == cudaSuccess) e = cudaStreamSynchronize(s);
-		if (e != cudaSuccess) return cuda_fail(e, "diffusion residual read");
-		const double beta = hs[2] / hs[0];
-		e = cudaMemcpyAsync(sc, sc + 3, sizeof(double), cudaMemcpyDeviceToDevice, s);
-		if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
-		direction_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, beta, q, dv, pb);
+		alpha_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, tol * tol, sc);
+		update_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, dv, q, x, r, diag, pa);
+		beta_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc);
+		direction_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, q, dv, pb);
 		sum_kernel<<<1, 1, 0, s>>>(pb, kFluidBlocks, sc + 2);
 		if ((st = check_launch("diffusion iteration kernels")) != IBK_OK) return st;
 		++it;
 	}
+	// a bail-out leaves the last iteration's update undone, as pcg.h does
+	if (hs[5] != 0.0 && it > 0) --it;
 	finish_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, u, x, out);
 	if (iterations) *iterations = it;
 	return check_launch("finish_kernel");

@@ -148,7 +148,7 @@ int ibo_diffusion_step(int dims, const int* points, const int* periodic, const d
 	apply(&o, 0, u, lu);
 	apply(&o, 1, f, idf);
 	for (long long i = 0; i < n; ++i) b[i] = k * idf[i] + k * mu * (lu[i] + rhs[i]);
-	/* Jacobi diagonal of I~ - lambda L */
+	/* Jacobi preconditioner: the reciprocal diagonal of I~ - lambda L */
 	const int P0 = o.P[0], P1 = o.P[1];
 	for (long long idx = 0; idx < n; ++idx) {
 		const int i = (int) (idx % P0);
@@ -159,10 +159,10 @@ int ibo_diffusion_step(int dims, const int* points, const int* periodic, const d
 		double l = iz * iy * o.dg[0][i];
 		if (dims > 1) l += iz * o.dg[1][j] * ix;
 		if (dims > 2) l += o.dg[2][kk] * iy * ix;
-		diag[idx] = iz * iy * ix - o.lambda * l;
+		diag[idx] = 1.0 / (iz * iy * ix - o.lambda * l);      /* reciprocal */
 	}
 	double* rr = b;    /* the residual starts as b */
-	for (long long i = 0; i < n; ++i) d[i] = rr[i] / diag[i];
+	for (long long i = 0; i < n; ++i) d[i] = rr[i] * diag[i];
 	double delta = dot(rr, d, n);
 	int it = 0;
 	while (sqrt(dot(d, d, n)) > tolerance) {
@@ -173,7 +173,7 @@ int ibo_diffusion_step(int dims, const int* points, const int* periodic, const d
 		const double alpha = delta / nu;
 		for (long long i = 0; i < n; ++i) x[i] += alpha * d[i];
 		for (long long i = 0; i < n; ++i) rr[i] -= alpha * q[i];
-		for (long long i = 0; i < n; ++i) q[i] = rr[i] / diag[i];
+		for (long long i = 0; i < n; ++i) q[i] = rr[i] * diag[i];
 		const double old = delta;
 		delta = dot(rr, q, n);
 		const double beta = delta / old;
