@@ -103,12 +103,14 @@ class _InstanceIO(ctypes.Structure):
 
 class BatchConfig(ctypes.Structure):
     _fields_ = [("spread_tile", ctypes.c_int * 3), ("interp_tile", ctypes.c_int * 3),
-                ("spread_ctas_per_sm", ctypes.c_int), ("interp_ctas_per_sm", ctypes.c_int)]
+                ("spread_ctas_per_sm", ctypes.c_int), ("interp_ctas_per_sm", ctypes.c_int),
+                ("spread_threads", ctypes.c_int)]
 
     def as_dict(self):
         return {"spread_tile": list(self.spread_tile), "interp_tile": list(self.interp_tile),
                 "spread_ctas_per_sm": self.spread_ctas_per_sm,
-                "interp_ctas_per_sm": self.interp_ctas_per_sm}
+                "interp_ctas_per_sm": self.interp_ctas_per_sm,
+                "spread_threads": self.spread_threads or 256}
 
 
 class IoHeader(ctypes.Structure):
@@ -586,13 +588,14 @@ class Batch:
         check(lib().ibk_batch_capture(self._h, int(op)))
 
     def configure(self, spread_tile=(16, 16, 16), interp_tile=(16, 16, 16),
-                  spread_ctas_per_sm=0, interp_ctas_per_sm=0):
+                  spread_ctas_per_sm=0, interp_ctas_per_sm=0, spread_threads=0):
         c = BatchConfig()
         for d in range(3):
             c.spread_tile[d] = int(spread_tile[d])
             c.interp_tile[d] = int(interp_tile[d])
         c.spread_ctas_per_sm = int(spread_ctas_per_sm)
         c.interp_ctas_per_sm = int(interp_ctas_per_sm)
+        c.spread_threads = int(spread_threads)
         check(lib().ibk_batch_configure(self._h, ctypes.byref(c)))
 
     def config(self) -> dict:

@@ -205,8 +205,8 @@ __device__ __forceinline__ void next_item(int* next, int nitems, int nact, const
 
 // Persistent spread over the active instances' items: tiles (FP32C, every
 // component) or (tile, component) (FP64).
-template <typename D, int DIMS, int PREC>
-__global__ void __launch_bounds__(kTileThreads, PREC == IBK_PRECISION_FP32C ? 4 : 3)
+template <typename D, int DIMS, int PREC, int NT = kTileThreads>
+__global__ void __launch_bounds__(NT, PREC == IBK_PRECISION_FP32C ? 1024 / NT : 3)
 batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __restrict__ next,
                     const PointRec* __restrict__ recs, const int* __restrict__ off, const unsigned* __restrict__ binmax,
                     int step, Deferral defer)
@@ -227,8 +227,8 @@ batch_spread_kernel(const BatchInst* __restrict__ insts, BatchTable t, int* __re
 		if constexpr (PREC == IBK_PRECISION_FP32C) {
 			const BinStatsView bs{binmax + (size_t) si.bin_s * kMaxDims};
 			// a dense tile is deferred by its work-item index
-			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
-			                           off + si.bin_s, bs, fe, local, -1, defer, item);
+			spread_tile<D, DIMS, PREC, false, NT>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs,
+			                                      so.pbase, off + si.bin_s, bs, fe, local, -1, defer, item);
 		} else {
 			spread_tile<D, DIMS, PREC>(si.g, si.ts, so.n, step ? so.xn : so.x, step ? so.fs : so.fl, recs, so.pbase,
 			                           off + si.bin_s, BinStatsView{nullptr}, fe, local / DIMS, local % DIMS);
@@ -449,8 +449,12 @@ ibk_status batch_run_impl(Batch& b, int op, cudaStream_t s)
 			ibk_status ds = cuda_check(cudaMemsetAsync(b.d_defer, 0, sizeof(int), s), "cudaMemsetAsync");
 			if (ds != IBK_OK) return ds;
 		}
-		batch_spread_kernel<D, DIMS, PREC><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
-			b.d_inst, t, b.d_next, b.d_recs, b.d_off, b.d_binmax, step ? 1 : 0, defer);
+		if (PREC == IBK_PRECISION_FP32C && b.config.spread_threads == 512)
+			batch_spread_kernel<D, DIMS, PREC, 512><<<b.grid_s, 512, b.smem_s, s>>>(
+				b.d_inst, t, b.d_next, b.d_recs, b.d_off, b.d_binmax, step ? 1 : 0, defer);
+		else
+			batch_spread_kernel<D, DIMS, PREC><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
+				b.d_inst, t, b.d_next, b.d_recs, b.d_off, b.d_binmax, step ? 1 : 0, defer);
 		b.launches += 1;
 		if (PREC == IBK_PRECISION_FP32C) {
 			batch_spread_dense_kernel<D, DIMS><<<b.grid_s, kTileThreads, b.smem_s, s>>>(
@@ -482,7 +486,9 @@ template <int KIND, int ORDER, int DIMS, int PREC>
 ibk_status batch_prepare_impl(Batch& b)
 {
 	using D = Delta<KIND, ORDER>;
-	auto ks = batch_spread_kernel<D, DIMS, PREC>;
+	const bool wide = PREC == IBK_PRECISION_FP32C && b.config.spread_threads == 512;
+	auto ks = wide ? batch_spread_kernel<D, DIMS, PREC, 512> : batch_spread_kernel<D, DIMS, PREC>;
+	const int nts = wide ? 512 : kTileThreads;
 	auto ki = batch_interp_kernel<D, DIMS, PREC>;
 	ibk_status st;
 	if constexpr (PREC == IBK_PRECISION_FP32C) {
@@ -495,7 +501,7 @@ ibk_status batch_prepare_impl(Batch& b)
 	if ((st = cuda_check(cudaFuncSetAttribute(ki, cudaFuncAttributeMaxDynamicSharedMemorySize, (int) b.smem_i),
 	                     "cudaFuncSetAttribute")) != IBK_OK) return st;
 	int occ_s = 0, occ_i = 0;
-	if ((st = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, ks, kTileThreads, b.smem_s),
+	if ((st = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_s, ks, nts, b.smem_s),
 	                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor")) != IBK_OK) return st;
 	if ((st = cuda_check(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&occ_i, ki, kTileThreads, b.smem_i),
 	                     "cudaOccupancyMaxActiveBlocksPerMultiprocessor")) != IBK_OK) return st;
@@ -952,6 +958,9 @@ ibk_status ibk_batch_configure(ibk_batch handle, const ibk_batch_config* config)
 			return set_error(IBK_ERR_INVALID_ARGUMENT, "tile extents must lie in [2, 64]");
 	if (config->spread_ctas_per_sm < 0 || config->interp_ctas_per_sm < 0)
 		return set_error(IBK_ERR_INVALID_ARGUMENT, "negative CTAs per SM");
+	if (config->spread_threads != 0 && config->spread_threads != kTileThreads &&
+	    !(config->spread_threads == 512 && b->precision == IBK_PRECISION_FP32C))
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "spread threads per CTA: 256, or 512 with FP32C");
 	const ibk_batch_config old = b->config;
 	ibk_status st = configure(*b, *config);
 	if (st != IBK_OK) configure(*b, old);
@@ -1010,6 +1019,15 @@ ibk_status ibk_batch_tune(ibk_batch handle, int op, void* stream, ibk_batch_conf
 				if (cs == IBK_ERR_UNSUPPORTED) continue;     // shape does not fit in shared memory
 				if (cs != IBK_OK) { st = cs; break; }
 				if (ms < best_ms) { best_ms = ms; cur = c; }
+			}
+			// threads per spread CTA (points of a tile shared by more threads)
+			if (spread_pass && b->precision == IBK_PRECISION_FP32C && st == IBK_OK) {
+				ibk_batch_config c = cur;
+				c.spread_threads = cur.spread_threads == 512 ? kTileThreads : 512;
+				float ms = 0.0f;
+				ibk_status cs = time_cfg(c, ms);
+				if (cs != IBK_OK && cs != IBK_ERR_UNSUPPORTED) st = cs;
+				else if (cs == IBK_OK && ms < best_ms) { best_ms = ms; cur = c; }
 			}
 			// persistent CTAs per SM for the chosen shape
 			for (int occ = 1; occ <= 4 && st == IBK_OK; ++occ) {

@@ -246,13 +246,16 @@ typedef enum {
 } ibk_batch_op;
 
 /* Launch shape of a batch: preferred tile extents in cells per axis (shrunk
- * per instance so the last tile keeps at least M cells) and persistent CTAs
- * per SM (0: as many as fit). */
+ * per instance so the last tile keeps at least M cells), persistent CTAs per
+ * SM (0: as many as fit) and threads per spread CTA (0 or 256; 512 with
+ * FP32C: the points of a tile shared by more threads, half as many CTAs per
+ * SM). */
 typedef struct {
 	int spread_tile[3];
 	int interp_tile[3];
 	int spread_ctas_per_sm;
 	int interp_ctas_per_sm;
+	int spread_threads;
 } ibk_batch_config;
 
 /* max_points bounds the sum of the bound point counts; all scratch is

@@ -237,6 +237,28 @@ def test_tune_keeps_results_within_fp32c_bar(ibk, cuda):
             assert np.abs(a - b).max() <= FP32C_TOL * np.abs(b).max()
 
 
+def test_spread_threads_per_cta_keep_the_result(ibk, cuda):
+    """512 threads per FP32C spread CTA sum the same exact fixed-point terms as
+    256: the grids are identical bit for bit."""
+    import torch
+    batch, cases = _make(ibk, 1, cuda)
+    batch.bind([c.io() for c in cases])
+    out = []
+    for threads in (256, 512):
+        batch.configure(spread_threads=threads)
+        assert batch.config()["spread_threads"] == threads
+        for c in cases:
+            for a in c.fe:
+                a.fill_(np.nan)
+        batch.run(ibk.OP_SPREAD)
+        torch.cuda.synchronize()
+        out.append([a.cpu().numpy().copy() for c in cases for a in c.fe])
+    for a, b in zip(*out):
+        assert np.array_equal(a, b)
+    with pytest.raises(ibk.IbkError):
+        batch.configure(spread_threads=384)
+
+
 def test_bind_beyond_capacity_is_rejected(ibk, cuda):
     batch, cases = _make(ibk, 1, cuda, capacity_extra=-1)
     with pytest.raises(ibk.IbkError) as e:
