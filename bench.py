@@ -813,8 +813,11 @@ def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
     per-sample normal and patch area) and the Skalak tension from it and the
     rest geometry (computed once), then the bending force (the curvature field
     at the data sites through the data-site operators, its derivatives at the
-    samples).  Random operators and positions of the reference's shapes: the
-    timing does not depend on their values."""
+    samples), then the viscous dissipation (the velocity's five derivatives
+    at the samples, then the per-sample stress divergence): the reference's
+    red-cell force set (test/ib-whole.cc:210-213).  Random operators,
+    positions and velocities of the reference's shapes: the timing does not
+    depend on their values."""
     import torch
     gen = torch.Generator(device=dev)
     gen.manual_seed(11)
@@ -827,9 +830,10 @@ def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
     x0 = torch.randn(3 * nd * nc, generator=gen, dtype=torch.float64, device=dev)
     x1 = x0 + 0.01 * torch.randn(3 * nd * nc, generator=gen, dtype=torch.float64, device=dev)
     rest = plan.geometry(x0, nc)
+    vel = torch.randn(3 * nd * nc, generator=gen, dtype=torch.float64, device=dev)
     stream = torch.cuda.current_stream()
-    ev = [torch.cuda.Event(enable_timing=True) for _ in range(4)]
-    geo_ms, ten_ms, ben_ms = [], [], []
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(5)]
+    geo_ms, ten_ms, ben_ms, dis_ms = [], [], [], []
     for it in range(warmup + steps):
         ev[0].record(stream)
         cur = plan.geometry(x1, nc)
@@ -838,21 +842,27 @@ def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
         ev[2].record(stream)
         fb = ibk.membrane_bending(dplan, plan, 1.0, False, None, x1, None, cur, nc)
         ev[3].record(stream)
+        fd = ibk.membrane_dissipation(plan, 0.25, vel, cur, nc)
+        ev[4].record(stream)
         torch.cuda.synchronize()
         if it >= warmup:
             geo_ms.append(ev[0].elapsed_time(ev[1]))
             ten_ms.append(ev[1].elapsed_time(ev[2]))
             ben_ms.append(ev[2].elapsed_time(ev[3]))
-        del cur, f, fb
+            dis_ms.append(ev[3].elapsed_time(ev[4]))
+        del cur, f, fb, fd
     g, t, b = float(np.median(geo_ms)), float(np.median(ten_ms)), float(np.median(ben_ms))
+    d = float(np.median(dis_ms))
     bflops = (5 * 2.0 * nd * nd * 3 * nc) + (5 * 2.0 * ns * nd * nc)
+    dflops = 5 * 2.0 * ns * nd * 3 * nc
     flops = 6 * 2.0 * ns * nd * 3 * nc
     tbytes = (2 * 15 + 1 + 3) * 8.0 * ns * nc     # rest t, tt and area + current t, tt read; f written
     peak, _ = measured_peaks()
-    del plan, dplan, rest
+    del plan, dplan, rest, vel
     torch.cuda.empty_cache()
     return {"shapes": nc, "data_sites": nd, "samples": ns, "law": "skalak", "steps": steps,
-            "ms_per_step": g + t + b, "geometry_ms": g, "tension_ms": t, "bending_ms": b,
+            "ms_per_step": g + t + b + d, "geometry_ms": g, "tension_ms": t, "bending_ms": b,
+            "dissipation_ms": d, "dissipation_tflops": dflops / (d * 1e-3) / 1e12,
             "bending_gemm_tflops": bflops / (b * 1e-3) / 1e12,
             "geometry_tflops": flops / (g * 1e-3) / 1e12,
             "tension_gbs": tbytes / (t * 1e-3) / 1e9, "tension_frac_of_hbm": tbytes / (t * 1e-3) / 1e9 / peak,

@@ -37,7 +37,7 @@ PERIODIC, SOLID = 0, 1
 TAG_MAC, TAG_CENTERED = 0, 1
 BSPLINE, PESKIN, ROMA, COSINE, HAT = 0, 1, 2, 3, 4
 FP64, FP32C = 0, 1
-SKALAK, NEOHOOKEAN = 0, 1          # ibk_tension_law
+SKALAK, NEOHOOKEAN, HOOKEAN = 0, 1, 2    # ibk_tension_law
 
 # Every symbol include/ibk.h declares (checked by the CPU test suite).
 ABI_SYMBOLS = (
@@ -54,7 +54,7 @@ ABI_SYMBOLS = (
     "ibk_server_save", "ibk_server_admit_from",
     "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
     "ibk_surface_plan_create", "ibk_surface_plan_destroy", "ibk_surface_geometry", "ibk_membrane_tension",
-    "ibk_membrane_bending",
+    "ibk_membrane_bending", "ibk_membrane_dissipation", "ibk_membrane_tether", "ibk_membrane_repelling",
     "ibk_diffusion_create", "ibk_diffusion_destroy", "ibk_diffusion_apply", "ibk_diffusion_step",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
@@ -232,6 +232,12 @@ def lib() -> ctypes.CDLL:
         L.ibk_diffusion_step.argtypes = [_vp, ctypes.c_double, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int), _vp]
         L.ibk_membrane_bending.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                            ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
+        L.ibk_membrane_dissipation.argtypes = [_vp, ctypes.c_double, ctypes.c_int, _vp, ctypes.POINTER(_Surface),
+                                               _vp, _vp]
+        L.ibk_membrane_tether.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.POINTER(_Surface),
+                                          ctypes.POINTER(_Surface), _vp, _vp]
+        L.ibk_membrane_repelling.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                             ctypes.POINTER(_Surface), _vp, _vp]
         for name in ABI_SYMBOLS:
             if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_", "ibk_surface_", "ibk_membrane_",
                                 "ibk_diffusion_")) \
@@ -759,9 +765,10 @@ class SurfacePlan:
 
 
 def membrane_tension(law, shear, bulk, rest, current, stream=None):
-    """Tension force at every sample site (forces::tension with the Skalak or
-    neo-Hookean law, include/forces/tension.h:55-116) from the rest and
-    current geometry dicts; returns 3*npoints forces [component][site]."""
+    """Tension force at every sample site (forces::tension with the Skalak,
+    neo-Hookean or Hookean law, include/forces/tension.h:55-116) from the
+    rest and current geometry dicts; returns 3*npoints forces
+    [component][site]."""
     import torch
     n = int(rest["sigma"].numel())
     f = torch.empty(3 * n, dtype=torch.float64, device=rest["sigma"].device)
@@ -786,6 +793,47 @@ def membrane_bending(data_plan, sample_plan, modulus, preferred, x_rest, x_curre
     check(lib().ibk_membrane_bending(data_plan.handle, sample_plan.handle, modulus, int(bool(preferred)), nc,
                                      _ptr(x_rest), x_current.data_ptr(), ctypes.byref(r) if r is not None else None,
                                      ctypes.byref(c), f.data_ptr(), _stream_handle(stream)))
+    return f
+
+
+def membrane_dissipation(sample_plan, modulus, u, current, nc, stream=None):
+    """Viscous dissipation at every sample (forces::dissipation,
+    include/forces/dissipation.h:128-272): u is the data-site velocity
+    (3*nd*nc, [component][shape][site]), current the sample geometry dict;
+    returns 3*ns*nc forces."""
+    import torch
+    f = torch.empty(3 * sample_plan.ns * nc, dtype=torch.float64, device=u.device)
+    c = _surface_struct(current)
+    check(lib().ibk_membrane_dissipation(sample_plan.handle, modulus, nc, u.data_ptr(), ctypes.byref(c),
+                                         f.data_ptr(), _stream_handle(stream)))
+    return f
+
+
+def membrane_tether(modulus, rest, current, stream=None):
+    """Tether force modulus (rest position - current position) at every
+    sample (forces::tether, include/forces/tether.h:9-26)."""
+    import torch
+    n = int(current["position"].numel()) // 3
+    f = torch.empty(3 * n, dtype=torch.float64, device=current["position"].device)
+    r, c = _surface_struct(rest), _surface_struct(current)
+    check(lib().ibk_membrane_tether(modulus, n, ctypes.byref(r), ctypes.byref(c), f.data_ptr(),
+                                    _stream_handle(stream)))
+    return f
+
+
+REPELLING_HEIGHT, REPELLING_RANGE = 1.6, 0.025     # 16 um and 0.25 um in units of 10 um
+
+
+def membrane_repelling(modulus, current, height=REPELLING_HEIGHT, range_=REPELLING_RANGE, stream=None):
+    """Repulsion from the wall y = height (forces::repelling,
+    include/forces/repelling.h:9-49), reaching 2 range from it, at every
+    sample of the current geometry dict (position and sigma read)."""
+    import torch
+    n = int(current["sigma"].numel())
+    f = torch.empty(3 * n, dtype=torch.float64, device=current["sigma"].device)
+    c = _surface_struct(current)
+    check(lib().ibk_membrane_repelling(modulus, height, range_, n, ctypes.byref(c), f.data_ptr(),
+                                       _stream_handle(stream)))
     return f
 
 

@@ -2,10 +2,14 @@
 // shapes that share one set of RBF operators (bases::geometry<2>::compute,
 // include/bases/geometry.h:74-124) and the in-plane tension of a
 // hyperelastic membrane (forces::tension, include/forces/tension.h:9-118)
-// under the Skalak (include/forces/skalak.h:11-37) and neo-Hookean
-// (include/forces/neohookean.h:10-37) laws, and the bending force
-// (forces::bending, include/forces/bending.h:10-229).  These produce the
-// point forces that a spread takes.
+// under the Skalak (include/forces/skalak.h:11-37), neo-Hookean
+// (include/forces/neohookean.h:10-37) and Hookean
+// (include/forces/hookean.h:11-35) laws, the bending force (forces::bending,
+// include/forces/bending.h:10-229), the viscous dissipation
+// (forces::dissipation, include/forces/dissipation.h:128-272), the tether
+// (include/forces/tether.h:9-26) and the wall repulsion
+// (include/forces/repelling.h:9-49).  These produce the point forces that a
+// spread takes.
 //
 // Arithmetic: FP64.  Every per-sample expression is evaluated in the order
 // the reference writes it, with no contraction (the build compiles this file
@@ -82,6 +86,10 @@ __device__ __forceinline__ LawValues law_values(double e, double kappa, double i
 	if constexpr (LAW == IBK_LAW_SKALAK) {
 		// skalak.h:22-31
 		return {e * (i1 - 1), (kappa * (i2 - 1) - e), e, 0.0, kappa};
+	} else if constexpr (LAW == IBK_LAW_HOOKEAN) {
+		// hookean.h:19-30: a function of i1 alone; kappa unused
+		const double j = sqrt(i1);
+		return {e * (1 - 1. / j), 0.0, e / (2 * i1 * j), 0.0, 0.0};
 	} else {
 		// neohookean.h:22-32
 		const double j = sqrt(i2);
@@ -246,6 +254,101 @@ bending_kernel(long long n, SurfaceFull cur, SurfaceFull rest, int preferred, co
 	f[2 * n + p] = mag * nrm.z;
 }
 
+// Viscous dissipation at the samples (dissipation.h:216-265): the rate of
+// change of the metric and of the Christoffel symbols from the velocity's
+// derivatives (vd: u, v, uu, uv, vv, each 3n values [component][site]) and
+// the current geometry, the in-plane stress g^-1 g' adj(g) they give and its
+// surface divergence, times kappa sigma / det g.
+__global__ void __launch_bounds__(kMembraneThreads)
+dissipation_kernel(long long n, SurfaceIn cur, const double* __restrict__ vd, double kappa, double* __restrict__ f)
+{
+	const long long p = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	const V3 tu = load3(cur.t[0], n, p), tv = load3(cur.t[1], n, p);
+	const V3 tuu = load3(cur.tt[0], n, p), tuv = load3(cur.tt[1], n, p), tvv = load3(cur.tt[2], n, p);
+	const V3 su = load3(vd, n, p), sv = load3(vd + 3 * n, n, p);
+	const V3 suu = load3(vd + 6 * n, n, p), suv = load3(vd + 9 * n, n, p), svv = load3(vd + 12 * n, n, p);
+	const Metric m = metric(tu, tv, tuu, tuv, tvv);
+	const double e = m.e, ff = m.f, g = m.g, eu = m.eu, fu = m.fu, gu = m.gu, ev = m.ev, fv = m.fv, gv = m.gv;
+	const double i = m.i, iu = m.iu, iv = m.iv;
+
+	// dot_metric: g'_ij = t_i . u_j + u_i . t_j (dissipation.h:57-79)
+	const double de = dot(tu, su) + dot(su, tu);
+	const double df = dot(tu, sv) + dot(su, tv);
+	const double dg = dot(tv, sv) + dot(sv, tv);
+	// dot_christoffel: G'_ij,k = u_ij . t_k + t_ij . u_k (dissipation.h:89-127),
+	// and g'_ij,k = G'_ik,j + G'_kj,i (dissipation.h:193-206)
+	const double c00_0 = dot(suu, tu) + dot(tuu, su), c00_1 = dot(suu, tv) + dot(tuu, sv);
+	const double c01_0 = dot(suv, tu) + dot(tuv, su), c01_1 = dot(suv, tv) + dot(tuv, sv);
+	const double c11_0 = dot(svv, tu) + dot(tvv, su), c11_1 = dot(svv, tv) + dot(tvv, sv);
+	const double deu = 2 * c00_0, dfu = c00_1 + c01_0, dgu = 2 * c01_1;
+	const double dev = 2 * c01_0, dfv = c01_1 + c11_0, dgv = 2 * c11_1;
+
+	const double pig[4] = {(g * de - ff * df) / i, (g * df - ff * dg) / i,
+	                       (e * df - ff * de) / i, (e * dg - ff * df) / i};
+	const double pigu[4] = {
+		(gu * de + g * deu - fu * df - ff * dfu - iu * pig[0]) / i,
+		(gu * df + g * dfu - fu * dg - ff * dgu - iu * pig[1]) / i,
+		(eu * df + e * dfu - fu * de - ff * deu - iu * pig[2]) / i,
+		(eu * dg + e * dgu - fu * df - ff * dfu - iu * pig[3]) / i};
+	const double pigv[4] = {
+		(gv * de + g * dev - fv * df - ff * dfv - iv * pig[0]) / i,
+		(gv * df + g * dfv - fv * dg - ff * dgv - iv * pig[1]) / i,
+		(ev * df + e * dfv - fv * de - ff * dev - iv * pig[2]) / i,
+		(ev * dg + e * dgv - fv * df - ff * dfv - iv * pig[3]) / i};
+	const double pif[3] = {
+		pig[0] * g - pig[1] * ff,
+		0.5 * (pig[1] * e + pig[2] * g - (pig[0] + pig[3]) * ff),
+		pig[3] * e - pig[2] * ff};
+	const double pifu[3] = {
+		pigu[0] * g + pig[0] * gu - pigu[1] * ff - pig[1] * fu,
+		0.5 * (pigu[1] * e + pig[1] * eu + pigu[2] * g + pig[2] * gu
+		       - ((pigu[0] + pigu[3]) * ff + (pig[0] + pig[3]) * fu)),
+		pigu[3] * e + pig[3] * eu - pigu[2] * ff - pig[2] * fu};
+	const double pifv[3] = {
+		pigv[0] * g + pig[0] * gv - pigv[1] * ff - pig[1] * fv,
+		0.5 * (pigv[1] * e + pig[1] * ev + pigv[2] * g + pig[2] * gv
+		       - ((pigv[0] + pigv[3]) * ff + (pig[0] + pig[3]) * fv)),
+		pigv[3] * e + pig[3] * ev - pigv[2] * ff - pig[2] * fv};
+	const double c0 = pifu[0] + pifv[1] - (iu * pif[0] + iv * pif[1]) / (2 * i);
+	const double c1 = pifu[1] + pifv[2] - (iu * pif[1] + iv * pif[2]) / (2 * i);
+
+	const double scale = __ldg(cur.sigma + p) * kappa / i;
+	const double two_pif1 = 2 * pif[1];
+	const double uc[3] = {tu.x, tu.y, tu.z}, vc[3] = {tv.x, tv.y, tv.z};
+	const double uuc[3] = {tuu.x, tuu.y, tuu.z}, uvc[3] = {tuv.x, tuv.y, tuv.z}, vvc[3] = {tvv.x, tvv.y, tvv.z};
+#pragma unroll
+	for (int k = 0; k < 3; ++k)
+		f[k * n + p] = scale * (c0 * uc[k] + c1 * vc[k] + pif[0] * uuc[k] + two_pif1 * uvc[k] + pif[2] * vvc[k]);
+}
+
+// Tether (tether.h:14-22): modulus (x_rest - x_current), element by element
+// over 3n values.
+__global__ void __launch_bounds__(kMembraneThreads)
+tether_kernel(long long m, const double* __restrict__ xr, const double* __restrict__ xc, double modulus,
+              double* __restrict__ f)
+{
+	const long long p = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= m) return;
+	f[p] = modulus * (__ldg(xr + p) - __ldg(xc + p));
+}
+
+// Wall repulsion (repelling.h:15-45): r = |height - y| / range and, inside
+// r < 2, fy = -log(r / 2) exp(-4 / (4 - r^2)); f = -modulus (0, fy, 0) sigma.
+__global__ void __launch_bounds__(kMembraneThreads)
+repelling_kernel(long long n, const double* __restrict__ x, const double* __restrict__ sigma, double modulus,
+                 double height, double range, double* __restrict__ f)
+{
+	const long long p = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	const double r = fabs(height - __ldg(x + n + p)) / range;
+	const double fy = r < 2 ? -log(r / 2) * exp(-4 / (4 - r * r)) : 0.0;
+	const double fc[3] = {0.0, fy, 0.0};
+	const double s = __ldg(sigma + p);
+#pragma unroll
+	for (int k = 0; k < 3; ++k) f[k * n + p] = -modulus * fc[k] * s;
+}
+
 ibk_status blas_check(cublasStatus_t st, const char* what)
 {
 	if (st == CUBLAS_STATUS_SUCCESS) return IBK_OK;
@@ -374,7 +477,7 @@ ibk_status ibk_surface_geometry(ibk_surface_plan plan, int nc, const double* x, 
 ibk_status ibk_membrane_tension(int law, double shear, double bulk, int npoints, const ibk_surface* rest,
                                 const ibk_surface* current, double* f, void* stream)
 {
-	if (law != IBK_LAW_SKALAK && law != IBK_LAW_NEOHOOKEAN)
+	if (law != IBK_LAW_SKALAK && law != IBK_LAW_NEOHOOKEAN && law != IBK_LAW_HOOKEAN)
 		return set_error(IBK_ERR_INVALID_ARGUMENT, "unknown tension law");
 	if (npoints <= 0) return IBK_OK;
 	if (!rest || !current || !f) return set_error(IBK_ERR_INVALID_ARGUMENT, "null geometry or force array");
@@ -389,9 +492,58 @@ ibk_status ibk_membrane_tension(int law, double shear, double bulk, int npoints,
 	const long long n = npoints;
 	if (law == IBK_LAW_SKALAK)
 		tension_kernel<IBK_LAW_SKALAK><<<blocks_of(n), kMembraneThreads, 0, s>>>(n, r, c, shear, bulk, f);
-	else
+	else if (law == IBK_LAW_NEOHOOKEAN)
 		tension_kernel<IBK_LAW_NEOHOOKEAN><<<blocks_of(n), kMembraneThreads, 0, s>>>(n, r, c, shear, bulk, f);
+	else
+		tension_kernel<IBK_LAW_HOOKEAN><<<blocks_of(n), kMembraneThreads, 0, s>>>(n, r, c, shear, bulk, f);
 	return check_launch("tension_kernel");
+}
+
+ibk_status ibk_membrane_dissipation(ibk_surface_plan sample_plan, double modulus, int nc, const double* u,
+                                    const ibk_surface* current, double* f, void* stream)
+{
+	if (!sample_plan) return set_error(IBK_ERR_INVALID_ARGUMENT, "null surface plan");
+	if (nc < 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "negative shape count");
+	if (nc == 0) return IBK_OK;
+	if (!u || !current || !f) return set_error(IBK_ERR_INVALID_ARGUMENT, "null velocity, geometry or force array");
+	if (!current->t[0] || !current->t[1] || !current->tt[0] || !current->tt[1] || !current->tt[2] || !current->sigma)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null sample tangents, second derivatives or patch areas");
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	const long long n = (long long) sample_plan->ns * nc;
+	// scratch: the velocity's five derivatives at the samples (dissipation.h:41-53)
+	ibk_status st = grow_scratch(*sample_plan, sizeof(double) * (size_t) (15 * n), s);
+	if (st != IBK_OK) return st;
+	double* vd = sample_plan->scratch;
+	double* outs[6] = {nullptr, vd, vd + 3 * n, vd + 6 * n, vd + 9 * n, vd + 12 * n};
+	if ((st = apply_ops(*sample_plan, 3 * nc, u, outs, s)) != IBK_OK) return st;
+	SurfaceIn c{{current->t[0], current->t[1]}, {current->tt[0], current->tt[1], current->tt[2]}, current->sigma};
+	dissipation_kernel<<<blocks_of(n), kMembraneThreads, 0, s>>>(n, c, vd, modulus, f);
+	return check_launch("dissipation_kernel");
+}
+
+ibk_status ibk_membrane_tether(double modulus, int npoints, const ibk_surface* rest, const ibk_surface* current,
+                               double* f, void* stream)
+{
+	if (npoints <= 0) return IBK_OK;
+	if (!rest || !current || !rest->position || !current->position || !f)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null positions or force array");
+	const long long m = 3LL * npoints;
+	tether_kernel<<<blocks_of(m), kMembraneThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+		m, rest->position, current->position, modulus, f);
+	return check_launch("tether_kernel");
+}
+
+ibk_status ibk_membrane_repelling(double modulus, double height, double range, int npoints,
+                                  const ibk_surface* current, double* f, void* stream)
+{
+	if (npoints <= 0) return IBK_OK;
+	if (!current || !current->position || !current->sigma || !f)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null positions, patch areas or force array");
+	if (!(range > 0)) return set_error(IBK_ERR_INVALID_ARGUMENT, "the repulsion range must be positive");
+	const long long n = npoints;
+	repelling_kernel<<<blocks_of(n), kMembraneThreads, 0, static_cast<cudaStream_t>(stream)>>>(
+		n, current->position, current->sigma, modulus, height, range, f);
+	return check_launch("repelling_kernel");
 }
 
 ibk_status ibk_membrane_bending(ibk_surface_plan data_plan, ibk_surface_plan sample_plan, double modulus,

@@ -397,8 +397,13 @@ ibk_status ibk_io_read_scalar(const char* path, long long offset, double* value,
  * (bases::geometry<2>::compute, include/bases/geometry.h:74-124) and the
  * in-plane tension of a hyperelastic membrane (forces::tension,
  * include/forces/tension.h:9-118) under the Skalak law
- * (include/forces/skalak.h:11-37) or the neo-Hookean law
- * (include/forces/neohookean.h:10-37).  FP64 throughout.
+ * (include/forces/skalak.h:11-37), the neo-Hookean law
+ * (include/forces/neohookean.h:10-37) or the Hookean law
+ * (include/forces/hookean.h:11-35), the bending force, the viscous
+ * dissipation, the tether and the wall repulsion.  FP64 throughout.  The
+ * reference sums a shape's forces (forces::combine,
+ * include/forces/combine.h:11-35: (f1 + f2) + f3 ...); the caller adds the
+ * outputs in that order.
  *
  * Layout, as the reference's shape matrices: nc shapes of ns sample sites
  * (or nd data sites); a per-site vector quantity is 3 blocks of ns*nc values,
@@ -434,8 +439,10 @@ ibk_status ibk_surface_plan_destroy(ibk_surface_plan plan);
 ibk_status ibk_surface_geometry(ibk_surface_plan plan, int nc, const double* x, const ibk_surface* out,
                                 void* stream);
 
-/* Tension laws: w(I1, I2) and its second derivatives. */
-typedef enum { IBK_LAW_SKALAK = 0, IBK_LAW_NEOHOOKEAN = 1 } ibk_tension_law;
+/* Tension laws: w(I1, I2) and its second derivatives.  Hookean: w1 =
+ * shear (1 - 1/sqrt(I1)), w11 = shear / (2 I1 sqrt(I1)), the rest 0 (bulk
+ * unused). */
+typedef enum { IBK_LAW_SKALAK = 0, IBK_LAW_NEOHOOKEAN = 1, IBK_LAW_HOOKEAN = 2 } ibk_tension_law;
 
 /* Tension force at npoints sample sites (forces::tension::operator(),
  * tension.h:55-116): from the rest geometry (t, tt, sigma read) and the
@@ -463,6 +470,33 @@ ibk_status ibk_membrane_tension(int law, double shear, double bulk, int npoints,
 ibk_status ibk_membrane_bending(ibk_surface_plan data_plan, ibk_surface_plan sample_plan, double modulus,
                                 int preferred, int nc, const double* x_rest, const double* x_current,
                                 const ibk_surface* rest, const ibk_surface* current, double* f, void* stream);
+
+/* Viscous dissipation (forces::dissipation, include/forces/dissipation.h:
+ * 128-272): from the data-site velocity u (3*nd*nc, [component][shape][site])
+ * its first and second derivatives at the samples through sample_plan's
+ * derivative operators; with the current sample geometry (t, tt, sigma read)
+ * the rate of change of the metric g' and of the Christoffel symbols, the
+ * stress g^-1 g' adj(g) and its surface divergence, times modulus sigma /
+ * det g.  modulus: surface viscosity in internal units (the reference's
+ * dissipation{dyn s / cm}).  Overwrites f (3*ns*nc).  Device scratch of
+ * 15 ns nc doubles is kept by sample_plan (shared with bending: calls on one
+ * plan are ordered on one stream) and grown on first use. */
+ibk_status ibk_membrane_dissipation(ibk_surface_plan sample_plan, double modulus, int nc, const double* u,
+                                    const ibk_surface* current, double* f, void* stream);
+
+/* Tether (forces::tether, include/forces/tether.h:9-26): f = modulus
+ * (rest->position - current->position) at npoints samples (3*npoints). */
+ibk_status ibk_membrane_tether(double modulus, int npoints, const ibk_surface* rest, const ibk_surface* current,
+                               double* f, void* stream);
+
+/* Wall repulsion (forces::repelling, include/forces/repelling.h:9-49): with
+ * r = |height - y| / range at each sample (current->position's y), fy =
+ * -log(r/2) exp(-4 / (4 - r^2)) for r < 2 (else 0) and f = -modulus (0, fy,
+ * 0) sigma (current->sigma read).  The reference fixes height = 16 um and
+ * range = 0.25 um (1.6 and 0.025 in its internal length unit of 10 um).
+ * range must be positive. */
+ibk_status ibk_membrane_repelling(double modulus, double height, double range, int npoints,
+                                  const ibk_surface* current, double* f, void* stream);
 
 /* ---- The fluid step that consumes the spread: implicit diffusion --------
  * ins::diffusion (include/ins/diffusion.h:12-78) on one component grid of a

@@ -12,8 +12,13 @@
  *             (normal, patch area); include/algo/cross.h, include/algo/dot.h
  *   metric    include/forces/load.h:247-341 (metric, Christoffel symbols)
  *   tension   include/forces/tension.h:35-51 (helper), 71-112 (force)
- *   laws      include/forces/skalak.h:22-31, include/forces/neohookean.h:22-32
+ *   laws      include/forces/skalak.h:22-31, include/forces/neohookean.h:22-32,
+ *             include/forces/hookean.h:19-30
  *   bending   include/forces/bending.h:46-74 (curvatures), 145-229 (force)
+ *   dissipation include/forces/dissipation.h:57-127 (rates of the metric and
+ *             the Christoffel symbols), 193-206 (helpers), 216-265 (force)
+ *   tether    include/forces/tether.h:14-22
+ *   repelling include/forces/repelling.h:15-45
  *
  * Parity unpinned: the reference's membrane code is device lambdas over its
  * linalg layer and does not build on the host here, so this restatement is
@@ -118,6 +123,13 @@ void ibo_membrane_tension(int law, double e, double kappa, int npoints, const do
 			w11 = e;
 			w12 = 0.0;
 			w22 = kappa;
+		} else if (law == 2) {             /* Hookean (hookean.h:19-30) */
+			const double j = sqrt(i1);
+			w1 = e * (1 - 1. / j);
+			w2 = 0.0;
+			w11 = e / (2 * i1 * j);
+			w12 = 0.0;
+			w22 = 0.0;
 		} else {                           /* neo-Hookean */
 			const double j = sqrt(i2);
 			w1 = e / j;
@@ -232,4 +244,104 @@ void ibo_membrane_bending(int ns, int nd, int nc, const double* const* data_ops,
 	free(h);
 	free(h0);
 	free(hd);
+}
+
+/* Operator products of the derivative operators ops[1..5] (ns x nd,
+ * column-major) with y (nd x cols): out + (q - 1) * ns * cols, same loop as
+ * ibo_surface_geometry. */
+static void derivatives(int ns, int nd, int cols, const double* const* ops, const double* y, double* out)
+{
+	for (int q = 1; q < 6; ++q) {
+		const double* op = ops[q];
+		double* o = out + (size_t) (q - 1) * ns * cols;
+		for (int j = 0; j < cols; ++j)
+			for (int r = 0; r < ns; ++r) {
+				double s = 0.0;
+				for (int k = 0; k < nd; ++k) s += op[(size_t) k * ns + r] * y[(size_t) j * nd + k];
+				o[(size_t) j * ns + r] = s;
+			}
+	}
+}
+
+void ibo_membrane_dissipation(int ns, int nd, int nc, const double* const* sample_ops, double kappa,
+                              const double* u, const double* const* cur, double* f)
+{
+	const long long n = (long long) ns * nc;
+	double* vd = (double*) malloc(sizeof(double) * 15 * (size_t) n);
+	derivatives(ns, nd, 3 * nc, sample_ops, u, vd);
+	for (long long p = 0; p < n; ++p) {
+		const v3 tu = ld3(cur[0], n, p), tv = ld3(cur[1], n, p);
+		const v3 tuu = ld3(cur[2], n, p), tuv = ld3(cur[3], n, p), tvv = ld3(cur[4], n, p);
+		const v3 su = ld3(vd, n, p), sv = ld3(vd + 3 * n, n, p);
+		const v3 suu = ld3(vd + 6 * n, n, p), suv = ld3(vd + 9 * n, n, p), svv = ld3(vd + 12 * n, n, p);
+		const metric_t m = metric(tu, tv, tuu, tuv, tvv);
+		const double e = m.e, ff = m.f, g = m.g, eu = m.eu, fu = m.fu, gu = m.gu, ev = m.ev, fv = m.fv, gv = m.gv;
+		const double i = m.i, iu = m.iu, iv = m.iv;
+
+		/* dot_metric (dissipation.h:57-79) */
+		const double de = dot3(tu, su) + dot3(su, tu);
+		const double df = dot3(tu, sv) + dot3(su, tv);
+		const double dg = dot3(tv, sv) + dot3(sv, tv);
+		/* dot_christoffel (dissipation.h:89-127) and dot_helper (193-206) */
+		const double c00_0 = dot3(suu, tu) + dot3(tuu, su), c00_1 = dot3(suu, tv) + dot3(tuu, sv);
+		const double c01_0 = dot3(suv, tu) + dot3(tuv, su), c01_1 = dot3(suv, tv) + dot3(tuv, sv);
+		const double c11_0 = dot3(svv, tu) + dot3(tvv, su), c11_1 = dot3(svv, tv) + dot3(tvv, sv);
+		const double deu = 2 * c00_0, dfu = c00_1 + c01_0, dgu = 2 * c01_1;
+		const double dev = 2 * c01_0, dfv = c01_1 + c11_0, dgv = 2 * c11_1;
+
+		/* dissipation.h:223-256 */
+		double pig[4], pigu[4], pigv[4], pif[3], pifu[3], pifv[3];
+		pig[0] = (g * de - ff * df) / i;
+		pig[1] = (g * df - ff * dg) / i;
+		pig[2] = (e * df - ff * de) / i;
+		pig[3] = (e * dg - ff * df) / i;
+		pigu[0] = (gu * de + g * deu - fu * df - ff * dfu - iu * pig[0]) / i;
+		pigu[1] = (gu * df + g * dfu - fu * dg - ff * dgu - iu * pig[1]) / i;
+		pigu[2] = (eu * df + e * dfu - fu * de - ff * deu - iu * pig[2]) / i;
+		pigu[3] = (eu * dg + e * dgu - fu * df - ff * dfu - iu * pig[3]) / i;
+		pigv[0] = (gv * de + g * dev - fv * df - ff * dfv - iv * pig[0]) / i;
+		pigv[1] = (gv * df + g * dfv - fv * dg - ff * dgv - iv * pig[1]) / i;
+		pigv[2] = (ev * df + e * dfv - fv * de - ff * dev - iv * pig[2]) / i;
+		pigv[3] = (ev * dg + e * dgv - fv * df - ff * dfv - iv * pig[3]) / i;
+		pif[0] = pig[0] * g - pig[1] * ff;
+		pif[1] = 0.5 * (pig[1] * e + pig[2] * g - (pig[0] + pig[3]) * ff);
+		pif[2] = pig[3] * e - pig[2] * ff;
+		pifu[0] = pigu[0] * g + pig[0] * gu - pigu[1] * ff - pig[1] * fu;
+		pifu[1] = 0.5 * (pigu[1] * e + pig[1] * eu + pigu[2] * g + pig[2] * gu
+		                 - ((pigu[0] + pigu[3]) * ff + (pig[0] + pig[3]) * fu));
+		pifu[2] = pigu[3] * e + pig[3] * eu - pigu[2] * ff - pig[2] * fu;
+		pifv[0] = pigv[0] * g + pig[0] * gv - pigv[1] * ff - pig[1] * fv;
+		pifv[1] = 0.5 * (pigv[1] * e + pig[1] * ev + pigv[2] * g + pig[2] * gv
+		                 - ((pigv[0] + pigv[3]) * ff + (pig[0] + pig[3]) * fv));
+		pifv[2] = pigv[3] * e + pig[3] * ev - pigv[2] * ff - pig[2] * fv;
+		const double c0 = pifu[0] + pifv[1] - (iu * pif[0] + iv * pif[1]) / (2 * i);
+		const double c1 = pifu[1] + pifv[2] - (iu * pif[1] + iv * pif[2]) / (2 * i);
+
+		/* dissipation.h:258-264: fd = c0 t_u + c1 t_v + pif0 t_uu + 2 pif1 t_uv
+		 * + pif2 t_vv, f = s kappa / i fd */
+		const double uc[3] = {tu.x, tu.y, tu.z}, vc[3] = {tv.x, tv.y, tv.z};
+		const double uuc[3] = {tuu.x, tuu.y, tuu.z}, uvc[3] = {tuv.x, tuv.y, tuv.z}, vvc[3] = {tvv.x, tvv.y, tvv.z};
+		for (int k = 0; k < 3; ++k) {
+			const double fd = c0 * uc[k] + c1 * vc[k] + pif[0] * uuc[k] + 2 * pif[1] * uvc[k] + pif[2] * vvc[k];
+			f[k * n + p] = cur[5][p] * kappa / i * fd;
+		}
+	}
+	free(vd);
+}
+
+void ibo_membrane_tether(double modulus, int npoints, const double* x_rest, const double* x_cur, double* f)
+{
+	for (long long p = 0; p < 3LL * npoints; ++p) f[p] = modulus * (x_rest[p] - x_cur[p]);
+}
+
+void ibo_membrane_repelling(double modulus, double height, double range, int npoints, const double* x,
+                            const double* sigma, double* f)
+{
+	const long long n = npoints;
+	for (long long p = 0; p < n; ++p) {
+		const double r = fabs(height - x[n + p]) / range;
+		const double fy = r < 2 ? -log(r / 2) * exp(-4 / (4 - r * r)) : 0.0;
+		const double fc[3] = {0.0, fy, 0.0};
+		for (int k = 0; k < 3; ++k) f[k * n + p] = -modulus * fc[k] * sigma[p];
+	}
 }

@@ -93,8 +93,8 @@ int ibo_max_threads(void);
  * sigma (ns*nc), NULL to skip (tu, tv and sigma required). */
 void ibo_surface_geometry(int ns, int nd, int nc, const double* const* ops, const double* weights,
                           const double* x, double* const* out);
-/* Tension force (law 0 Skalak, 1 neo-Hookean): rest[0..5] = tu, tv, tuu,
- * tuv, tvv, sigma; cur[0..4] = tu, tv, tuu, tuv, tvv; f 3*npoints. */
+/* Tension force (law 0 Skalak, 1 neo-Hookean, 2 Hookean): rest[0..5] = tu,
+ * tv, tuu, tuv, tvv, sigma; cur[0..4] = tu, tv, tuu, tuv, tvv; f 3*npoints. */
 void ibo_membrane_tension(int law, double e, double kappa, int npoints, const double* const* rest,
                           const double* const* cur, double* f);
 /* Bending force: data_ops (nd x nd, evaluation NULL) with data_weights give
@@ -104,6 +104,17 @@ void ibo_membrane_tension(int law, double e, double kappa, int npoints, const do
 void ibo_membrane_bending(int ns, int nd, int nc, const double* const* data_ops, const double* data_weights,
                           const double* const* sample_ops, double modulus, int preferred, const double* x_rest,
                           const double* x_cur, const double* const* rest, const double* const* cur, double* f);
+
+/* Dissipation force: sample_ops[1..5] (ns x nd) give the derivatives of the
+ * data-site velocity u (3*nd*nc) at the samples; cur[0..5] = tu, tv, tuu,
+ * tuv, tvv, sigma of the current sample geometry; f 3*ns*nc. */
+void ibo_membrane_dissipation(int ns, int nd, int nc, const double* const* sample_ops, double kappa,
+                              const double* u, const double* const* cur, double* f);
+/* Tether: f = modulus (x_rest - x_cur), 3*npoints values. */
+void ibo_membrane_tether(double modulus, int npoints, const double* x_rest, const double* x_cur, double* f);
+/* Wall repulsion at npoints samples: x 3*npoints positions, sigma npoints. */
+void ibo_membrane_repelling(double modulus, double height, double range, int npoints, const double* x,
+                            const double* sigma, double* f);
 
 /* Implicit diffusion step on one component grid (ibk_fluid_oracle.c):
  * points / periodic / shift per axis (dims of them), res the resolution,

@@ -127,6 +127,11 @@ def lib():
             L.ibo_membrane_bending.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp), _dp,
                                                ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int, _dp, _dp,
                                                ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
+            L.ibo_membrane_dissipation.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
+                                                   ctypes.c_double, _dp, ctypes.POINTER(_dp), _dp]
+            L.ibo_membrane_tether.argtypes = [ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+            L.ibo_membrane_repelling.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                 _dp, _dp, _dp]
             _lib = L
     return _lib
 
@@ -271,7 +276,8 @@ def surface_geometry(ops, weights, x, nc):
 
 def membrane_tension(law, shear, bulk, rest, cur):
     """Tension force at every sample (include/forces/tension.h:71-112;
-    law 0 Skalak, 1 neo-Hookean) from rest and current geometry dicts."""
+    law 0 Skalak, 1 neo-Hookean, 2 Hookean) from rest and current geometry
+    dicts."""
     keep = [np.ascontiguousarray(rest[k], dtype=np.float64) for k in ("tu", "tv", "tuu", "tuv", "tvv", "sigma")]
     keep += [np.ascontiguousarray(cur[k], dtype=np.float64) for k in ("tu", "tv", "tuu", "tuv", "tvv")]
     n = keep[5].size
@@ -301,6 +307,38 @@ def membrane_bending(data_ops, data_weights, sample_ops, modulus, preferred, x_r
     sp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cms])
     lib().ibo_membrane_bending(ns, nd, nc, dp, _d(dw), sp, float(modulus), int(bool(preferred)), _d(xr), _d(xc),
                                (_dp * 6)(*[_d(a) for a in r]), (_dp * 7)(*[_d(a) for a in c]), _d(f))
+    return f
+
+
+def membrane_dissipation(sample_ops, modulus, u, cur, nc):
+    """Viscous dissipation at every sample (include/forces/dissipation.h:
+    216-265): sample_ops as for surface_geometry, u the data-site velocity
+    (3*nd*nc), cur the current sample geometry dict; returns 3*ns*nc forces."""
+    cms = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in sample_ops]
+    ns, nd = cms[1].shape
+    c = [np.ascontiguousarray(cur[k], dtype=np.float64) for k in ("tu", "tv", "tuu", "tuv", "tvv", "sigma")]
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    f = np.zeros(3 * ns * nc)
+    sp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cms])
+    lib().ibo_membrane_dissipation(ns, nd, nc, sp, float(modulus), _d(uu), (_dp * 6)(*[_d(a) for a in c]), _d(f))
+    return f
+
+
+def membrane_tether(modulus, x_rest, x_cur):
+    """Tether force modulus (x_rest - x_cur) (include/forces/tether.h:14-22)."""
+    xr = np.ascontiguousarray(x_rest, dtype=np.float64)
+    xc = np.ascontiguousarray(x_cur, dtype=np.float64)
+    f = np.zeros(xr.size)
+    lib().ibo_membrane_tether(float(modulus), xr.size // 3, _d(xr), _d(xc), _d(f))
+    return f
+
+
+def membrane_repelling(modulus, height, range_, x, sigma):
+    """Wall repulsion at every sample (include/forces/repelling.h:15-45)."""
+    xx = np.ascontiguousarray(x, dtype=np.float64)
+    s = np.ascontiguousarray(sigma, dtype=np.float64)
+    f = np.zeros(xx.size)
+    lib().ibo_membrane_repelling(float(modulus), float(height), float(range_), s.size, _d(xx), _d(s), _d(f))
     return f
 
 

@@ -1,5 +1,5 @@
-"""Membrane forces (tension and bending) on the device against the oracle,
-through the C ABI.
+"""Membrane forces (tension, bending, dissipation, tether, repelling) on the
+device against the oracle, through the C ABI.
 
 The tension kernel evaluates the reference's expressions in its order
 without contraction, so it matches the oracle bit for bit.  The surface
@@ -46,7 +46,7 @@ def _analytic(shapes):
     return g
 
 
-@pytest.mark.parametrize("law", [0, 1])
+@pytest.mark.parametrize("law", [0, 1, 2])
 def test_tension_matches_oracle_bit_for_bit(ibk, cuda, oracle, law):
     rest, cur = _analytic(_shapes(3, cur=False)), _analytic(_shapes(3))
     f_ref = oracle.membrane_tension(law, SHEAR, BULK, rest, cur)
@@ -162,3 +162,109 @@ def test_no_bending_force_on_the_clifford_torus_gpu(ibk, cuda):
         g = sample_plan.geometry(x, 1)
         out.append(ibk.membrane_bending(data_plan, sample_plan, 1.0, False, None, x, None, g, 1).abs().max().item())
     assert out[0] <= 1e-3 * out[1]
+
+
+KAPPA = 0.7
+
+
+def _velocity(nc, phase=0.3):
+    u, v = T.grid(NU, NV)
+    one = [np.stack([np.sin(u + phase + c) * np.cos(v), np.cos(2 * u) + 0.3 * np.sin(v - phase),
+                     np.sin(u - 2 * v + c)]) for c in range(nc)]
+    return np.stack(one, axis=1).reshape(-1)
+
+
+def test_dissipation_kernel_matches_oracle_bit_for_bit(ibk, cuda, oracle):
+    """Integer operators and velocities make every operator product exact
+    whatever the GEMM's summation order, so the per-sample kernel sees the
+    oracle's inputs and must give its bits."""
+    import torch
+    rng = np.random.default_rng(17)
+    ns, nd, nc = 300, 40, 3
+    ops = [rng.integers(-3, 4, size=(ns, nd)).astype(np.float64) for _ in range(6)]
+    u = rng.integers(-5, 6, size=3 * nd * nc).astype(np.float64)
+    n = ns * nc
+    cur = {k: rng.normal(size=3 * n) for k in ("tu", "tv", "tuu", "tuv", "tvv")}
+    cur["tu"] = (cur["tu"].reshape(3, n) + np.array([[2.0], [0.0], [0.0]])).reshape(-1)
+    cur["tv"] = (cur["tv"].reshape(3, n) + np.array([[0.0], [2.0], [0.0]])).reshape(-1)
+    cur["sigma"] = rng.uniform(0.5, 1.5, size=n)
+    plan = ibk.SurfacePlan([torch.from_numpy(m).to(cuda) for m in ops],
+                           torch.from_numpy(rng.uniform(0.5, 1.0, size=ns)).to(cuda))
+    f = ibk.membrane_dissipation(plan, KAPPA, torch.from_numpy(u).to(cuda), _to(cur, cuda), nc).cpu().numpy()
+    f_ref = oracle.membrane_dissipation(ops, KAPPA, u, cur, nc)
+    assert np.array_equal(f, f_ref)
+
+
+def test_dissipation_pipeline(ibk, cuda, oracle):
+    """Geometry then dissipation on sheared tori: the oracle's forces (to the
+    GEMMs' summation order), none under rigid motion, and zero total force
+    and torque to the grid's accuracy."""
+    import torch
+    w = T.weights(NU, NV)
+    ops = T.operators(NU, NV)
+    plan = ibk.SurfacePlan([torch.from_numpy(m).to(cuda) for m in ops], torch.from_numpy(w).to(cuda))
+    nc = 3
+    x = T.pack(_shapes(nc))["position"]
+    X = torch.from_numpy(x).to(cuda)
+    cur = plan.geometry(X, nc)
+    U = _velocity(nc)
+    f = ibk.membrane_dissipation(plan, KAPPA, torch.from_numpy(U).to(cuda), cur, nc).cpu().numpy()
+    g = oracle.surface_geometry(ops, w, x, nc)
+    f_ref = oracle.membrane_dissipation(ops, KAPPA, U, g, nc)
+    assert np.abs(f - f_ref).max() <= 1e-9 * np.abs(f_ref).max()
+    n = NU * NV
+    pos = x.reshape(3, nc, n)
+    F = f.reshape(3, nc, n)
+    for c in range(nc):
+        Fc, Mc = T.totals(F[:, c].reshape(-1), pos[:, c].reshape(-1), n)
+        scale = np.abs(F[:, c]).sum()
+        # the grid's accuracy for the stress divergence on these sheared tori
+        # at 48 x 24 (the oracle gives up to 1.5e-6, converging to 1.5e-8 at
+        # 64 x 32 and 5e-13 at 96 x 48)
+        assert np.abs(Fc).max() <= 1e-5 * scale and np.abs(Mc).max() <= 1e-5 * scale
+    omega, a = np.array([0.3, -0.5, 0.8]), np.array([1.0, 2.0, -0.5])
+    rigid = np.stack([a[:, None] + np.cross(omega, pos[:, c].T).T for c in range(nc)], axis=1).reshape(-1)
+    fr = ibk.membrane_dissipation(plan, KAPPA, torch.from_numpy(rigid).to(cuda), cur, nc).cpu().numpy()
+    assert np.abs(fr).max() <= 1e-11 * np.abs(f).max()
+
+
+def test_tether_and_repelling_match_oracle(ibk, cuda, oracle):
+    rng = np.random.default_rng(23)
+    n = 20000
+    rest = {"position": rng.normal(size=3 * n)}
+    cur = {"position": rest["position"] + 0.05 * rng.normal(size=3 * n), "sigma": rng.uniform(0.5, 1.5, size=n)}
+    f = ibk.membrane_tether(3.0, _to(rest, cuda), _to(cur, cuda)).cpu().numpy()
+    assert np.array_equal(f, oracle.membrane_tether(3.0, rest["position"], cur["position"]))
+    # a wall at y = 0.3 reaching 0.5 either side: about a third of the samples
+    f = ibk.membrane_repelling(2.0, _to(cur, cuda), height=0.3, range_=0.25).cpu().numpy()
+    f_ref = oracle.membrane_repelling(2.0, 0.3, 0.25, cur["position"], cur["sigma"])
+    # the device's log and exp against the C library's: a few ulp apart
+    assert np.abs(f - f_ref).max() <= 4e-15 * np.abs(f_ref).max()
+    assert np.array_equal(f == 0, f_ref == 0)
+
+
+def test_red_cell_force_set_balances(ibk, cuda):
+    """The reference's red-cell forces (tension, bending, dissipation; summed
+    as forces::combine does) on deformed, moving tori: zero total force and
+    torque per shape to the grid's accuracy."""
+    import torch
+    w = torch.from_numpy(T.weights(NU, NV)).to(cuda)
+    ops = [torch.from_numpy(m).to(cuda) for m in T.operators(NU, NV)]
+    data_plan = ibk.SurfacePlan([None] + ops[1:], w)
+    sample_plan = ibk.SurfacePlan(ops, w)
+    nc = 3
+    X0 = torch.from_numpy(T.pack([T.shape(NU, NV, R=2.0, r=0.7) for _ in range(nc)])["position"]).to(cuda)
+    X1 = torch.from_numpy(T.pack([T.shape(NU, NV, R=2.0, r=0.7, A=MATS[i], eps=0.02 * (i + 1))
+                                  for i in range(nc)])["position"]).to(cuda)
+    rest, cur = sample_plan.geometry(X0, nc), sample_plan.geometry(X1, nc)
+    U = torch.from_numpy(_velocity(nc)).to(cuda)
+    f = (ibk.membrane_tension(ibk.SKALAK, SHEAR, BULK, rest, cur)
+         + ibk.membrane_bending(data_plan, sample_plan, 0.05, False, X0, X1, rest, cur, nc)) \
+        + ibk.membrane_dissipation(sample_plan, KAPPA, U, cur, nc)
+    n = NU * NV
+    F = f.cpu().numpy().reshape(3, nc, n)
+    pos = X1.cpu().numpy().reshape(3, nc, n)
+    for c in range(nc):
+        Fc, Mc = T.totals(F[:, c].reshape(-1), pos[:, c].reshape(-1), n)
+        scale = np.abs(F[:, c]).sum()
+        assert np.abs(Fc).max() <= 1e-5 * scale and np.abs(Mc).max() <= 1e-5 * scale
