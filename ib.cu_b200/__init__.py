@@ -55,6 +55,7 @@ ABI_SYMBOLS = (
     "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
     "ibk_surface_plan_create", "ibk_surface_plan_destroy", "ibk_surface_geometry", "ibk_membrane_tension",
     "ibk_membrane_bending", "ibk_membrane_dissipation", "ibk_membrane_tether", "ibk_membrane_repelling",
+    "ibk_curve_plan_create", "ibk_curve_tension",
     "ibk_diffusion_create", "ibk_diffusion_destroy", "ibk_diffusion_apply", "ibk_diffusion_step",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
@@ -234,13 +235,16 @@ def lib() -> ctypes.CDLL:
                                            ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
         L.ibk_membrane_dissipation.argtypes = [_vp, ctypes.c_double, ctypes.c_int, _vp, ctypes.POINTER(_Surface),
                                                _vp, _vp]
+        L.ibk_curve_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp), _vp, ctypes.POINTER(_vp)]
+        L.ibk_curve_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                        ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
         L.ibk_membrane_tether.argtypes = [ctypes.c_double, ctypes.c_int, ctypes.POINTER(_Surface),
                                           ctypes.POINTER(_Surface), _vp, _vp]
         L.ibk_membrane_repelling.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                              ctypes.POINTER(_Surface), _vp, _vp]
         for name in ABI_SYMBOLS:
             if name.startswith(("ibk_batch_", "ibk_server_", "ibk_io_", "ibk_surface_", "ibk_membrane_",
-                                "ibk_diffusion_")) \
+                                "ibk_diffusion_", "ibk_curve_")) \
                     and name != "ibk_server_clock":
                 getattr(L, name).restype = ctypes.c_int
         L.ibk_last_error.restype = ctypes.c_char_p
@@ -762,6 +766,51 @@ class SurfacePlan:
         if getattr(self, "handle", None):
             lib().ibk_surface_plan_destroy(self.handle)
             self.handle = None
+
+
+_CURVE_FIELDS = ("position", "tu", "tuu", "normal", "sigma")
+
+
+class CurvePlan(SurfacePlan):
+    """Geometry of a family of closed curves in a two-dimensional run
+    (bases::geometry<1>): ops = three CUDA float64 ns x nd tensors
+    (evaluation or None, d/ds, d2/ds2), weights: ns."""
+
+    def __init__(self, ops, weights):
+        import torch
+        self.ns = int(weights.numel())
+        self.nd = int(ops[1].shape[1])
+        self._ops = [None if o is None else o.t().contiguous().t() for o in ops]
+        self._weights = weights.contiguous()
+        arr = (_vp * 3)(*[None if o is None else o.data_ptr() for o in self._ops])
+        h = _vp()
+        check(lib().ibk_curve_plan_create(self.ns, self.nd, arr, self._weights.data_ptr(), ctypes.byref(h)))
+        self.handle = h
+        self._torch = torch
+
+    def geometry(self, x, nc, stream=None):
+        """x: 2*nd*nc positions [component][curve][site]; returns a dict of
+        position, tu, tuu, normal (2*ns*nc) and sigma (ns*nc)."""
+        torch = self._torch
+        m = self.ns * nc
+        g = {k: torch.empty(m if k == "sigma" else 2 * m, dtype=torch.float64, device=x.device)
+             for k in _CURVE_FIELDS}
+        s = _surface_struct(g)
+        check(lib().ibk_surface_geometry(self.handle, nc, x.data_ptr(), ctypes.byref(s), _stream_handle(stream)))
+        return g
+
+
+def curve_tension(law, shear, bulk, rest, current, stream=None):
+    """One-dimensional tension (forces::tension1d with skalak1d or
+    hookean1d, include/forces/tension.h:160-200) from rest and current curve
+    geometry dicts; returns 2*npoints forces [component][site]."""
+    import torch
+    n = int(rest["sigma"].numel())
+    f = torch.empty(2 * n, dtype=torch.float64, device=rest["sigma"].device)
+    r, c = _surface_struct(rest), _surface_struct(current)
+    check(lib().ibk_curve_tension(law, shear, bulk, n, ctypes.byref(r), ctypes.byref(c), f.data_ptr(),
+                                  _stream_handle(stream)))
+    return f
 
 
 def membrane_tension(law, shear, bulk, rest, current, stream=None):

@@ -8,8 +8,10 @@
 // include/forces/bending.h:10-229), the viscous dissipation
 // (forces::dissipation, include/forces/dissipation.h:128-272), the tether
 // (include/forces/tether.h:9-26) and the wall repulsion
-// (include/forces/repelling.h:9-49).  These produce the point forces that a
-// spread takes.
+// (include/forces/repelling.h:9-49); for curves in two-dimensional runs the
+// geometry and the one-dimensional tension (forces::tension1d,
+// include/forces/tension.h:120-205) under the skalak1d and hookean1d laws.
+// These produce the point forces that a spread takes.
 //
 // Arithmetic: FP64.  Every per-sample expression is evaluated in the order
 // the reference writes it, with no contraction (the build compiles this file
@@ -22,6 +24,7 @@
 
 struct ibk_surface_plan_s {
 	int ns = 0, nd = 0, device = 0;
+	int dims = 2;                   // 2: surfaces in 3-D; 1: curves in 2-D (ops[0], ops[1], ops[3] only)
 	const double* ops[6] = {};
 	const double* weights = nullptr;
 	cublasHandle_t blas = nullptr;
@@ -254,6 +257,59 @@ bending_kernel(long long n, SurfaceFull cur, SurfaceFull rest, int preferred, co
 	f[2 * n + p] = mag * nrm.z;
 }
 
+// Curves in two-dimensional runs: bases::geometry<1> (geometry.h:74-124 with
+// one tangent over two components, whose algo::cross is (t1, -t0)) and
+// forces::tension1d (tension.h:120-205).
+__device__ __forceinline__ double dot2(double a0, double a1, double b0, double b1) { return a0 * b0 + a1 * b1; }
+
+__global__ void __launch_bounds__(kMembraneThreads)
+curve_metrics_kernel(long long n, int ns, const double* __restrict__ t, const double* __restrict__ weights,
+                     double* __restrict__ normal, double* __restrict__ sigma)
+{
+	const long long p = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	const double c0 = __ldg(t + n + p), c1 = -__ldg(t + p);
+	const double detf = sqrt(dot2(c0, c1, c0, c1));
+	if (normal) {
+		normal[p] = c0 / detf;
+		normal[n + p] = c1 / detf;
+	}
+	sigma[p] = __ldg(weights + p % ns) * detf;
+}
+
+// tension.h:172-200 with the skalak1d (skalak.h:49-55) or hookean1d
+// (hookean.h:48-54) law of the stretch invariant i = |t|^2 / |t0|^2.
+template <int LAW>
+__global__ void __launch_bounds__(kMembraneThreads)
+curve_tension_kernel(long long n, SurfaceIn rest, SurfaceIn cur, double e, double kappa, double* __restrict__ f)
+{
+	const long long p = (long long) blockIdx.x * blockDim.x + threadIdx.x;
+	if (p >= n) return;
+	const double ou0 = __ldg(rest.t[0] + p), ou1 = __ldg(rest.t[0] + n + p);
+	const double ouu0 = __ldg(rest.tt[0] + p), ouu1 = __ldg(rest.tt[0] + n + p);
+	const double u0 = __ldg(cur.t[0] + p), u1 = __ldg(cur.t[0] + n + p);
+	const double uu0 = __ldg(cur.tt[0] + p), uu1 = __ldg(cur.tt[0] + n + p);
+	const double oi = dot2(ou0, ou1, ou0, ou1), odi = 2 * dot2(ouu0, ouu1, ou0, ou1);
+	const double ci = dot2(u0, u1, u0, u1), cdi = 2 * dot2(uu0, uu1, u0, u1);
+	const double i = ci / oi;
+	const double iu = (cdi - i * odi) / oi;
+	double phi, phi1;
+	if constexpr (LAW == IBK_LAW_SKALAK) {
+		phi = e * (i - 1) - kappa * i * (i * i - 1);
+		phi1 = e - kappa * (3 * i * i - 1);
+	} else {
+		const double j = sqrt(i);
+		phi = e * (1 - 1. / j);
+		phi1 = e / (2 * i * j);
+	}
+	const double phiu = phi1 * iu;
+	const double scale = __ldg(rest.sigma + p) / oi;
+	const double uc[2] = {u0, u1}, uuc[2] = {uu0, uu1};
+#pragma unroll
+	for (int k = 0; k < 2; ++k)
+		f[k * n + p] = scale * (+ phi * uuc[k] - odi / (2 * oi) * phi * uc[k] + phiu * uc[k]);
+}
+
 // Viscous dissipation at the samples (dissipation.h:216-265): the rate of
 // change of the metric and of the Christoffel symbols from the velocity's
 // derivatives (vd: u, v, uu, uv, vv, each 3n values [component][site]) and
@@ -383,6 +439,15 @@ ibk_status apply_ops(ibk_surface_plan_s& plan, int cols, const double* y, double
 
 ibk_status geometry_impl(ibk_surface_plan_s& plan, int nc, const double* x, const ibk_surface& out, cudaStream_t s)
 {
+	if (plan.dims == 1) {
+		double* outs[6] = {out.position, out.t[0], nullptr, out.tt[0], nullptr, nullptr};
+		const ibk_status st = apply_ops(plan, 2 * nc, x, outs, s);
+		if (st != IBK_OK) return st;
+		const long long n = (long long) plan.ns * nc;
+		curve_metrics_kernel<<<blocks_of(n), kMembraneThreads, 0, s>>>(n, plan.ns, out.t[0], plan.weights,
+		                                                               out.normal, out.sigma);
+		return check_launch("curve_metrics_kernel");
+	}
 	double* outs[6] = {out.position, out.t[0], out.t[1], out.tt[0], out.tt[1], out.tt[2]};
 	const ibk_status st = apply_ops(plan, 3 * nc, x, outs, s);
 	if (st != IBK_OK) return st;
@@ -451,6 +516,34 @@ ibk_status ibk_surface_plan_create(int ns, int nd, const double* const* ops, con
 	return IBK_OK;
 }
 
+ibk_status ibk_curve_plan_create(int ns, int nd, const double* const* ops, const double* weights,
+                                 ibk_surface_plan* out)
+{
+	if (!out) return set_error(IBK_ERR_INVALID_ARGUMENT, "null output handle");
+	*out = nullptr;
+	if (ns <= 0 || nd <= 0 || !ops || !weights)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "sizes must be positive, operators and weights given");
+	if (!ops[1] || !ops[2]) return set_error(IBK_ERR_INVALID_ARGUMENT, "null derivative operator");
+	if (!ops[0] && ns != nd)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "without an evaluation operator the samples are the data sites (ns == nd)");
+	auto* plan = new ibk_surface_plan_s;
+	plan->ns = ns;
+	plan->nd = nd;
+	plan->dims = 1;
+	plan->ops[0] = ops[0];
+	plan->ops[1] = ops[1];
+	plan->ops[3] = ops[2];
+	plan->weights = weights;
+	cudaGetDevice(&plan->device);
+	const ibk_status st = blas_check(cublasCreate(&plan->blas), "cublasCreate");
+	if (st != IBK_OK) {
+		delete plan;
+		return st;
+	}
+	*out = plan;
+	return IBK_OK;
+}
+
 ibk_status ibk_surface_plan_destroy(ibk_surface_plan plan)
 {
 	if (!plan) return IBK_OK;
@@ -469,6 +562,11 @@ ibk_status ibk_surface_geometry(ibk_surface_plan plan, int nc, const double* x, 
 	if (!plan || !out) return set_error(IBK_ERR_INVALID_ARGUMENT, "null plan or output");
 	if (nc < 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "negative shape count");
 	if (nc == 0) return IBK_OK;
+	if (plan->dims == 1) {
+		if (!x || !out->t[0] || !out->tt[0] || !out->sigma)
+			return set_error(IBK_ERR_INVALID_ARGUMENT, "null positions, tangent, second derivative or lengths");
+		return geometry_impl(*plan, nc, x, *out, static_cast<cudaStream_t>(stream));
+	}
 	if (!x || !out->t[0] || !out->t[1] || !out->tt[0] || !out->tt[1] || !out->tt[2] || !out->sigma)
 		return set_error(IBK_ERR_INVALID_ARGUMENT, "null positions, tangents, second derivatives or areas");
 	return geometry_impl(*plan, nc, x, *out, static_cast<cudaStream_t>(stream));
@@ -499,10 +597,31 @@ ibk_status ibk_membrane_tension(int law, double shear, double bulk, int npoints,
 	return check_launch("tension_kernel");
 }
 
+ibk_status ibk_curve_tension(int law, double shear, double bulk, int npoints, const ibk_surface* rest,
+                             const ibk_surface* current, double* f, void* stream)
+{
+	if (law != IBK_LAW_SKALAK && law != IBK_LAW_HOOKEAN)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "curves take the Skalak or Hookean law");
+	if (npoints <= 0) return IBK_OK;
+	if (!rest || !current || !f) return set_error(IBK_ERR_INVALID_ARGUMENT, "null geometry or force array");
+	if (!rest->t[0] || !rest->tt[0] || !rest->sigma || !current->t[0] || !current->tt[0])
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "null tangent, second derivative or rest lengths");
+	SurfaceIn r{{rest->t[0], nullptr}, {rest->tt[0], nullptr, nullptr}, rest->sigma};
+	SurfaceIn c{{current->t[0], nullptr}, {current->tt[0], nullptr, nullptr}, nullptr};
+	cudaStream_t s = static_cast<cudaStream_t>(stream);
+	const long long n = npoints;
+	if (law == IBK_LAW_SKALAK)
+		curve_tension_kernel<IBK_LAW_SKALAK><<<blocks_of(n), kMembraneThreads, 0, s>>>(n, r, c, shear, bulk, f);
+	else
+		curve_tension_kernel<IBK_LAW_HOOKEAN><<<blocks_of(n), kMembraneThreads, 0, s>>>(n, r, c, shear, bulk, f);
+	return check_launch("curve_tension_kernel");
+}
+
 ibk_status ibk_membrane_dissipation(ibk_surface_plan sample_plan, double modulus, int nc, const double* u,
                                     const ibk_surface* current, double* f, void* stream)
 {
 	if (!sample_plan) return set_error(IBK_ERR_INVALID_ARGUMENT, "null surface plan");
+	if (sample_plan->dims != 2) return set_error(IBK_ERR_INVALID_ARGUMENT, "dissipation acts on surfaces, not curves");
 	if (nc < 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "negative shape count");
 	if (nc == 0) return IBK_OK;
 	if (!u || !current || !f) return set_error(IBK_ERR_INVALID_ARGUMENT, "null velocity, geometry or force array");
@@ -553,6 +672,8 @@ ibk_status ibk_membrane_bending(ibk_surface_plan data_plan, ibk_surface_plan sam
 	if (!data_plan || !sample_plan) return set_error(IBK_ERR_INVALID_ARGUMENT, "null surface plan");
 	if (nc < 0) return set_error(IBK_ERR_INVALID_ARGUMENT, "negative shape count");
 	if (nc == 0) return IBK_OK;
+	if (data_plan->dims != 2 || sample_plan->dims != 2)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "bending acts on surfaces, not curves");
 	if (data_plan->ns != data_plan->nd || sample_plan->nd != data_plan->nd)
 		return set_error(IBK_ERR_INVALID_ARGUMENT, "the data plan must map the data sites to themselves, "
 		                                           "and both plans must share them");

@@ -498,6 +498,33 @@ ibk_status ibk_membrane_tether(double modulus, int npoints, const ibk_surface* r
 ibk_status ibk_membrane_repelling(double modulus, double height, double range, int npoints,
                                   const ibk_surface* current, double* f, void* stream);
 
+/* ---- Curves in two-dimensional runs -------------------------------------
+ * bases::geometry<1> (include/bases/geometry.h:74-124 with one tangent over
+ * two components) and forces::tension1d (include/forces/tension.h:120-205)
+ * under the skalak1d (include/forces/skalak.h:39-61) or hookean1d
+ * (include/forces/hookean.h:38-60) law, as test/ib-platelet1d.cc uses them.
+ * Layout: nc curves of ns samples (nd data sites), a vector quantity 2 blocks
+ * of ns*nc values [component][curve][site]; ibk_surface's t[0], tt[0],
+ * normal, sigma and position carry the tangent, the second derivative, the
+ * normal (t1, -t0)/|t|, the segment lengths weight*|t| and the positions
+ * (t[1], tt[1], tt[2] unused). */
+
+/* ops[0] evaluation (NULL when ns == nd), ops[1] d/ds, ops[2] d2/ds2, each a
+ * column-major ns x nd device matrix kept by pointer; weights: ns.  The plan
+ * serves ibk_surface_geometry (x: 2*nd*nc) and is refused by the surface
+ * forces (bending, dissipation). */
+ibk_status ibk_curve_plan_create(int ns, int nd, const double* const* ops, const double* weights,
+                                 ibk_surface_plan* out);
+
+/* One-dimensional tension at npoints samples: i = |t|^2 / |t_rest|^2, its
+ * derivative along the curve, the law's phi(i) and phi'(i), and f = sigma_rest
+ * / |t_rest|^2 (phi t_ss - (|t_rest|^2)' / (2 |t_rest|^2) phi t_s + phi' i' t_s)
+ * (tension.h:172-200).  law: IBK_LAW_SKALAK (skalak1d: phi = shear (i - 1) -
+ * bulk i (i^2 - 1)) or IBK_LAW_HOOKEAN (hookean1d; bulk unused).  Reads rest
+ * t[0], tt[0], sigma and current t[0], tt[0]; overwrites f (2*npoints). */
+ibk_status ibk_curve_tension(int law, double shear, double bulk, int npoints, const ibk_surface* rest,
+                             const ibk_surface* current, double* f, void* stream);
+
 /* ---- The fluid step that consumes the spread: implicit diffusion --------
  * ins::diffusion (include/ins/diffusion.h:12-78) on one component grid of a
  * plan: with L the second-order finite-difference Laplacian and I~ the

@@ -19,6 +19,10 @@
  *             the Christoffel symbols), 193-206 (helpers), 216-265 (force)
  *   tether    include/forces/tether.h:14-22
  *   repelling include/forces/repelling.h:15-45
+ *   curves    include/bases/geometry.h:95-119 for one tangent (algo::cross,
+ *             include/algo/cross.h, of one 2-vector: (t1, -t0));
+ *             include/forces/tension.h:148-200 (tension1d),
+ *             include/forces/skalak.h:49-55, include/forces/hookean.h:48-54
  *
  * Parity unpinned: the reference's membrane code is device lambdas over its
  * linalg layer and does not build on the host here, so this restatement is
@@ -343,5 +347,63 @@ void ibo_membrane_repelling(double modulus, double height, double range, int npo
 		const double fy = r < 2 ? -log(r / 2) * exp(-4 / (4 - r * r)) : 0.0;
 		const double fc[3] = {0.0, fy, 0.0};
 		for (int k = 0; k < 3; ++k) f[k * n + p] = -modulus * fc[k] * sigma[p];
+	}
+}
+
+void ibo_curve_geometry(int ns, int nd, int nc, const double* const* ops, const double* weights,
+                        const double* x, double* const* out)
+{
+	const long long n = (long long) ns * nc;
+	/* out[0..2] = position, t, tt: ops[0..2] times x (2 nc columns) */
+	for (int q = 0; q < 3; ++q) {
+		double* y = out[q];
+		if (!y) continue;
+		if (q == 0 && !ops[0]) {
+			for (long long i = 0; i < 2LL * nd * nc; ++i) y[i] = x[i];
+			continue;
+		}
+		const double* op = ops[q];
+		for (int j = 0; j < 2 * nc; ++j)
+			for (int r = 0; r < ns; ++r) {
+				double s = 0.0;
+				for (int k = 0; k < nd; ++k) s += op[(size_t) k * ns + r] * x[(size_t) j * nd + k];
+				y[(size_t) j * ns + r] = s;
+			}
+	}
+	for (long long p = 0; p < n; ++p) {
+		const double c0 = out[1][n + p], c1 = -out[1][p];
+		const double detf = sqrt(c0 * c0 + c1 * c1);
+		if (out[3]) {
+			out[3][p] = c0 / detf;
+			out[3][n + p] = c1 / detf;
+		}
+		out[4][p] = weights[p % ns] * detf;
+	}
+}
+
+void ibo_curve_tension(int law, double e, double kappa, int npoints, const double* const* rest,
+                       const double* const* cur, double* f)
+{
+	const long long n = npoints;
+	for (long long p = 0; p < n; ++p) {
+		const double ou[2] = {rest[0][p], rest[0][n + p]}, ouu[2] = {rest[1][p], rest[1][n + p]};
+		const double u[2] = {cur[0][p], cur[0][n + p]}, uu[2] = {cur[1][p], cur[1][n + p]};
+		/* helper (tension.h:148-158): i = t . t, i' = 2 G_00,0 = 2 tt . t */
+		const double oi = ou[0] * ou[0] + ou[1] * ou[1], odi = 2 * (ouu[0] * ou[0] + ouu[1] * ou[1]);
+		const double ci = u[0] * u[0] + u[1] * u[1], cdi = 2 * (uu[0] * u[0] + uu[1] * u[1]);
+		const double i = ci / oi;
+		const double iu = (cdi - i * odi) / oi;
+		double phi, phi1;
+		if (law == 0) {                     /* skalak1d */
+			phi = e * (i - 1) - kappa * i * (i * i - 1);
+			phi1 = e - kappa * (3 * i * i - 1);
+		} else {                            /* hookean1d */
+			const double j = sqrt(i);
+			phi = e * (1 - 1. / j);
+			phi1 = e / (2 * i * j);
+		}
+		const double phiu = phi1 * iu;
+		for (int k = 0; k < 2; ++k)
+			f[k * n + p] = rest[2][p] / oi * (+ phi * uu[k] - odi / (2 * oi) * phi * u[k] + phiu * u[k]);
 	}
 }

@@ -116,6 +116,16 @@ void ibo_membrane_tether(double modulus, int npoints, const double* x_rest, cons
 void ibo_membrane_repelling(double modulus, double height, double range, int npoints, const double* x,
                             const double* sigma, double* f);
 
+/* Curves (2 components): ops[0..2] = evaluation (NULL: samples are the data
+ * sites), d/ds, d2/ds2 (ns x nd, column-major); x 2*nd*nc; out[0..4] =
+ * position, t, tt (2*ns*nc each), normal (2*ns*nc) and sigma (ns*nc), NULL to
+ * skip (t and sigma required).  ibo_curve_tension: law 0 skalak1d, 2
+ * hookean1d; rest[0..2] = t, tt, sigma; cur[0..1] = t, tt; f 2*npoints. */
+void ibo_curve_geometry(int ns, int nd, int nc, const double* const* ops, const double* weights,
+                        const double* x, double* const* out);
+void ibo_curve_tension(int law, double e, double kappa, int npoints, const double* const* rest,
+                       const double* const* cur, double* f);
+
 /* Implicit diffusion step on one component grid (ibk_fluid_oracle.c):
  * points / periodic / shift per axis (dims of them), res the resolution,
  * robin[axis][side][2] the wall conditions (a, b).  ibo_wall_weights: out =

@@ -129,6 +129,10 @@ def lib():
                                                ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
             L.ibo_membrane_dissipation.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
                                                    ctypes.c_double, _dp, ctypes.POINTER(_dp), _dp]
+            L.ibo_curve_geometry.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
+                                             _dp, _dp, ctypes.POINTER(_dp)]
+            L.ibo_curve_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                            ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
             L.ibo_membrane_tether.argtypes = [ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
             L.ibo_membrane_repelling.argtypes = [ctypes.c_double, ctypes.c_double, ctypes.c_double, ctypes.c_int,
                                                  _dp, _dp, _dp]
@@ -321,6 +325,38 @@ def membrane_dissipation(sample_ops, modulus, u, cur, nc):
     f = np.zeros(3 * ns * nc)
     sp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cms])
     lib().ibo_membrane_dissipation(ns, nd, nc, sp, float(modulus), _d(uu), (_dp * 6)(*[_d(a) for a in c]), _d(f))
+    return f
+
+
+CURVE_FIELDS = ("position", "tu", "tuu", "normal", "sigma")
+
+
+def curve_geometry(ops, weights, x, nc):
+    """Geometry of nc closed curves in a two-dimensional run
+    (include/bases/geometry.h:74-124 with one tangent): ops = three (ns, nd)
+    arrays (evaluation or None, d/ds, d2/ds2), x 2*nd*nc positions; returns
+    a dict of the CURVE_FIELDS arrays."""
+    weights = np.ascontiguousarray(weights, dtype=np.float64)
+    ns = weights.size
+    cm = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in ops]
+    x = np.ascontiguousarray(x, dtype=np.float64)
+    m = ns * nc
+    out = {k: np.zeros(m if k == "sigma" else 2 * m) for k in CURVE_FIELDS}
+    opp = (_dp * 3)(*[None if o is None else o.ctypes.data_as(_dp) for o in cm])
+    outp = (_dp * 5)(*[_d(out[k]) for k in CURVE_FIELDS])
+    lib().ibo_curve_geometry(ns, cm[1].shape[1], nc, opp, _d(weights), _d(x), outp)
+    return out
+
+
+def curve_tension(law, shear, bulk, rest, cur):
+    """One-dimensional tension (include/forces/tension.h:160-200; law 0
+    skalak1d, 2 hookean1d) from rest and current curve geometry dicts."""
+    keep = [np.ascontiguousarray(rest[k], dtype=np.float64) for k in ("tu", "tuu", "sigma")]
+    keep += [np.ascontiguousarray(cur[k], dtype=np.float64) for k in ("tu", "tuu")]
+    n = keep[2].size
+    f = np.zeros(2 * n)
+    lib().ibo_curve_tension(int(law), float(shear), float(bulk), n, (_dp * 3)(*[_d(a) for a in keep[:3]]),
+                            (_dp * 2)(*[_d(a) for a in keep[3:]]), _d(f))
     return f
 
 

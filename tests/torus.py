@@ -104,3 +104,29 @@ def totals(f, x, n):
     F = f.reshape(3, n)
     X = x.reshape(3, n)
     return F.sum(axis=1), np.cross(X.T, F.T).sum(axis=0)
+
+
+# ---- closed curves for the two-dimensional (curve) forces
+def curve_shape(n, R=1.0, A=None, eps=0.0):
+    """Analytic geometry of A @ circle(R) + eps * bump on n equispaced
+    parameter values: dict of (2, n) arrays position, tu, tuu."""
+    s = 2 * np.pi * np.arange(n) / n
+    c, si = np.cos(s), np.sin(s)
+    c3, s3 = np.cos(3 * s), np.sin(3 * s)
+    g = {"position": np.stack([R * c, R * si]), "tu": np.stack([-R * si, R * c]),
+         "tuu": np.stack([-R * c, -R * si])}
+    b = {"position": np.stack([c3, s3 * c]),
+         "tu": np.stack([-3 * s3, 3 * c3 * c - s3 * si]),
+         "tuu": np.stack([-9 * c3, -9 * s3 * c - 3 * c3 * si - 3 * c3 * si - s3 * c])}
+    A = np.eye(2) if A is None else np.asarray(A, dtype=np.float64)
+    return {k: A @ g[k] + eps * b[k] for k in g}
+
+
+def curve_weights(n):
+    return np.full(n, 2 * np.pi / n)
+
+
+def curve_operators(n):
+    """Fourier evaluation (identity), d/ds and d2/ds2 on n equispaced points
+    (even n): exact for trigonometric polynomials of degree below n/2."""
+    return [np.eye(n), _d1(n), _d2(n)]
