@@ -275,7 +275,7 @@ def run_ours(args):
         elif args.leg == "membrane":
             res = run_membrane(ibk, dev, steps=max(5, args.steps))
         elif args.leg == "fluid":
-            res = run_fluid(ibk, W, dev, steps=max(3, args.steps // 2))
+            res = run_fluid(ibk, W, dev, steps=max(3, args.steps // 2), workload=args.workload)
         else:
             res = run_serving(ibk, W, dev, seed=rank, rates=[1000, 2000, 5000, 10000, 20000, 50000])
         if rank == 0:
@@ -870,14 +870,15 @@ def run_membrane(ibk, dev, steps, nc=64, ns=10000, nd=2500, warmup=3):
                     "kernels; median of the timed steps, CUDA events"}
 
 
-def run_fluid(ibk, W, dev, steps, warmup=1):
+def run_fluid(ibk, W, dev, steps, warmup=1, workload="large-channel"):
     """The fluid step that consumes the spread's force density: one implicit
     diffusion step (Crank-Nicolson, gamma = 1) of the x-velocity grid of the
-    large channel (512 x 256 x 512 cells, walls in y: Dirichlet), mu = 1,
-    timestep 1e-3 (internal units: mu k / h^2 = 1.6), solver tolerance 1e-11
-    as the reference's drivers set it.  Random velocity, force and rhs."""
+    large channel (512 x 256 x 512 cells, walls in y: Dirichlet; or another
+    channel workload's grid), mu = 1, timestep 1e-3 (internal units: mu k /
+    h^2 = 1.6), solver tolerance 1e-11 as the reference's drivers set it.
+    Random velocity, force and rhs."""
     import torch
-    w = make_workload("large-channel")
+    w = make_workload(workload)
     dom = ibk.Domain(*[ibk.Dimension(l, b) for l, b in zip(w.lengths, w.boundaries)])
     plan = ibk.Plan(ibk.Mac(w.refinement), dom, ibk.Bspline(3), ibk.FP64)
     d = ibk.Diffusion(plan, 0, 1e-3, 1.0, tolerance=1e-11, max_iterations=5000)
@@ -900,7 +901,8 @@ def run_fluid(ibk, W, dev, steps, warmup=1):
     iters = int(np.median(its))
     per_iter_bytes = 13 * 8.0 * d.size     # operator (2 vectors), update (8), direction (3)
     peak, _ = measured_peaks()
-    res = {"faces": d.size, "grid": "512x256x512 (x faces)", "steps": steps, "ms_per_step": ms,
+    res = {"faces": d.size, "grid": "x".join(str(int(round(l / 0.025))) for l in w.lengths) + " (x faces)",
+           "steps": steps, "ms_per_step": ms,
            "iterations": iters, "ms_per_iteration": ms / max(iters, 1),
            "iteration_gbs": per_iter_bytes * iters / (ms * 1e-3) / 1e9,
            "iteration_frac_of_hbm": per_iter_bytes * iters / (ms * 1e-3) / 1e9 / peak,

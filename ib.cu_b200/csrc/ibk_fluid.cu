@@ -19,6 +19,7 @@
 // below tolerance^2) with a Jacobi preconditioner in place of the
 // reference's Chebyshev one, which changes the iteration count, not the
 // solution it converges to.  FP64, compiled without contraction.
+#include <algorithm>
 #include <cmath>
 #include <string>
 #include <vector>
@@ -64,50 +65,112 @@ __device__ __forceinline__ void face_coords(long long idx, int P0, int P1, int& 
 	}
 }
 
-__device__ __forceinline__ double axis_apply(const AxisOps& a, const double* __restrict__ u, long long idx, int i,
-                                             long long stride)
-{
-	// tridiagonal row i along this axis (wrapping on a periodic axis)
-	const double um = i > 0 ? u[idx - stride] : (a.periodic ? u[idx + (long long) (a.P - 1) * stride] : 0.0);
-	const double up = i + 1 < a.P ? u[idx + stride] : (a.periodic ? u[idx - (long long) (a.P - 1) * stride] : 0.0);
-	return a.lo[i] * um + a.diag[i] * u[idx] + a.hi[i] * up;
-}
+// op 0: L u, 1: I~ u, 2: (I~ - lambda L) u, per face
+//     (L u) = Iz Iy (Lx u) + Iz (Ly u) Ix + (Lz u) Iy Ix
+// with (L_d u) = lo u[-1] + diag u + hi u[+1] along axis d (wrapping on a
+// periodic axis).  Each thread marches along z through kMarchZ planes of one
+// (x, y) column: its x and y coefficients and neighbour offsets are taken
+// once, the z neighbours move through registers (one new load per face), and
+// no face needs a division for its coordinates.  A block is 32 columns along
+// x (one warp, coalesced) by 8 along y.  With dot != nullptr the per-block
+// partial sums of u . out go to dot[block] (fixed order).
+constexpr int kMarchX = 32, kMarchY = 8, kMarchZ = 16;
 
-// op 0: L u, 1: I~ u, 2: (I~ - lambda L) u.  With dot != nullptr also the
-// per-block partial sums of u . out (fixed grid and block order).
-__global__ void __launch_bounds__(kFluidThreads)
-apply_kernel(FluidOps o, int op, const double* __restrict__ u, double* __restrict__ out, double* __restrict__ dot)
+template <int OP, int DIMS>
+__global__ void __launch_bounds__(kMarchX * kMarchY, 5)
+march_apply_kernel(FluidOps o, const double* __restrict__ u, double* __restrict__ out, double* __restrict__ dot)
 {
-	__shared__ double red[kFluidThreads / 32];
+	constexpr int op = OP;
+	__shared__ double red[kMarchY];
+	const int P0 = o.ax[0].P;
+	const int P1 = DIMS > 1 ? o.ax[1].P : 1;
+	const int P2 = DIMS > 2 ? o.ax[2].P : 1;
+	const int i = blockIdx.x * kMarchX + threadIdx.x;
+	const int j = blockIdx.y * kMarchY + threadIdx.y;
+	const int k0 = blockIdx.z * kMarchZ;
+	const int k1 = min(k0 + kMarchZ, P2);
 	double acc = 0.0;
-	const int P0 = o.ax[0].P, P1 = o.ax[1].P;
-	for (long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x; idx < o.size;
-	     idx += (long long) gridDim.x * blockDim.x) {
-		int i, j, k;
-		face_coords(idx, P0, P1, i, j, k);
-		const double ix = o.ax[0].id[i], iy = o.dims > 1 ? o.ax[1].id[j] : 1.0;
-		const double iz = o.dims > 2 ? o.ax[2].id[k] : 1.0;
-		double v = 0.0;
-		if (op != 1) {
-			double l = iz * iy * axis_apply(o.ax[0], u, idx, i, 1);
-			if (o.dims > 1) l += iz * axis_apply(o.ax[1], u, idx, j, P0) * ix;
-			if (o.dims > 2) l += axis_apply(o.ax[2], u, idx, k, (long long) P0 * P1) * iy * ix;
-			v = l;
+	if (i < P0 && j < P1) {
+		// 32-bit offsets: the plan's grids hold fewer than 2^31 faces
+		const int sy = P0, sz = P0 * P1;
+		const AxisOps& X = o.ax[0];
+		const double ix = X.id[i], xl = X.lo[i], xd = X.diag[i], xh = X.hi[i];
+		const bool has_xm = i > 0 || X.periodic, has_xp = i + 1 < P0 || X.periodic;
+		const int dxm = i > 0 ? -1 : P0 - 1, dxp = i + 1 < P0 ? 1 : 1 - P0;
+		double iy = 1.0, yl = 0.0, yd = 0.0, yh = 0.0;
+		bool has_ym = false, has_yp = false;
+		int dym = 0, dyp = 0;
+		if (DIMS > 1) {
+			const AxisOps& Y = o.ax[1];
+			iy = Y.id[j]; yl = Y.lo[j]; yd = Y.diag[j]; yh = Y.hi[j];
+			has_ym = j > 0 || Y.periodic;
+			has_yp = j + 1 < P1 || Y.periodic;
+			dym = j > 0 ? -sy : (P1 - 1) * sy;
+			dyp = j + 1 < P1 ? sy : (1 - P1) * sy;
 		}
-		if (op == 1) v = iz * iy * ix * u[idx];
-		if (op == 2) v = iz * iy * ix * u[idx] - o.lambda * v;
-		out[idx] = v;
-		if (dot) acc += u[idx] * v;
+		const AxisOps& Z = o.ax[2];
+		const int base = i + j * sy + k0 * sz;
+		const double* __restrict__ pu = u + base;      // this column at plane k
+		double* __restrict__ po = out + base;
+		// register window along z: uzm, uc, uzp = planes k - 1, k, k + 1 (wrapped
+		// on a periodic axis, 0 past a wall), and the plane after next loaded
+		// one iteration ahead
+		double uc = pu[0];
+		double uzm = 0.0, uzp = 0.0;
+		if (DIMS > 2) {
+			uzm = k0 > 0 ? pu[-sz] : (Z.periodic ? pu[(P2 - 1) * sz] : 0.0);
+			uzp = k0 + 1 < P2 ? pu[sz] : (Z.periodic ? pu[(1 - P2) * sz] : 0.0);
+		}
+		for (int k = k0; k < k1; ++k) {
+			double unx = 0.0;
+			if (DIMS > 2 && k + 1 < k1)      // k + 2 <= P2: plane k + 2, or plane 0 past a periodic end
+				unx = k + 2 < P2 ? pu[2 * sz] : (Z.periodic ? pu[(2 - P2) * sz] : 0.0);
+			const double iz = DIMS > 2 ? Z.id[k] : 1.0;
+			double v = 0.0;
+			if (op != 1) {
+				const double um = has_xm ? pu[dxm] : 0.0, up = has_xp ? pu[dxp] : 0.0;
+				double l = iz * iy * (xl * um + xd * uc + xh * up);
+				if (DIMS > 1) {
+					const double vm = has_ym ? pu[dym] : 0.0, vp = has_yp ? pu[dyp] : 0.0;
+					l += iz * (yl * vm + yd * uc + yh * vp) * ix;
+				}
+				if (DIMS > 2) l += (Z.lo[k] * uzm + Z.diag[k] * uc + Z.hi[k] * uzp) * iy * ix;
+				v = l;
+			}
+			if (op == 1) v = iz * iy * ix * uc;
+			if (op == 2) v = iz * iy * ix * uc - o.lambda * v;
+			*po = v;
+			if (dot) acc += uc * v;
+			uzm = uc;
+			uc = uzp;
+			uzp = unx;
+			pu += sz;
+			po += sz;
+		}
 	}
 	if (!dot) return;
 	for (int s = 16; s > 0; s >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, s);
-	if ((threadIdx.x & 31) == 0) red[threadIdx.x >> 5] = acc;
+	if (threadIdx.x == 0) red[threadIdx.y] = acc;
 	__syncthreads();
-	if (threadIdx.x == 0) {
+	if (threadIdx.x == 0 && threadIdx.y == 0) {
 		double t = 0.0;
-		for (int w = 0; w < kFluidThreads / 32; ++w) t += red[w];
-		dot[blockIdx.x] = t;
+		for (int w = 0; w < kMarchY; ++w) t += red[w];
+		dot[blockIdx.x + gridDim.x * (blockIdx.y + gridDim.y * blockIdx.z)] = t;
 	}
+}
+
+template <int OP>
+void launch_march_dims(const FluidOps& o, dim3 grid, const double* u, double* out, double* dot, cudaStream_t s)
+{
+	if (o.dims == 3) march_apply_kernel<OP, 3><<<grid, dim3(kMarchX, kMarchY), 0, s>>>(o, u, out, dot);
+	else march_apply_kernel<OP, 2><<<grid, dim3(kMarchX, kMarchY), 0, s>>>(o, u, out, dot);
+}
+
+void launch_march(const FluidOps& o, int op, dim3 grid, const double* u, double* out, double* dot, cudaStream_t s)
+{
+	if (op == 0) launch_march_dims<0>(o, grid, u, out, dot, s);
+	else if (op == 1) launch_march_dims<1>(o, grid, u, out, dot, s);
+	else launch_march_dims<2>(o, grid, u, out, dot, s);
 }
 
 // Reciprocal of the diagonal of I~ - lambda L (the Jacobi preconditioner).
@@ -141,12 +204,30 @@ __device__ __forceinline__ void block_partial(double acc, double* __restrict__ o
 	}
 }
 
-// Sum of the per-block partials into *out (one thread, fixed order).
-__global__ void sum_kernel(const double* __restrict__ partial, int n, double* __restrict__ out)
+// Sum of n per-block partials by one block of kSumThreads threads in a
+// fixed order (strided per-thread sums, then a fixed tree); every thread
+// returns the total.
+constexpr int kSumThreads = 256;
+
+__device__ __forceinline__ double sum_partials(const double* __restrict__ partial, int n)
 {
+	__shared__ double s[kSumThreads];
 	double t = 0.0;
-	for (int b = 0; b < n; ++b) t += partial[b];
-	*out = t;
+	for (int b = threadIdx.x; b < n; b += kSumThreads) t += partial[b];
+	s[threadIdx.x] = t;
+	__syncthreads();
+	for (int w = kSumThreads / 2; w > 0; w >>= 1) {
+		if (threadIdx.x < w) s[threadIdx.x] += s[threadIdx.x + w];
+		__syncthreads();
+	}
+	return s[0];
+}
+
+__global__ void __launch_bounds__(kSumThreads) sum_kernel(const double* __restrict__ partial, int n,
+                                                          double* __restrict__ out)
+{
+	const double t = sum_partials(partial, n);
+	if (threadIdx.x == 0) *out = t;
 }
 
 // rhs = k I~ f + k mu (L u + rhs0): the right-hand side of the solve
@@ -182,21 +263,23 @@ start_kernel(long long n, const double* __restrict__ r, const double* __restrict
 // [2] |d|^2, [3] alpha, [4] beta, [5] stop (1 when nu fell below tol^2).
 
 // nu from its partials; alpha = delta / nu, or stop (pcg.h:23-31).
-__global__ void alpha_kernel(const double* __restrict__ partial, int n, double tol2, double* __restrict__ sc)
+__global__ void __launch_bounds__(kSumThreads) alpha_kernel(const double* __restrict__ partial, int n, double tol2,
+                                                            double* __restrict__ sc)
 {
-	double t = 0.0;
-	for (int b = 0; b < n; ++b) t += partial[b];
+	const double t = sum_partials(partial, n);
+	if (threadIdx.x != 0) return;
 	sc[1] = t;
 	if (fabs(t) < tol2) { sc[5] = 1.0; sc[3] = 0.0; return; }
 	sc[3] = sc[0] / t;
 }
 
 // delta_new from its partials; beta = delta_new / delta (pcg.h:36-39).
-__global__ void beta_kernel(const double* __restrict__ partial, int n, double* __restrict__ sc)
+__global__ void __launch_bounds__(kSumThreads) beta_kernel(const double* __restrict__ partial, int n,
+                                                           double* __restrict__ sc)
 {
 	if (sc[5] != 0.0) return;
-	double t = 0.0;
-	for (int b = 0; b < n; ++b) t += partial[b];
+	const double t = sum_partials(partial, n);
+	if (threadIdx.x != 0) return;
 	sc[4] = t / sc[0];
 	sc[0] = t;
 }
@@ -277,7 +360,9 @@ struct ibk_diffusion_s {
 	int max_iterations = 0;
 	double* coef = nullptr;        // per axis: lo, diag, hi, id (4 P_d doubles)
 	double* work = nullptr;        // b, r, d, q, x, diag, tmp (7 size doubles)
-	double* partial = nullptr;     // 2 * kFluidBlocks partial sums
+	double* partial = nullptr;     // partial sums: max(march blocks, kFluidBlocks) + kFluidBlocks
+	dim3 march_grid;               // march_apply_kernel's grid
+	int march_blocks = 0;
 	double* scalars = nullptr;     // device scalars of the loop (see alpha_kernel)
 };
 
@@ -350,9 +435,19 @@ ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin
 		d->ops.ax[a].periodic = periodic;
 		off += 4 * P;
 	}
+	d->march_grid = dim3((unsigned) ((d->ops.ax[0].P + kMarchX - 1) / kMarchX),
+	                     (unsigned) ((d->ops.ax[1].P + kMarchY - 1) / kMarchY),
+	                     (unsigned) ((d->ops.ax[2].P + kMarchZ - 1) / kMarchZ));
+	d->march_blocks = (int) (d->march_grid.x * d->march_grid.y * d->march_grid.z);
+	if (d->march_grid.y > 65535u || d->march_grid.z > 65535u || size >= (1LL << 31)) {
+		delete d;
+		return set_error(IBK_ERR_UNSUPPORTED, "grid too large for the operator kernel (2^31 faces)");
+	}
+	const int first_partials = std::max(d->march_blocks, kFluidBlocks);
 	cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d->coef), sizeof(double) * (size_t) total);
 	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->work), sizeof(double) * 7 * (size_t) size);
-	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->partial), sizeof(double) * 2 * kFluidBlocks);
+	if (e == cudaSuccess)
+		e = cudaMalloc(reinterpret_cast<void**>(&d->partial), sizeof(double) * (size_t) (first_partials + kFluidBlocks));
 	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->scalars), sizeof(double) * 8);
 	if (e == cudaSuccess) e = cudaMemcpy(d->coef, host.data(), sizeof(double) * (size_t) total, cudaMemcpyHostToDevice);
 	if (e != cudaSuccess) {
@@ -405,8 +500,8 @@ ibk_status ibk_diffusion_apply(ibk_diffusion d, int op, const double* u, double*
 {
 	if (!d || !u || !out || op < 0 || op > 2) return set_error(IBK_ERR_INVALID_ARGUMENT, "null arrays or unknown operator");
 	cudaStream_t s = static_cast<cudaStream_t>(stream);
-	apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, op, u, out, nullptr);
-	return check_launch("apply_kernel");
+	launch_march(d->ops, op, d->march_grid, u, out, nullptr, s);
+	return check_launch("march_apply_kernel");
 }
 
 ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, const double* rhs, const double* f,
@@ -422,19 +517,20 @@ ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, co
 	double* x = q + n;
 	double* diag = x + n;
 	double* tmp = diag + n;
-	double* pa = d->partial;
-	double* pb = d->partial + kFluidBlocks;
+	double* pa = d->partial;                                            // march_blocks or kFluidBlocks
+	double* pb = d->partial + std::max(d->march_blocks, kFluidBlocks);   // kFluidBlocks
 	double* sc = d->scalars;
 	const double k = gamma * d->timestep;
 	// rhs of the solve: k I~ f + k mu (L u + rhs)
-	apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 0, u, tmp, nullptr);
-	apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 1, f, q, nullptr);
+	const dim3 mg = d->march_grid;
+	launch_march(d->ops, 0, mg, u, tmp, nullptr, s);
+	launch_march(d->ops, 1, mg, f, q, nullptr, s);
 	rhs_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, k, k * d->mu, tmp, rhs, q, b);
 	cudaError_t e = cudaMemcpyAsync(r, b, sizeof(double) * (size_t) n, cudaMemcpyDeviceToDevice, s);
 	if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
 	start_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, r, diag, x, dv, pa, pb);
-	sum_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc + 0);
-	sum_kernel<<<1, 1, 0, s>>>(pb, kFluidBlocks, sc + 2);
+	sum_kernel<<<1, kSumThreads, 0, s>>>(pa, kFluidBlocks, sc + 0);
+	sum_kernel<<<1, kSumThreads, 0, s>>>(pb, kFluidBlocks, sc + 2);
 	ibk_status st = check_launch("diffusion set-up kernels");
 	if (st != IBK_OK) return st;
 	e = cudaMemsetAsync(sc + 5, 0, sizeof(double), s);
@@ -453,12 +549,12 @@ ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, co
 			if (iterations) *iterations = it;
 			return set_error(IBK_ERR_DEVICE_CHECK, "diffusion solve did not converge within max_iterations");
 		}
-		apply_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(d->ops, 2, dv, q, pa);
-		alpha_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, tol * tol, sc);
+		launch_march(d->ops, 2, mg, dv, q, pa, s);
+		alpha_kernel<<<1, kSumThreads, 0, s>>>(pa, d->march_blocks, tol * tol, sc);
 		update_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, dv, q, x, r, diag, pa);
-		beta_kernel<<<1, 1, 0, s>>>(pa, kFluidBlocks, sc);
+		beta_kernel<<<1, kSumThreads, 0, s>>>(pa, kFluidBlocks, sc);
 		direction_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, q, dv, pb);
-		sum_kernel<<<1, 1, 0, s>>>(pb, kFluidBlocks, sc + 2);
+		sum_kernel<<<1, kSumThreads, 0, s>>>(pb, kFluidBlocks, sc + 2);
 		if ((st = check_launch("diffusion iteration kernels")) != IBK_OK) return st;
 		++it;
 	}
