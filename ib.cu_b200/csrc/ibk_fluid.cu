@@ -286,7 +286,7 @@ __global__ void __launch_bounds__(kSumThreads) beta_kernel(const double* __restr
 
 // x += alpha d, r -= alpha q, q = M^-1 r; partial sums of r . q.  Does
 // nothing once the loop has stopped.
-__global__ void __launch_bounds__(kFluidThreads)
+__global__ void __launch_bounds__(kFluidThreads, 8)
 update_kernel(long long n, const double* __restrict__ sc, const double* __restrict__ d, double* __restrict__ q,
               double* __restrict__ x, double* __restrict__ r, const double* __restrict__ dinv, double* __restrict__ rq)
 {
