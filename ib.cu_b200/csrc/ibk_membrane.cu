@@ -30,6 +30,7 @@ struct ibk_surface_plan_s {
 	cublasHandle_t blas = nullptr;
 	double* scratch = nullptr;      // bending's intermediate fields, grown on use
 	size_t scratch_bytes = 0;
+	const double** gemm_ptrs = nullptr;   // device pointer arrays of a batched product: A[6], B[6], C[6]
 };
 
 namespace ibk {
@@ -413,14 +414,37 @@ ibk_status blas_check(cublasStatus_t st, const char* what)
 
 int blocks_of(long long n) { return (int) ((n + kMembraneThreads - 1) / kMembraneThreads); }
 
+// Pointer arrays of one batched product, written on the stream (so a call
+// needs no host-to-device copy and stays in stream order).
+struct GemmPtrs {
+	const double* a[6];
+	const double* b;
+	double* c[6];
+	int count;
+};
+
+__global__ void gemm_ptrs_kernel(GemmPtrs g, const double** dst)
+{
+	const int i = threadIdx.x;
+	if (i < g.count) {
+		dst[i] = g.a[i];
+		dst[6 + i] = g.b;
+		dst[12 + i] = g.c[i];
+	}
+}
+
 // Operator products of one plan: out[q] = ops[q] (ns x nd) * y (nd x cols),
 // column-major, for the q with out[q] set (q = 0: evaluation, a copy when
-// the plan has none).
+// the plan has none).  The products go to the library as one batched call:
+// one product of ns x cols outputs fills only part of the GPU's last wave of
+// tiles, several together fill it.
 ibk_status apply_ops(ibk_surface_plan_s& plan, int cols, const double* y, double* const* out, cudaStream_t s)
 {
 	ibk_status st = blas_check(cublasSetStream(plan.blas, s), "cublasSetStream");
 	if (st != IBK_OK) return st;
 	const double one = 1.0, zero = 0.0;
+	GemmPtrs g{};
+	g.b = y;
 	for (int q = 0; q < 6; ++q) {
 		if (!out[q]) continue;
 		if (q == 0 && !plan.ops[0]) {
@@ -430,11 +454,20 @@ ibk_status apply_ops(ibk_surface_plan_s& plan, int cols, const double* y, double
 			if (e != cudaSuccess) return set_error(IBK_ERR_CUDA, std::string("cudaMemcpyAsync: ") + cudaGetErrorString(e));
 			continue;
 		}
-		st = blas_check(cublasDgemm(plan.blas, CUBLAS_OP_N, CUBLAS_OP_N, plan.ns, cols, plan.nd, &one, plan.ops[q],
-		                            plan.ns, y, plan.nd, &zero, out[q], plan.ns), "cublasDgemm");
-		if (st != IBK_OK) return st;
+		g.a[g.count] = plan.ops[q];
+		g.c[g.count] = out[q];
+		++g.count;
 	}
-	return IBK_OK;
+	if (g.count == 0) return IBK_OK;
+	if (g.count == 1)
+		return blas_check(cublasDgemm(plan.blas, CUBLAS_OP_N, CUBLAS_OP_N, plan.ns, cols, plan.nd, &one, g.a[0],
+		                              plan.ns, y, plan.nd, &zero, g.c[0], plan.ns), "cublasDgemm");
+	gemm_ptrs_kernel<<<1, 32, 0, s>>>(g, plan.gemm_ptrs);
+	if ((st = check_launch("gemm_ptrs_kernel")) != IBK_OK) return st;
+	return blas_check(cublasDgemmBatched(plan.blas, CUBLAS_OP_N, CUBLAS_OP_N, plan.ns, cols, plan.nd, &one,
+	                                     plan.gemm_ptrs, plan.ns, plan.gemm_ptrs + 6, plan.nd, &zero,
+	                                     const_cast<double**>(plan.gemm_ptrs + 12), plan.ns, g.count),
+	                  "cublasDgemmBatched");
 }
 
 ibk_status geometry_impl(ibk_surface_plan_s& plan, int nc, const double* x, const ibk_surface& out, cudaStream_t s)
@@ -478,6 +511,25 @@ ibk_status grow_scratch(ibk_surface_plan_s& plan, size_t bytes, cudaStream_t s)
 	return IBK_OK;
 }
 
+// cuBLAS handle and the batched products' pointer arrays of a new plan.
+ibk_status finish_plan(ibk_surface_plan_s* plan, ibk_surface_plan* out)
+{
+	cudaGetDevice(&plan->device);
+	ibk_status st = blas_check(cublasCreate(&plan->blas), "cublasCreate");
+	if (st == IBK_OK && cudaMalloc(reinterpret_cast<void**>(&plan->gemm_ptrs), 18 * sizeof(double*)) != cudaSuccess) {
+		cudaGetLastError();
+		plan->gemm_ptrs = nullptr;
+		st = set_error(IBK_ERR_OUT_OF_MEMORY, "cudaMalloc of the product pointer arrays failed");
+	}
+	if (st != IBK_OK) {
+		if (plan->blas) cublasDestroy(plan->blas);
+		delete plan;
+		return st;
+	}
+	*out = plan;
+	return IBK_OK;
+}
+
 SurfaceFull full(const ibk_surface& g)
 {
 	return SurfaceFull{{g.t[0], g.t[1]}, {g.tt[0], g.tt[1], g.tt[2]}, g.normal, g.sigma};
@@ -506,14 +558,7 @@ ibk_status ibk_surface_plan_create(int ns, int nd, const double* const* ops, con
 	plan->nd = nd;
 	for (int q = 0; q < 6; ++q) plan->ops[q] = ops[q];
 	plan->weights = weights;
-	cudaGetDevice(&plan->device);
-	const ibk_status st = blas_check(cublasCreate(&plan->blas), "cublasCreate");
-	if (st != IBK_OK) {
-		delete plan;
-		return st;
-	}
-	*out = plan;
-	return IBK_OK;
+	return finish_plan(plan, out);
 }
 
 ibk_status ibk_curve_plan_create(int ns, int nd, const double* const* ops, const double* weights,
@@ -534,14 +579,7 @@ ibk_status ibk_curve_plan_create(int ns, int nd, const double* const* ops, const
 	plan->ops[1] = ops[1];
 	plan->ops[3] = ops[2];
 	plan->weights = weights;
-	cudaGetDevice(&plan->device);
-	const ibk_status st = blas_check(cublasCreate(&plan->blas), "cublasCreate");
-	if (st != IBK_OK) {
-		delete plan;
-		return st;
-	}
-	*out = plan;
-	return IBK_OK;
+	return finish_plan(plan, out);
 }
 
 ibk_status ibk_surface_plan_destroy(ibk_surface_plan plan)
@@ -552,6 +590,7 @@ ibk_status ibk_surface_plan_destroy(ibk_surface_plan plan)
 	cudaSetDevice(plan->device);
 	if (plan->blas) cublasDestroy(plan->blas);
 	if (plan->scratch) cudaFree(plan->scratch);
+	if (plan->gemm_ptrs) cudaFree(plan->gemm_ptrs);
 	cudaSetDevice(dev);
 	delete plan;
 	return IBK_OK;

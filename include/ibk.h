@@ -427,7 +427,10 @@ typedef struct {
  * column-major ns x nd device matrix; ops[0] may be NULL when the samples
  * are the data sites (ns == nd; the reference then copies the positions).
  * weights: ns quadrature weights.  The arrays are kept by pointer and must
- * outlive the plan.  Binds the current CUDA device. */
+ * outlive the plan.  Binds the current CUDA device.  A plan keeps per-call
+ * device state (the batched products' pointer arrays, the bending and
+ * dissipation scratch): calls that use one plan must be ordered, on one
+ * stream or synchronised between streams. */
 ibk_status ibk_surface_plan_create(int ns, int nd, const double* const* ops, const double* weights,
                                    ibk_surface_plan* out);
 ibk_status ibk_surface_plan_destroy(ibk_surface_plan plan);
