@@ -379,6 +379,10 @@ ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin
 	if (component < 0 || component >= g.dims) return set_error(IBK_ERR_INVALID_ARGUMENT, "component out of range");
 	if (!(timestep > 0.0) || !(mu >= 0.0) || !(tolerance > 0.0) || max_iterations < 1)
 		return set_error(IBK_ERR_INVALID_ARGUMENT, "timestep and tolerance must be positive, mu non-negative");
+	for (int a = 0; a < g.dims; ++a)
+		for (int side = 0; side < 2 && g.solid[a]; ++side)
+			if (robin[a][side][0] == 0.0 && robin[a][side][1] == 0.0)
+				return set_error(IBK_ERR_INVALID_ARGUMENT, "a wall's Robin condition needs a or b nonzero");
 	const CompGeom& cg = g.comp[component];
 	auto* d = new ibk_diffusion_s;
 	cudaGetDevice(&d->device);

@@ -545,9 +545,11 @@ ibk_status ibk_curve_tension(int law, double shear, double bulk, int npoints, co
 typedef struct ibk_diffusion_s* ibk_diffusion;
 
 /* robin[d][side][0..1]: (a, b) of the lower (side 0) and upper (side 1) wall
- * of axis d (ignored on periodic axes).  mu: diffusivity (viscosity /
- * density) in internal units; timestep in internal units; max_iterations
- * bounds each solve.  Allocates the component's working vectors. */
+ * of axis d (ignored on periodic axes; a wall with a = b = 0 is rejected).
+ * mu: diffusivity (viscosity / density) in internal units; timestep in
+ * internal units; max_iterations bounds each solve.  Allocates the
+ * component's working vectors; grids of 2^31 faces or more are
+ * IBK_ERR_UNSUPPORTED. */
 ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin[3][2][2], double timestep,
                                 double mu, double tolerance, int max_iterations, ibk_diffusion* out);
 ibk_status ibk_diffusion_destroy(ibk_diffusion d);

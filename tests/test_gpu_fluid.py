@@ -74,3 +74,53 @@ def test_budget_exhausted_is_reported(ibk, cuda):
         d.step(u, u, u)
     # the device stays usable
     assert torch.isfinite(d.apply(2, u)).all()
+
+
+# Grids whose sizes leave partial operator blocks on every axis (blocks of 32
+# x 8 columns marching 16 planes): 40 x 25 x 35 faces, periodic or walled,
+# and a two-dimensional grid.
+EDGE_CASES = [(3, [4.0, 2.5, 3.5], [0, 0, 0]), (3, [4.0, 2.5, 3.5], [1, 0, 1]), (3, [4.0, 2.5, 3.5], [0, 1, 0]),
+              (2, [4.0, 2.5], [0, 1])]
+ROBIN_WALLS = [((1.0, 0.0), (0.0, 1.0)), ((2.0, 0.5), (1.0, 0.0)), ((1.0, 0.0), (1.0, 0.0))]
+
+
+@pytest.mark.parametrize("case", range(len(EDGE_CASES)))
+def test_operators_on_ragged_grids_match_oracle_bit_for_bit(ibk, cuda, oracle, case):
+    import torch
+    dims, lengths, solid = EDGE_CASES[case]
+    dom = ibk.Domain(*[ibk.Dimension(l, ibk.SOLID if s else ibk.PERIODIC) for l, s in zip(lengths, solid)])
+    plan = ibk.Plan(ibk.Mac(5), dom, ibk.Bspline(3), ibk.FP64)
+    dt, mu = 2e-3, 1.5
+    for comp in range(dims):
+        fg = oracle.FluidGrid(oracle.geometry(dims, lengths, solid, tag=oracle.TAG_MAC, refinement=5), comp, ROBIN_WALLS)
+        d = ibk.Diffusion(plan, comp, dt, mu, robin=ROBIN_WALLS)
+        assert d.size == fg.size
+        u = np.random.default_rng(100 + 10 * case + comp).normal(size=fg.size)
+        U = torch.from_numpy(u).to(cuda)
+        for op in (0, 1, 2):
+            assert np.array_equal(d.apply(op, U).cpu().numpy(), oracle.diffusion_apply(fg, op, u, lam=dt * mu / 2)), \
+                (comp, op)
+
+
+@pytest.mark.parametrize("case", [1, 3])
+def test_step_on_ragged_grids_matches_oracle(ibk, cuda, oracle, case):
+    import torch
+    dims, lengths, solid = EDGE_CASES[case]
+    dom = ibk.Domain(*[ibk.Dimension(l, ibk.SOLID if s else ibk.PERIODIC) for l, s in zip(lengths, solid)])
+    plan = ibk.Plan(ibk.Mac(5), dom, ibk.Bspline(3), ibk.FP64)
+    fg = oracle.FluidGrid(oracle.geometry(dims, lengths, solid, tag=oracle.TAG_MAC, refinement=5), 0, ROBIN_WALLS)
+    dt, mu, tol = 2e-3, 1.5, 1e-12
+    d = ibk.Diffusion(plan, 0, dt, mu, tolerance=tol, robin=ROBIN_WALLS)
+    rng = np.random.default_rng(40 + case)
+    u, rhs, f = (rng.normal(size=fg.size) for _ in range(3))
+    got = d.step(*(torch.from_numpy(a).to(cuda) for a in (u, rhs, f)), gamma=1.0).cpu().numpy()
+    want, it = oracle.diffusion_step(fg, dt, mu, tol, 10000, 1.0, u, rhs, f)
+    assert d.iterations > 0 and abs(d.iterations - it) <= 2
+    assert np.abs(got - want).max() <= 1e-10 * np.abs(want).max()
+
+
+def test_degenerate_wall_is_rejected(ibk, cuda):
+    plan = _plan(ibk, ibk.Mac(8))
+    bad = [((0.0, 0.0), (0.0, 1.0)), ((1.0, 0.0), (1.0, 0.0)), ((0.0, 0.0), (0.0, 0.0))]   # x lower wall: a = b = 0
+    with pytest.raises(ibk.IbkError):
+        ibk.Diffusion(plan, 0, 2e-3, 1.5, robin=bad)
