@@ -899,15 +899,19 @@ def run_fluid(ibk, W, dev, steps, warmup=1, workload="large-channel"):
         del out
     ms = float(np.median(times))
     iters = int(np.median(its))
-    per_iter_bytes = 13 * 8.0 * d.size     # operator (2 vectors), update (8), direction (3)
+    # Chebyshev-preconditioned iteration, bytes per face: operator (d in, q
+    # out: 16), x / r update (48), the three polynomial steps (16 + 24 + 24),
+    # direction (24)
+    per_iter_bytes = 152.0 * d.size
     peak, _ = measured_peaks()
     res = {"faces": d.size, "grid": "x".join(str(int(round(l / 0.025))) for l in w.lengths) + " (x faces)",
            "steps": steps, "ms_per_step": ms,
            "iterations": iters, "ms_per_iteration": ms / max(iters, 1),
            "iteration_gbs": per_iter_bytes * iters / (ms * 1e-3) / 1e9,
            "iteration_frac_of_hbm": per_iter_bytes * iters / (ms * 1e-3) / 1e9 / peak,
-           "note": "FP64 matrix-free operator and PCG (Jacobi), the convergence test read back once per "
-                   "iteration; median of the timed steps, CUDA events"}
+           "note": "FP64 matrix-free operator and PCG with the reference's degree-4 Chebyshev preconditioner "
+                   "(Gershgorin interval), the convergence test read back once per iteration; median of the "
+                   "timed steps, CUDA events"}
     del d, plan, u, f, rhs
     torch.cuda.empty_cache()
     return res

@@ -57,6 +57,7 @@ ABI_SYMBOLS = (
     "ibk_membrane_bending", "ibk_membrane_dissipation", "ibk_membrane_tether", "ibk_membrane_repelling",
     "ibk_curve_plan_create", "ibk_curve_tension",
     "ibk_diffusion_create", "ibk_diffusion_destroy", "ibk_diffusion_apply", "ibk_diffusion_step",
+    "ibk_diffusion_set_preconditioner", "ibk_diffusion_info",
     "ibk_last_error", "ibk_status_string", "ibk_version",
 )
 OP_SPREAD, OP_INTERPOLATE, OP_STEP, OP_SPREAD_INTERPOLATE = 1, 2, 3, 4
@@ -231,6 +232,8 @@ def lib() -> ctypes.CDLL:
         L.ibk_diffusion_destroy.argtypes = [_vp]
         L.ibk_diffusion_apply.argtypes = [_vp, ctypes.c_int, _vp, _vp, _vp]
         L.ibk_diffusion_step.argtypes = [_vp, ctypes.c_double, _vp, _vp, _vp, _vp, ctypes.POINTER(ctypes.c_int), _vp]
+        L.ibk_diffusion_set_preconditioner.argtypes = [_vp, ctypes.c_int]
+        L.ibk_diffusion_info.argtypes = [_vp, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
         L.ibk_membrane_bending.argtypes = [_vp, _vp, ctypes.c_double, ctypes.c_int, ctypes.c_int, _vp, _vp,
                                            ctypes.POINTER(_Surface), ctypes.POINTER(_Surface), _vp, _vp]
         L.ibk_membrane_dissipation.argtypes = [_vp, ctypes.c_double, ctypes.c_int, _vp, ctypes.POINTER(_Surface),
@@ -888,6 +891,7 @@ def membrane_repelling(modulus, current, height=REPELLING_HEIGHT, range_=REPELLI
 
 # ------------------------------------------- the fluid step: implicit diffusion
 DIRICHLET, NEUMANN = (1.0, 0.0), (0.0, 1.0)    # Robin (a, b) of a wall: a u + b du/dn
+CHEBYSHEV, JACOBI = 0, 1                        # ibk_preconditioner
 
 
 class Diffusion:
@@ -895,9 +899,11 @@ class Diffusion:
     of a plan: step(u, rhs, f, gamma) = u + (I~ - lambda L)^-1 (k I~ f +
     k mu (L u + rhs)), k = gamma * timestep, lambda = timestep * mu / 2.
     robin[axis] = ((a, b) lower wall, (a, b) upper wall), ignored on periodic
-    axes; default Dirichlet walls."""
+    axes; default Dirichlet walls.  preconditioner: CHEBYSHEV (the
+    reference's, the default) or JACOBI."""
 
-    def __init__(self, plan, component, timestep, mu, tolerance=1e-11, max_iterations=10000, robin=None):
+    def __init__(self, plan, component, timestep, mu, tolerance=1e-11, max_iterations=10000, robin=None,
+                 preconditioner=None):
         if robin is None:
             robin = [(DIRICHLET, DIRICHLET)] * 3
         flat = (ctypes.c_double * 12)(*[float(v) for axis in robin for side in axis for v in side])
@@ -907,6 +913,16 @@ class Diffusion:
         self.handle = h
         self.size = int(plan.info.size[component])
         self.iterations = 0
+        if preconditioner is not None:
+            check(lib().ibk_diffusion_set_preconditioner(self.handle, int(preconditioner)))
+
+    def info(self):
+        """(Gershgorin interval (lower, upper) of I~ - lambda L, the four
+        Chebyshev weights)."""
+        b = (ctypes.c_double * 2)()
+        w = (ctypes.c_double * 4)()
+        check(lib().ibk_diffusion_info(self.handle, b, w))
+        return (b[0], b[1]), list(w)
 
     def apply(self, op, u, stream=None):
         """op 0: L u, 1: I~ u, 2: (I~ - lambda L) u."""

@@ -13,12 +13,14 @@
 // include/fd/identity.h:22-47, include/fd/discretization.h:47-80).  So
 //     (L u)_ijk = Iz Iy (Lx u) + Iz (Ly u) Ix + (Lz u) Iy Ix,   I~ = Iz Iy Ix,
 // a 7-point stencil whose coefficients differ from the interior only at the
-// walls: applied matrix-free here, one thread per face.  The solve is the
-// reference's preconditioned CG loop (include/solvers/pcg.h:12-45: stop when
-// |d|_2 <= tolerance for the search direction d, bail out when <d, H d> is
-// below tolerance^2) with a Jacobi preconditioner in place of the
-// reference's Chebyshev one, which changes the iteration count, not the
-// solution it converges to.  FP64, compiled without contraction.
+// walls: applied matrix-free here.  The solve is the reference's
+// preconditioned CG loop (include/solvers/pcg.h:12-45: stop when |d|_2 <=
+// tolerance for the search direction d, bail out when <d, H d> is below
+// tolerance^2) with the reference's preconditioner, a degree-4 Chebyshev
+// polynomial in H = I~ - lambda L on its Gershgorin interval
+// (include/solvers/chebpcg.h, include/solvers/preconditioners/chebyshev.h,
+// include/algo/chebyshev.h, include/algo/gershgorin.h), or, selectable, a
+// Jacobi preconditioner.  FP64, compiled without contraction.
 #include <algorithm>
 #include <cmath>
 #include <string>
@@ -65,7 +67,9 @@ __device__ __forceinline__ void face_coords(long long idx, int P0, int P1, int& 
 	}
 }
 
-// op 0: L u, 1: I~ u, 2: (I~ - lambda L) u, per face
+// op 0: L u, 1: I~ u, 2: H u with H = I~ - lambda L, 3: wa r - H u, 4: wa r -
+// H (wb r) with u = r (the steps of the Chebyshev preconditioner, whose
+// first step's wb r is formed per loaded value instead of stored), per face
 //     (L u) = Iz Iy (Lx u) + Iz (Ly u) Ix + (Lz u) Iy Ix
 // with (L_d u) = lo u[-1] + diag u + hi u[+1] along axis d (wrapping on a
 // periodic axis).  Each thread marches along z through kMarchZ planes of one
@@ -73,14 +77,18 @@ __device__ __forceinline__ void face_coords(long long idx, int P0, int P1, int& 
 // once, the z neighbours move through registers (one new load per face), and
 // no face needs a division for its coordinates.  A block is 32 columns along
 // x (one warp, coalesced) by 8 along y.  With dot != nullptr the per-block
-// partial sums of u . out go to dot[block] (fixed order).
+// partial sums of u . out (ops 0-2) or r . out (ops 3, 4) go to dot[block]
+// (fixed order).
 constexpr int kMarchX = 32, kMarchY = 8, kMarchZ = 16;
 
 template <int OP, int DIMS>
 __global__ void __launch_bounds__(kMarchX * kMarchY, 5)
-march_apply_kernel(FluidOps o, const double* __restrict__ u, double* __restrict__ out, double* __restrict__ dot)
+march_apply_kernel(FluidOps o, const double* __restrict__ u, double* __restrict__ out, double* __restrict__ dot,
+                   const double* __restrict__ rr, double wa, double wb)
 {
 	constexpr int op = OP;
+	// a loaded value of the operand: wb r for op 4, else u itself
+	auto ld = [wb](const double* p) { return OP == 4 ? wb * *p : *p; };
 	__shared__ double red[kMarchY];
 	const int P0 = o.ax[0].P;
 	const int P1 = DIMS > 1 ? o.ax[1].P : 1;
@@ -108,39 +116,50 @@ march_apply_kernel(FluidOps o, const double* __restrict__ u, double* __restrict_
 			dym = j > 0 ? -sy : (P1 - 1) * sy;
 			dyp = j + 1 < P1 ? sy : (1 - P1) * sy;
 		}
-		const AxisOps& Z = o.ax[2];
+		// z coefficients from one base: lo, diag, hi and id lie P2 apart
+		const double* __restrict__ zc = o.ax[2].lo;
+		const bool zper = o.ax[2].periodic;
 		const int base = i + j * sy + k0 * sz;
 		const double* __restrict__ pu = u + base;      // this column at plane k
+		const double* __restrict__ pr = OP == 3 ? rr + base : nullptr;   // op 4: r is u itself
 		double* __restrict__ po = out + base;
 		// register window along z: uzm, uc, uzp = planes k - 1, k, k + 1 (wrapped
 		// on a periodic axis, 0 past a wall), and the plane after next loaded
 		// one iteration ahead
-		double uc = pu[0];
+		double uc = ld(pu);
 		double uzm = 0.0, uzp = 0.0;
 		if (DIMS > 2) {
-			uzm = k0 > 0 ? pu[-sz] : (Z.periodic ? pu[(P2 - 1) * sz] : 0.0);
-			uzp = k0 + 1 < P2 ? pu[sz] : (Z.periodic ? pu[(1 - P2) * sz] : 0.0);
+			uzm = k0 > 0 ? ld(pu - sz) : (zper ? ld(pu + (P2 - 1) * sz) : 0.0);
+			uzp = k0 + 1 < P2 ? ld(pu + sz) : (zper ? ld(pu + (1 - P2) * sz) : 0.0);
 		}
 		for (int k = k0; k < k1; ++k) {
 			double unx = 0.0;
 			if (DIMS > 2 && k + 1 < k1)      // k + 2 <= P2: plane k + 2, or plane 0 past a periodic end
-				unx = k + 2 < P2 ? pu[2 * sz] : (Z.periodic ? pu[(2 - P2) * sz] : 0.0);
-			const double iz = DIMS > 2 ? Z.id[k] : 1.0;
+				unx = k + 2 < P2 ? ld(pu + 2 * sz) : (zper ? ld(pu + (2 - P2) * sz) : 0.0);
+			const double iz = DIMS > 2 ? zc[3 * P2 + k] : 1.0;
 			double v = 0.0;
 			if (op != 1) {
-				const double um = has_xm ? pu[dxm] : 0.0, up = has_xp ? pu[dxp] : 0.0;
+				const double um = has_xm ? ld(pu + dxm) : 0.0, up = has_xp ? ld(pu + dxp) : 0.0;
 				double l = iz * iy * (xl * um + xd * uc + xh * up);
 				if (DIMS > 1) {
-					const double vm = has_ym ? pu[dym] : 0.0, vp = has_yp ? pu[dyp] : 0.0;
+					const double vm = has_ym ? ld(pu + dym) : 0.0, vp = has_yp ? ld(pu + dyp) : 0.0;
 					l += iz * (yl * vm + yd * uc + yh * vp) * ix;
 				}
-				if (DIMS > 2) l += (Z.lo[k] * uzm + Z.diag[k] * uc + Z.hi[k] * uzp) * iy * ix;
+				if (DIMS > 2) l += (zc[k] * uzm + zc[P2 + k] * uc + zc[2 * P2 + k] * uzp) * iy * ix;
 				v = l;
 			}
 			if (op == 1) v = iz * iy * ix * uc;
-			if (op == 2) v = iz * iy * ix * uc - o.lambda * v;
+			if (op >= 2) v = iz * iy * ix * uc - o.lambda * v;
+			if constexpr (OP >= 3) {
+				// gemv(-1, H, s, w, t) with t = r: -(H s) + w r
+				const double rc = OP == 3 ? *pr : *pu;
+				v = wa * rc - v;
+				if (dot) acc += rc * v;
+				if (OP == 3) pr += sz;
+			} else {
+				if (dot) acc += uc * v;
+			}
 			*po = v;
-			if (dot) acc += uc * v;
 			uzm = uc;
 			uc = uzp;
 			uzp = unx;
@@ -160,17 +179,67 @@ march_apply_kernel(FluidOps o, const double* __restrict__ u, double* __restrict_
 }
 
 template <int OP>
-void launch_march_dims(const FluidOps& o, dim3 grid, const double* u, double* out, double* dot, cudaStream_t s)
+void launch_march_dims(const FluidOps& o, dim3 grid, const double* u, double* out, double* dot, const double* r,
+                       double wa, double wb, cudaStream_t s)
 {
-	if (o.dims == 3) march_apply_kernel<OP, 3><<<grid, dim3(kMarchX, kMarchY), 0, s>>>(o, u, out, dot);
-	else march_apply_kernel<OP, 2><<<grid, dim3(kMarchX, kMarchY), 0, s>>>(o, u, out, dot);
+	if (o.dims == 3) march_apply_kernel<OP, 3><<<grid, dim3(kMarchX, kMarchY), 0, s>>>(o, u, out, dot, r, wa, wb);
+	else march_apply_kernel<OP, 2><<<grid, dim3(kMarchX, kMarchY), 0, s>>>(o, u, out, dot, r, wa, wb);
 }
 
-void launch_march(const FluidOps& o, int op, dim3 grid, const double* u, double* out, double* dot, cudaStream_t s)
+void launch_march(const FluidOps& o, int op, dim3 grid, const double* u, double* out, double* dot, cudaStream_t s,
+                  const double* r = nullptr, double wa = 0.0, double wb = 0.0)
 {
-	if (op == 0) launch_march_dims<0>(o, grid, u, out, dot, s);
-	else if (op == 1) launch_march_dims<1>(o, grid, u, out, dot, s);
-	else launch_march_dims<2>(o, grid, u, out, dot, s);
+	switch (op) {
+	case 0: launch_march_dims<0>(o, grid, u, out, dot, r, wa, wb, s); break;
+	case 1: launch_march_dims<1>(o, grid, u, out, dot, r, wa, wb, s); break;
+	case 2: launch_march_dims<2>(o, grid, u, out, dot, r, wa, wb, s); break;
+	case 3: launch_march_dims<3>(o, grid, u, out, dot, r, wa, wb, s); break;
+	default: launch_march_dims<4>(o, grid, u, out, dot, r, wa, wb, s); break;
+	}
+}
+
+// Gershgorin interval of H = I~ - lambda L (algo/gershgorin.h:14-49): per
+// block the smallest diagonal - sum |off-diagonal| and the largest diagonal
+// + sum |off-diagonal| of its rows (minimum and maximum are exact in any
+// order).  part: 2 per block.
+__global__ void __launch_bounds__(kFluidThreads)
+gershgorin_kernel(FluidOps o, double* __restrict__ part)
+{
+	__shared__ double smin[kFluidThreads], smax[kFluidThreads];
+	double mn = INFINITY, mx = -INFINITY;
+	const int P0 = o.ax[0].P, P1 = o.ax[1].P;
+	for (long long idx = (long long) blockIdx.x * blockDim.x + threadIdx.x; idx < o.size;
+	     idx += (long long) gridDim.x * blockDim.x) {
+		int i, j, k;
+		face_coords(idx, P0, P1, i, j, k);
+		const double ix = o.ax[0].id[i], iy = o.dims > 1 ? o.ax[1].id[j] : 1.0;
+		const double iz = o.dims > 2 ? o.ax[2].id[k] : 1.0;
+		double l = iz * iy * o.ax[0].diag[i];
+		if (o.dims > 1) l += iz * o.ax[1].diag[j] * ix;
+		if (o.dims > 2) l += o.ax[2].diag[k] * iy * ix;
+		const double diag = iz * iy * ix - o.lambda * l;
+		double off = fabs(o.lambda * (iz * iy * o.ax[0].lo[i])) + fabs(o.lambda * (iz * iy * o.ax[0].hi[i]));
+		if (o.dims > 1)
+			off += fabs(o.lambda * (iz * o.ax[1].lo[j] * ix)) + fabs(o.lambda * (iz * o.ax[1].hi[j] * ix));
+		if (o.dims > 2)
+			off += fabs(o.lambda * (o.ax[2].lo[k] * iy * ix)) + fabs(o.lambda * (o.ax[2].hi[k] * iy * ix));
+		mn = fmin(mn, diag - off);
+		mx = fmax(mx, diag + off);
+	}
+	smin[threadIdx.x] = mn;
+	smax[threadIdx.x] = mx;
+	__syncthreads();
+	for (int w = kFluidThreads / 2; w > 0; w >>= 1) {
+		if (threadIdx.x < w) {
+			smin[threadIdx.x] = fmin(smin[threadIdx.x], smin[threadIdx.x + w]);
+			smax[threadIdx.x] = fmax(smax[threadIdx.x], smax[threadIdx.x + w]);
+		}
+		__syncthreads();
+	}
+	if (threadIdx.x == 0) {
+		part[2 * blockIdx.x] = smin[0];
+		part[2 * blockIdx.x + 1] = smax[0];
+	}
 }
 
 // Reciprocal of the diagonal of I~ - lambda L (the Jacobi preconditioner).
@@ -304,6 +373,31 @@ update_kernel(long long n, const double* __restrict__ sc, const double* __restri
 	block_partial(a, rq);
 }
 
+// x += alpha d, r -= alpha q (the Chebyshev preconditioner and the r . z
+// partials follow in the operator kernel).  Does nothing once the loop has
+// stopped.
+__global__ void __launch_bounds__(kFluidThreads, 8)
+update_xr_kernel(long long n, const double* __restrict__ sc, const double* __restrict__ d,
+                 const double* __restrict__ q, double* __restrict__ x, double* __restrict__ r)
+{
+	if (sc[5] != 0.0) return;
+	const double alpha = sc[3];
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x) {
+		x[i] += alpha * d[i];
+		r[i] = r[i] - alpha * q[i];
+	}
+}
+
+// |d|^2 partials (the start of the loop under the Chebyshev preconditioner).
+__global__ void __launch_bounds__(kFluidThreads)
+norm_kernel(long long n, const double* __restrict__ d, double* __restrict__ dd)
+{
+	double a = 0.0;
+	for (long long i = (long long) blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long) gridDim.x * blockDim.x)
+		a += d[i] * d[i];
+	block_partial(a, dd);
+}
+
 // d = q + beta d; partial sums of d . d.
 __global__ void __launch_bounds__(kFluidThreads)
 direction_kernel(long long n, const double* __restrict__ sc, const double* __restrict__ q, double* __restrict__ d,
@@ -343,6 +437,26 @@ WallWeights wall_weights(const double* p, double h, double s_in)
 	return {(p[1] + p[0] * h * (1 - s)) / denom, (-(p[1] * (1 - 2 * s) - p[0] * s * h * (1 - s))) / (2 * denom)};
 }
 
+// impl::polynomial and impl::chebw<4> (algo/chebyshev.h:48-65, 124-145):
+// p(a, b) = sum_i c_i a^i b^(n-1-i), evaluated as the reference does.
+double cheb_poly(const double* c, int n, double a, double b)
+{
+	double v = 0.0;
+	for (int i = 0; i < n; ++i) v += c[i] * std::pow(a, i) * std::pow(b, n - 1 - i);
+	return v;
+}
+
+void chebyshev_weights(double a, double b, double* w)
+{
+	static const double p1[] = {128}, p2[] = {256, 256}, p3[] = {160, 448, 160}, p4[] = {32, 224, 224, 32};
+	static const double q[] = {1, 28, 70, 28, 1};
+	const double qv = cheb_poly(q, 5, a, b);
+	w[0] = cheb_poly(p1, 1, a, b) / qv;
+	w[1] = cheb_poly(p2, 2, a, b) / qv;
+	w[2] = cheb_poly(p3, 3, a, b) / qv;
+	w[3] = cheb_poly(p4, 4, a, b) / qv;
+}
+
 ibk_status cuda_fail(cudaError_t e, const char* what)
 {
 	return set_error(IBK_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
@@ -359,7 +473,10 @@ struct ibk_diffusion_s {
 	double mu = 0.0, timestep = 0.0, tolerance = 0.0;
 	int max_iterations = 0;
 	double* coef = nullptr;        // per axis: lo, diag, hi, id (4 P_d doubles)
-	double* work = nullptr;        // b, r, d, q, x, diag, tmp (7 size doubles)
+	double* work = nullptr;        // b, r, d, q, x, diag, tmp, tmp2 (8 size doubles)
+	int precond = IBK_PRECOND_CHEBYSHEV;
+	double cheb_w[4] = {};         // chebw<4> on the Gershgorin interval
+	double bounds[2] = {};         // that interval (lower, upper)
 	double* partial = nullptr;     // partial sums: max(march blocks, kFluidBlocks) + kFluidBlocks
 	dim3 march_grid;               // march_apply_kernel's grid
 	int march_blocks = 0;
@@ -449,7 +566,7 @@ ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin
 	}
 	const int first_partials = std::max(d->march_blocks, kFluidBlocks);
 	cudaError_t e = cudaMalloc(reinterpret_cast<void**>(&d->coef), sizeof(double) * (size_t) total);
-	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->work), sizeof(double) * 7 * (size_t) size);
+	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->work), sizeof(double) * 8 * (size_t) size);
 	if (e == cudaSuccess)
 		e = cudaMalloc(reinterpret_cast<void**>(&d->partial), sizeof(double) * (size_t) (first_partials + kFluidBlocks));
 	if (e == cudaSuccess) e = cudaMalloc(reinterpret_cast<void**>(&d->scalars), sizeof(double) * 8);
@@ -473,15 +590,46 @@ ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin
 			ax.periodic = 0;
 		}
 	}
-	// the preconditioner's reciprocal diagonal, kept in work slot 5
+	// the Jacobi preconditioner's reciprocal diagonal, kept in work slot 5, and
+	// the Gershgorin interval of the Chebyshev preconditioner (through the
+	// partial-sum buffer, 2 per block)
 	diagonal_kernel<<<kFluidBlocks, kFluidThreads>>>(d->ops, d->work + 5 * size);
-	ibk_status st = check_launch("diagonal_kernel");
-	if (st == IBK_OK && (e = cudaDeviceSynchronize()) != cudaSuccess) st = cuda_fail(e, "diffusion set-up");
+	gershgorin_kernel<<<kFluidBlocks, kFluidThreads>>>(d->ops, d->partial);
+	ibk_status st = check_launch("diffusion set-up kernels");
+	std::vector<double> part(2 * kFluidBlocks);
+	if (st == IBK_OK && (e = cudaMemcpy(part.data(), d->partial, sizeof(double) * part.size(),
+	                                    cudaMemcpyDeviceToHost)) != cudaSuccess)
+		st = cuda_fail(e, "diffusion set-up");
 	if (st != IBK_OK) {
 		ibk_diffusion_destroy(d);
 		return st;
 	}
+	double lower = INFINITY, upper = -INFINITY;
+	for (int b = 0; b < kFluidBlocks; ++b) {
+		lower = std::min(lower, part[2 * b]);
+		upper = std::max(upper, part[2 * b + 1]);
+	}
+	d->bounds[0] = lower;
+	d->bounds[1] = upper;
+	chebyshev_weights(upper, lower, d->cheb_w);     // chebyshev(upper, lower, H): preconditioners/chebyshev.h:14-25
 	*out = d;
+	return IBK_OK;
+}
+
+ibk_status ibk_diffusion_set_preconditioner(ibk_diffusion d, int kind)
+{
+	if (!d) return set_error(IBK_ERR_INVALID_ARGUMENT, "null diffusion handle");
+	if (kind != IBK_PRECOND_CHEBYSHEV && kind != IBK_PRECOND_JACOBI)
+		return set_error(IBK_ERR_INVALID_ARGUMENT, "unknown preconditioner");
+	d->precond = kind;
+	return IBK_OK;
+}
+
+ibk_status ibk_diffusion_info(ibk_diffusion d, double* bounds, double* weights)
+{
+	if (!d) return set_error(IBK_ERR_INVALID_ARGUMENT, "null diffusion handle");
+	if (bounds) { bounds[0] = d->bounds[0]; bounds[1] = d->bounds[1]; }
+	if (weights) for (int q = 0; q < 4; ++q) weights[q] = d->cheb_w[q];
 	return IBK_OK;
 }
 
@@ -521,10 +669,13 @@ ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, co
 	double* x = q + n;
 	double* diag = x + n;
 	double* tmp = diag + n;
+	double* tmp2 = tmp + n;
 	double* pa = d->partial;                                            // march_blocks or kFluidBlocks
 	double* pb = d->partial + std::max(d->march_blocks, kFluidBlocks);   // kFluidBlocks
 	double* sc = d->scalars;
 	const double k = gamma * d->timestep;
+	const bool cheb = d->precond == IBK_PRECOND_CHEBYSHEV;
+	const double* w = d->cheb_w;
 	// rhs of the solve: k I~ f + k mu (L u + rhs)
 	const dim3 mg = d->march_grid;
 	launch_march(d->ops, 0, mg, u, tmp, nullptr, s);
@@ -532,8 +683,25 @@ ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, co
 	rhs_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, k, k * d->mu, tmp, rhs, q, b);
 	cudaError_t e = cudaMemcpyAsync(r, b, sizeof(double) * (size_t) n, cudaMemcpyDeviceToDevice, s);
 	if (e != cudaSuccess) return cuda_fail(e, "cudaMemcpyAsync");
-	start_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, r, diag, x, dv, pa, pb);
-	sum_kernel<<<1, kSumThreads, 0, s>>>(pa, kFluidBlocks, sc + 0);
+	// z = M^-1 r with the r . z partials in pa: the Chebyshev polynomial
+	// (algo/chebyshev.h:152-167: s = w0 r, then s = w_i r - H s, i = 1..3)
+	auto chebyshev = [&](double* z) {
+		launch_march(d->ops, 4, mg, r, tmp, nullptr, s, r, w[1], w[0]);
+		launch_march(d->ops, 3, mg, tmp, tmp2, nullptr, s, r, w[2]);
+		launch_march(d->ops, 3, mg, tmp2, z, pa, s, r, w[3]);
+	};
+	int za = kFluidBlocks;       // the count of r . z partials
+	if (cheb) {
+		// pcg.h:14-18: x = 0, d = M^-1 r, delta = r . d
+		e = cudaMemsetAsync(x, 0, sizeof(double) * (size_t) n, s);
+		if (e != cudaSuccess) return cuda_fail(e, "cudaMemsetAsync");
+		chebyshev(dv);
+		norm_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, dv, pb);
+		za = d->march_blocks;
+	} else {
+		start_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, r, diag, x, dv, pa, pb);
+	}
+	sum_kernel<<<1, kSumThreads, 0, s>>>(pa, za, sc + 0);
 	sum_kernel<<<1, kSumThreads, 0, s>>>(pb, kFluidBlocks, sc + 2);
 	ibk_status st = check_launch("diffusion set-up kernels");
 	if (st != IBK_OK) return st;
@@ -555,8 +723,15 @@ ibk_status ibk_diffusion_step(ibk_diffusion d, double gamma, const double* u, co
 		}
 		launch_march(d->ops, 2, mg, dv, q, pa, s);
 		alpha_kernel<<<1, kSumThreads, 0, s>>>(pa, d->march_blocks, tol * tol, sc);
-		update_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, dv, q, x, r, diag, pa);
-		beta_kernel<<<1, kSumThreads, 0, s>>>(pa, kFluidBlocks, sc);
+		if (cheb) {
+			// x += alpha d, r -= alpha q, q = M^-1 r (a bail-out leaves x and r as
+			// they are; the polynomial of the unchanged r is then not used)
+			update_xr_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, dv, q, x, r);
+			chebyshev(q);
+		} else {
+			update_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, dv, q, x, r, diag, pa);
+		}
+		beta_kernel<<<1, kSumThreads, 0, s>>>(pa, za, sc);
 		direction_kernel<<<kFluidBlocks, kFluidThreads, 0, s>>>(n, sc, q, dv, pb);
 		sum_kernel<<<1, kSumThreads, 0, s>>>(pb, kFluidBlocks, sc + 2);
 		if ((st = check_launch("diffusion iteration kernels")) != IBK_OK) return st;

@@ -552,6 +552,18 @@ typedef struct ibk_diffusion_s* ibk_diffusion;
  * IBK_ERR_UNSUPPORTED. */
 ibk_status ibk_diffusion_create(ibk_plan plan, int component, const double robin[3][2][2], double timestep,
                                 double mu, double tolerance, int max_iterations, ibk_diffusion* out);
+
+/* The solve's preconditioner.  IBK_PRECOND_CHEBYSHEV (the default, the
+ * reference's solvers::chebpcg, include/solvers/chebpcg.h): z = p(H) r with
+ * p the degree-4 polynomial of algo::chebyshev (include/algo/chebyshev.h:
+ * 124-167) on the Gershgorin interval of H = I~ - lambda L
+ * (include/algo/gershgorin.h), three operator applications per solve.
+ * IBK_PRECOND_JACOBI: z = r / diag(H). */
+typedef enum { IBK_PRECOND_CHEBYSHEV = 0, IBK_PRECOND_JACOBI = 1 } ibk_preconditioner;
+ibk_status ibk_diffusion_set_preconditioner(ibk_diffusion d, int kind);
+/* The Gershgorin interval {lower, upper} of H and the four Chebyshev
+ * weights (either output may be NULL). */
+ibk_status ibk_diffusion_info(ibk_diffusion d, double* bounds, double* weights);
 ibk_status ibk_diffusion_destroy(ibk_diffusion d);
 
 /* out = op(u) over the component grid: op 0 = L, 1 = I~, 2 = I~ - lambda L. */

@@ -135,7 +135,13 @@ void ibo_diffusion_apply(int dims, const int* points, const int* periodic, const
                          const double* robin, double lambda, int op, const double* u, double* out);
 int ibo_diffusion_step(int dims, const int* points, const int* periodic, const double* shift, double res,
                        const double* robin, double timestep, double mu, double tolerance, int max_iterations,
-                       double gamma, const double* u, const double* rhs, const double* f, double* out);
+                       double gamma, int precond, const double* u, const double* rhs, const double* f, double* out);
+/* Chebyshev preconditioner pieces (precond 0 of the step; 1 is Jacobi): the
+ * Gershgorin interval {lower, upper} of I~ - lambda L, and the four weights
+ * of chebw<4>(a, b) (the step passes a = upper, b = lower). */
+void ibo_gershgorin(int dims, const int* points, const int* periodic, const double* shift, double res,
+                    const double* robin, double lambda, double* bounds);
+void ibo_chebyshev_weights(double a, double b, double* w);
 
 #ifdef __cplusplus
 }

@@ -122,8 +122,10 @@ def lib():
                                               ctypes.c_int, _dp, _dp]
             L.ibo_diffusion_step.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, _dp, ctypes.c_double,
                                              ctypes.c_double, ctypes.c_double, ctypes.c_int, ctypes.c_double,
-                                             _dp, _dp, _dp, _dp]
+                                             ctypes.c_int, _dp, _dp, _dp, _dp]
             L.ibo_diffusion_step.restype = ctypes.c_int
+            L.ibo_gershgorin.argtypes = [ctypes.c_int, _ip, _ip, _dp, ctypes.c_double, _dp, ctypes.c_double, _dp]
+            L.ibo_chebyshev_weights.argtypes = [ctypes.c_double, ctypes.c_double, _dp]
             L.ibo_membrane_bending.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp), _dp,
                                                ctypes.POINTER(_dp), ctypes.c_double, ctypes.c_int, _dp, _dp,
                                                ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
@@ -432,15 +434,34 @@ def diffusion_apply(fg: FluidGrid, op, u, lam=0.0):
     return out
 
 
-def diffusion_step(fg: FluidGrid, timestep, mu, tolerance, max_iterations, gamma, u, rhs, f):
+CHEBYSHEV, JACOBI = 0, 1
+
+
+def diffusion_step(fg: FluidGrid, timestep, mu, tolerance, max_iterations, gamma, u, rhs, f, precond=CHEBYSHEV):
     """out = u + (I~ - lambda L)^-1 (k I~ f + k mu (L u + rhs)) and the
-    iteration count (include/ins/diffusion.h:47-56)."""
+    iteration count (include/ins/diffusion.h:47-56), preconditioned as the
+    reference does (CHEBYSHEV, include/solvers/chebpcg.h) or by JACOBI."""
     u, rhs, f = (np.ascontiguousarray(a, dtype=np.float64) for a in (u, rhs, f))
     out = np.zeros(fg.size)
     it = lib().ibo_diffusion_step(fg.dims, _i(fg.points), _i(fg.periodic), _d(fg.shift), fg.res, _d(fg.robin),
                                   float(timestep), float(mu), float(tolerance), int(max_iterations), float(gamma),
-                                  _d(u), _d(rhs), _d(f), _d(out))
+                                  int(precond), _d(u), _d(rhs), _d(f), _d(out))
     return out, it
+
+
+def gershgorin(fg: FluidGrid, lam):
+    """Gershgorin interval (lower, upper) of I~ - lam L (include/algo/gershgorin.h)."""
+    out = np.zeros(2)
+    lib().ibo_gershgorin(fg.dims, _i(fg.points), _i(fg.periodic), _d(fg.shift), fg.res, _d(fg.robin), float(lam),
+                         _d(out))
+    return out
+
+
+def chebyshev_weights(a, b):
+    """The four weights of impl::chebw<4>(a, b) (include/algo/chebyshev.h)."""
+    out = np.zeros(4)
+    lib().ibo_chebyshev_weights(float(a), float(b), _d(out))
+    return out
 
 
 def ref_wall_weights(length, resolution, shift, lower, upper):

@@ -2,9 +2,12 @@
 against the reference and against the numerics it restates: the wall
 weights equal the reference's own fd::discretization bit for bit (golden
 fixture from the bridge); the operator I~ - lambda L is symmetric; the CG
-solve agrees with a dense solve; and the reference's own diffusion test case
-(test/diffusion.cc: a parabolic profile between Dirichlet walls under a
-constant force, the discrete steady state) is left unchanged by a step."""
+solve agrees with a dense solve under both preconditioners; the reference's
+Chebyshev preconditioner has the residual polynomial of a shifted,
+scaled Chebyshev polynomial on the Gershgorin interval (which holds the
+spectrum); and the reference's own diffusion test case (test/diffusion.cc:
+a parabolic profile between Dirichlet walls under a constant force, the
+discrete steady state) is left unchanged by a step."""
 import os
 
 import numpy as np
@@ -53,9 +56,31 @@ def test_step_agrees_with_a_dense_solve(oracle):
     u, rhs, f = rng.normal(size=n), rng.normal(size=n), rng.normal(size=n)
     k = gamma * dt
     want = u + np.linalg.solve(H, k * (Id @ f) + k * mu * (L @ u + rhs))
-    got, it = oracle.diffusion_step(fg, dt, mu, 1e-13, 1000, gamma, u, rhs, f)
-    assert it > 0
-    assert np.abs(got - want).max() <= 1e-10 * np.abs(want).max()
+    its = []
+    for pc in (oracle.CHEBYSHEV, oracle.JACOBI):
+        got, it = oracle.diffusion_step(fg, dt, mu, 1e-13, 1000, gamma, u, rhs, f, precond=pc)
+        assert it > 0
+        assert np.abs(got - want).max() <= 1e-10 * np.abs(want).max()
+        its.append(it)
+    assert its[0] < its[1]          # the polynomial preconditioner needs fewer iterations
+    # the Gershgorin interval holds the spectrum of the (symmetric) operator
+    lo, hi = oracle.gershgorin(fg, lam)
+    ev = np.linalg.eigvalsh((H + H.T) / 2)
+    assert lo <= ev.min() + 1e-12 and ev.max() <= hi + 1e-12
+
+
+def test_chebyshev_weights_give_the_chebyshev_residual_polynomial(oracle):
+    """With p(z) = w3 - w2 z + w1 z^2 - w0 z^3 (the reference's Horner loop,
+    algo/chebyshev.h:152-167), 1 - z p(z) = T4(s(z)) / T4(s(0)) with s the
+    affine map of [lower, upper] onto [-1, 1] (algo/chebyshev.h:9-45)."""
+    for lower, upper in ((1.0, 10.6), (0.3, 2.0), (2.5, 7.0)):
+        w = oracle.chebyshev_weights(upper, lower)
+        z = np.linspace(lower, upper, 101)
+        p = w[3] - w[2] * z + w[1] * z ** 2 - w[0] * z ** 3
+        s = (2 * z - (lower + upper)) / (upper - lower)
+        s0 = -(lower + upper) / (upper - lower)
+        T4 = lambda t: 8 * t ** 4 - 8 * t ** 2 + 1
+        assert np.abs((1 - z * p) - T4(s) / T4(s0)).max() <= 1e-12
 
 
 def test_parabolic_steady_state_is_kept(oracle):

@@ -34,18 +34,18 @@ def test_operators_match_oracle_bit_for_bit(ibk, cuda, oracle, comp):
         assert np.array_equal(got, want), op
 
 
-@pytest.mark.parametrize("comp,gamma", [(0, 0.5), (1, 1.0), (2, 0.5)])
-def test_step_matches_oracle(ibk, cuda, oracle, comp, gamma):
+@pytest.mark.parametrize("comp,gamma,pc", [(0, 0.5, 0), (1, 1.0, 0), (2, 0.5, 0), (0, 1.0, 1), (2, 0.5, 1)])
+def test_step_matches_oracle(ibk, cuda, oracle, comp, gamma, pc):
     import torch
     plan = _plan(ibk, ibk.Mac(8))
     fg = oracle.FluidGrid(oracle.geometry(3, [1.6, 0.8, 0.8], [1, 1, 0], tag=oracle.TAG_MAC, refinement=8),
                           comp, ROBIN)
     dt, mu, tol = 2e-3, 1.5, 1e-12
-    d = ibk.Diffusion(plan, comp, dt, mu, tolerance=tol, robin=ROBIN)
+    d = ibk.Diffusion(plan, comp, dt, mu, tolerance=tol, robin=ROBIN, preconditioner=pc)
     rng = np.random.default_rng(10 + comp)
     u, rhs, f = (rng.normal(size=fg.size) for _ in range(3))
     got = d.step(*(torch.from_numpy(a).to(cuda) for a in (u, rhs, f)), gamma=gamma).cpu().numpy()
-    want, it = oracle.diffusion_step(fg, dt, mu, tol, 10000, gamma, u, rhs, f)
+    want, it = oracle.diffusion_step(fg, dt, mu, tol, 10000, gamma, u, rhs, f, precond=pc)
     assert d.iterations > 0 and abs(d.iterations - it) <= 2
     assert np.abs(got - want).max() <= 1e-10 * np.abs(want).max()
 
@@ -124,3 +124,21 @@ def test_degenerate_wall_is_rejected(ibk, cuda):
     bad = [((0.0, 0.0), (0.0, 1.0)), ((1.0, 0.0), (1.0, 0.0)), ((0.0, 0.0), (0.0, 0.0))]   # x lower wall: a = b = 0
     with pytest.raises(ibk.IbkError):
         ibk.Diffusion(plan, 0, 2e-3, 1.5, robin=bad)
+
+
+@pytest.mark.parametrize("case", range(len(EDGE_CASES)))
+def test_chebyshev_interval_and_weights_match_oracle(ibk, cuda, oracle, case):
+    """The device's Gershgorin interval (a min / max over the rows, exact in
+    any order) and the host's Chebyshev weights equal the oracle's bit for
+    bit."""
+    dims, lengths, solid = EDGE_CASES[case]
+    dom = ibk.Domain(*[ibk.Dimension(l, ibk.SOLID if s else ibk.PERIODIC) for l, s in zip(lengths, solid)])
+    plan = ibk.Plan(ibk.Mac(5), dom, ibk.Bspline(3), ibk.FP64)
+    dt, mu = 2e-3, 1.5
+    for comp in range(dims):
+        fg = oracle.FluidGrid(oracle.geometry(dims, lengths, solid, tag=oracle.TAG_MAC, refinement=5), comp,
+                              ROBIN_WALLS)
+        (lo, hi), w = ibk.Diffusion(plan, comp, dt, mu, robin=ROBIN_WALLS).info()
+        want = oracle.gershgorin(fg, dt * mu / 2)
+        assert (lo, hi) == (want[0], want[1])
+        assert np.array_equal(np.array(w), oracle.chebyshev_weights(hi, lo))
