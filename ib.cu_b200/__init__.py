@@ -53,6 +53,7 @@ ABI_SYMBOLS = (
     "ibk_server_read", "ibk_server_get_stats", "ibk_server_reset_stats", "ibk_server_run_poisson",
     "ibk_server_save", "ibk_server_admit_from",
     "ibk_io_write_dense", "ibk_io_write_scalar", "ibk_io_read_dense", "ibk_io_read_scalar",
+    "ibk_io_write_sparse", "ibk_io_read_sparse",
     "ibk_surface_plan_create", "ibk_surface_plan_destroy", "ibk_surface_geometry", "ibk_membrane_tension",
     "ibk_membrane_bending", "ibk_membrane_dissipation", "ibk_membrane_tether", "ibk_membrane_repelling",
     "ibk_curve_plan_create", "ibk_curve_tension",
@@ -222,6 +223,10 @@ def lib() -> ctypes.CDLL:
                                         ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
         L.ibk_io_read_scalar.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(ctypes.c_double),
                                          ctypes.POINTER(ctypes.c_longlong)]
+        L.ibk_io_write_sparse.argtypes = [ctypes.c_char_p, ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.c_int,
+                                          ctypes.c_int, _vp, _vp, _vp]
+        L.ibk_io_read_sparse.argtypes = [ctypes.c_char_p, ctypes.c_longlong, ctypes.POINTER(IoHeader), _vp, _vp,
+                                         _vp, ctypes.c_longlong, ctypes.POINTER(ctypes.c_longlong)]
         L.ibk_surface_plan_create.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.POINTER(_vp), _vp, ctypes.POINTER(_vp)]
         L.ibk_surface_plan_destroy.argtypes = [_vp]
         L.ibk_surface_geometry.argtypes = [_vp, ctypes.c_int, _vp, ctypes.POINTER(_Surface), _vp]
@@ -969,13 +974,62 @@ def io_write(path, objects):
             raise ValueError("only vectors and matrices")
 
 
+def io_write_sparse(path, obj, append=False):
+    """Write one sparse container in the reference's binary format: a
+    scipy.sparse matrix (CSR), or a sparse vector given as (size, indices,
+    values)."""
+    import numpy as np
+    if isinstance(obj, tuple):
+        n, idx, val = obj
+        idx = np.ascontiguousarray(idx, dtype=np.int32)
+        val = np.ascontiguousarray(val, dtype=np.float64)
+        check(lib().ibk_io_write_sparse(os.fsencode(path), int(bool(append)), 0, int(n), 1, idx.size, None,
+                                        idx.ctypes.data, val.ctypes.data))
+        return
+    m = obj.tocsr()
+    starts = np.ascontiguousarray(m.indptr, dtype=np.int32)
+    idx = np.ascontiguousarray(m.indices, dtype=np.int32)
+    val = np.ascontiguousarray(m.data, dtype=np.float64)
+    check(lib().ibk_io_write_sparse(os.fsencode(path), int(bool(append)), 1, m.shape[0], m.shape[1], idx.size,
+                                    starts.ctypes.data, idx.ctypes.data, val.ctypes.data))
+
+
+def _read_sparse(path, off):
+    import numpy as np
+    import scipy.sparse as sp
+    h = IoHeader()
+    check(lib().ibk_io_read_sparse(os.fsencode(path), off, ctypes.byref(h), None, None, None, 0, None))
+    starts = np.empty(h.rows + 1 if h.matrix and h.rows > 0 else 1, dtype=np.int32)
+    idx = np.empty(max(h.count, 1), dtype=np.int32)
+    val = np.empty(max(h.count, 1), dtype=np.float64)
+    nxt = ctypes.c_longlong()
+    check(lib().ibk_io_read_sparse(os.fsencode(path), off, ctypes.byref(h), starts.ctypes.data, idx.ctypes.data,
+                                   val.ctypes.data, idx.size, ctypes.byref(nxt)))
+    idx, val = idx[:h.count], val[:h.count]
+    if h.matrix:
+        indptr = starts if h.rows > 0 else np.zeros(1, dtype=np.int32)
+        obj = sp.csr_matrix((val, idx, indptr), shape=(h.rows, h.cols))
+    else:
+        obj = (h.rows, idx, val)
+    return obj, nxt.value
+
+
 def io_read(path, count=None):
-    """Read consecutive dense containers: vectors as 1-D arrays, matrices as
-    (rows, cols) arrays (values column-major in the file)."""
+    """Read consecutive containers: dense vectors as 1-D arrays, dense
+    matrices as (rows, cols) arrays (values column-major in the file),
+    sparse matrices as scipy.sparse CSR matrices and sparse vectors as
+    (size, indices, values)."""
     import numpy as np
     out, off = [], 0
     size = os.path.getsize(path)
     while off < size and (count is None or len(out) < count):
+        with open(path, "rb") as fh:
+            fh.seek(off)
+            magic = int.from_bytes(fh.read(4), "little")
+        if magic & 0xff00 == 0x7300:            # sparse layout
+            obj, off = _read_sparse(path, off)
+            out.append(obj)
+            continue
         h = IoHeader()
         check(lib().ibk_io_read_dense(os.fsencode(path), off, ctypes.byref(h), None, 0, None))
         buf = np.empty(max(h.count, 1), dtype=np.float64)

@@ -374,12 +374,15 @@ ibk_status ibk_server_admit_from(ibk_server server, int member, const char* path
  * 'd' dense | 'd' FP64 or 's' FP32), three 32-bit ints (rows, cols, values)
  * and the values column-major; scalars are raw bytes; objects follow each
  * other in one file.  Host arrays.  Writes are FP64; reads accept FP32 or
- * FP64 values and return FP64.  Sparse containers are not read. */
+ * FP64 values and return FP64.  A sparse container ('s' layout;
+ * io.h:432-470, 497-532) holds (rows, cols, nonzeros), then a matrix's CSR
+ * row starts (rows + 1 ints, none when rows is 0), the nonzeros' column (or,
+ * for a vector, row) indices and their values. */
 typedef struct {
 	int magic;
 	int matrix;             /* 1: matrix, 0: vector */
 	int rows, cols;
-	int count;              /* rows * cols */
+	int count;              /* dense: rows * cols; sparse: nonzeros */
 } ibk_io_header;
 
 ibk_status ibk_io_write_dense(const char* path, int append, int matrix, int rows, int cols,
@@ -390,6 +393,13 @@ ibk_status ibk_io_write_scalar(const char* path, int append, double value);
 ibk_status ibk_io_read_dense(const char* path, long long offset, ibk_io_header* header, double* values,
                              long long capacity, long long* next_offset);
 ibk_status ibk_io_read_scalar(const char* path, long long offset, double* value, long long* next_offset);
+/* Sparse vectors (matrix = 0, cols = 1, starts unused) and CSR matrices. */
+ibk_status ibk_io_write_sparse(const char* path, int append, int matrix, int rows, int cols, int nonzeros,
+                               const int* starts, const int* indices, const double* values);
+/* starts / indices / values all NULL: the header only; else indices and
+ * values of capacity >= nonzeros, and starts of rows + 1 for a matrix. */
+ibk_status ibk_io_read_sparse(const char* path, long long offset, ibk_io_header* header, int* starts,
+                              int* indices, double* values, long long capacity, long long* next_offset);
 
 /* ---- Membrane forces on RBF surfaces ------------------------------------
  * The producers of the point forces that a spread takes: the surface geometry

@@ -51,6 +51,64 @@ def test_reads_fp32_containers_and_rejects_garbage(ibk, tmp_path):
         ibk.io_read(short)
 
 
+MAT_SPARSE_F64 = 0x616d7364   # 'm','a' | 's' sparse | 'd' double
+VEC_SPARSE_F64 = 0x65767364
+
+
+def test_sparse_containers_bytes_and_round_trip(ibk, tmp_path):
+    """io.h:432-470: (rows, cols, nonzeros), a matrix's CSR row starts (rows +
+    1 ints), the indices, then the values."""
+    import scipy.sparse as sp
+    ibk.build()
+    p = str(tmp_path / "sparse.bin")
+    m = sp.csr_matrix(np.array([[0.0, 1.5, 0.0, -2.0], [0.0, 0.0, 0.0, 0.0], [3.0, 0.0, 4.25, 0.0]]))
+    ibk.io_write_sparse(p, m)
+    ibk.io_write_sparse(p, (6, [1, 4], [0.5, -7.0]), append=True)
+    ibk.io_write(str(tmp_path / "dense.bin"), [np.ones(2)])
+    raw = open(p, "rb").read()
+    assert struct.unpack("<4i", raw[:16]) == (MAT_SPARSE_F64, 3, 4, 4)
+    assert struct.unpack("<4i", raw[16:32]) == (0, 2, 2, 4)                 # row starts
+    assert struct.unpack("<4i", raw[32:48]) == (1, 3, 0, 2)                 # column indices
+    assert struct.unpack("<4d", raw[48:80]) == (1.5, -2.0, 3.0, 4.25)
+    assert struct.unpack("<4i", raw[80:96]) == (VEC_SPARSE_F64, 6, 1, 2)
+    assert struct.unpack("<2i", raw[96:104]) == (1, 4)
+    assert struct.unpack("<2d", raw[104:120]) == (0.5, -7.0)
+    assert len(raw) == 120
+    back_m, back_v = ibk.io_read(p)
+    assert (back_m != m).nnz == 0 and back_m.shape == (3, 4)
+    assert back_v[0] == 6 and list(back_v[1]) == [1, 4] and list(back_v[2]) == [0.5, -7.0]
+
+
+def test_sparse_edge_cases_and_mixed_files(ibk, tmp_path):
+    import scipy.sparse as sp
+    ibk.build()
+    # an empty matrix writes no row starts
+    p = str(tmp_path / "empty.bin")
+    ibk.io_write_sparse(p, sp.csr_matrix((0, 5)))
+    assert open(p, "rb").read() == struct.pack("<4i", MAT_SPARSE_F64, 0, 5, 0)
+    (e,) = ibk.io_read(p)
+    assert e.shape == (0, 5) and e.nnz == 0
+    # FP32 values are read as FP64
+    q = str(tmp_path / "f32.bin")
+    with open(q, "wb") as f:
+        f.write(struct.pack("<4i", 0x616d7373, 2, 2, 2) + struct.pack("<3i", 0, 1, 2) + struct.pack("<2i", 1, 0))
+        f.write(struct.pack("<2f", 1.25, -0.5))
+    (m,) = ibk.io_read(q)
+    assert np.array_equal(m.toarray(), np.array([[0.0, 1.25], [-0.5, 0.0]]))
+    # dense and sparse containers in one file
+    r = str(tmp_path / "mixed.bin")
+    rng = np.random.default_rng(1)
+    dense = rng.normal(size=(5, 3))
+    sparse = sp.random(40, 30, density=0.1, random_state=2, format="csr")
+    ibk.io_write(r, [dense])
+    ibk.io_write_sparse(r, sparse, append=True)
+    ibk.io_write(r + ".v", [rng.normal(size=4)])
+    with open(r, "ab") as f:
+        f.write(open(r + ".v", "rb").read())
+    a, b, c = ibk.io_read(r)
+    assert np.array_equal(a, dense) and (b != sparse).nnz == 0 and c.shape == (4,)
+
+
 # the reference's data tables, where its tree is available (IBK_REFERENCE_ROOT)
 REF_DATA = os.path.join(os.environ.get("IBK_REFERENCE_ROOT", ""), "data")
 
