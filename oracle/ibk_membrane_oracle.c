@@ -24,12 +24,13 @@
  *             include/forces/tension.h:148-200 (tension1d),
  *             include/forces/skalak.h:49-55, include/forces/hookean.h:48-54
  *
- * Parity unpinned: the reference's membrane code is device lambdas over its
- * linalg layer and does not build on the host here, so this restatement is
- * checked against the reference's text and against properties of the
- * mechanics (zero force at rest, zero total force and torque on a closed
- * surface, no bending force on the Clifford torus), not against the
- * reference's own output.
+ * Parity pinned: the reference's own force code (forces/skalak.h,
+ * neohookean.h, hookean.h, bending.h, dissipation.h, tether.h and tension1d)
+ * compiled on the host over shim containers (ref_forces.cc) gives the same
+ * bits as this restatement on the same geometry.  The surface geometry (the
+ * operator products, normal and patch area) is restated from the text and
+ * checked against analytic tori; the wall repulsion too, since the
+ * reference's repelling.h does not compile as written.
  */
 #include "ibk_oracle.h"
 

@@ -24,6 +24,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libibk_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libibref.so")
+REF_FORCES_PATH = os.path.join(HERE, "_ref", "libibref_forces.so")
 
 PERIODIC, SOLID = 0, 1
 TAG_MAC, TAG_CENTERED = 0, 1
@@ -33,6 +34,7 @@ DELTA_NAMES = {"bspline": BSPLINE, "peskin": PESKIN, "roma": ROMA, "cosine": COS
 _lock = threading.Lock()
 _lib = None
 _ref = None
+_ref_forces = None
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -140,6 +142,29 @@ def lib():
                                                  _dp, _dp, _dp]
             _lib = L
     return _lib
+
+
+def ref_forces():
+    """The reference's own membrane-force code built on host shims
+    (ref_forces.cc), or None where it cannot be built."""
+    global _ref_forces
+    if ref() is None or not os.path.exists(REF_FORCES_PATH):
+        return None
+    with _lock:
+        if _ref_forces is None:
+            R = ctypes.CDLL(REF_FORCES_PATH)
+            R.ibref_membrane_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                                 ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
+            R.ibref_membrane_bending.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
+                                                 ctypes.c_double, ctypes.c_int, ctypes.POINTER(_dp),
+                                                 ctypes.POINTER(_dp), ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
+            R.ibref_membrane_dissipation.argtypes = [ctypes.c_int, ctypes.c_int, ctypes.c_int, ctypes.POINTER(_dp),
+                                                     ctypes.c_double, _dp, ctypes.POINTER(_dp), _dp]
+            R.ibref_membrane_tether.argtypes = [ctypes.c_double, ctypes.c_int, _dp, _dp, _dp]
+            R.ibref_curve_tension.argtypes = [ctypes.c_int, ctypes.c_double, ctypes.c_double, ctypes.c_int,
+                                              ctypes.POINTER(_dp), ctypes.POINTER(_dp), _dp]
+            _ref_forces = R
+    return _ref_forces
 
 
 def ref():
@@ -472,3 +497,70 @@ def ref_wall_weights(length, resolution, shift, lower, upper):
                              float(upper[0]), float(upper[1]), _d(out))
     return out[:3], out[3:]
 
+
+
+# ---- the reference's own membrane forces (ref_forces.cc), for pinning the restatement
+_KEYS5 = ("tu", "tv", "tuu", "tuv", "tvv")
+
+
+def _parr(arrays):
+    keep = [None if a is None else np.ascontiguousarray(a, dtype=np.float64) for a in arrays]
+    return keep, (_dp * len(keep))(*[None if a is None else _d(a) for a in keep])
+
+
+def ref_membrane_tension(law, shear, bulk, rest, cur):
+    R = ref_forces()
+    kr, rp = _parr([rest[k] for k in _KEYS5] + [rest["sigma"]])
+    kc, cp = _parr([cur[k] for k in _KEYS5])
+    n = kr[5].size
+    f = np.zeros(3 * n)
+    R.ibref_membrane_tension(int(law), float(shear), float(bulk), n, rp, cp, _d(f))
+    return f
+
+
+def ref_membrane_bending(sample_ops, modulus, preferred, data_rest, data_cur, rest, cur, nc):
+    """data_rest / data_cur: the data-site geometry dicts (tu .. tvv, normal,
+    sigma) of the rest and current shapes; rest / cur: the sample ones."""
+    R = ref_forces()
+    cms = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in sample_ops]
+    ns, nd = cms[1].shape
+    keys = _KEYS5 + ("normal", "sigma")
+    k1, a1 = _parr([data_rest[k] for k in keys])
+    k2, a2 = _parr([data_cur[k] for k in keys])
+    k3, a3 = _parr([rest[k] for k in keys])
+    k4, a4 = _parr([cur[k] for k in keys])
+    sp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cms])
+    f = np.zeros(3 * ns * nc)
+    R.ibref_membrane_bending(ns, nd, nc, sp, float(modulus), int(bool(preferred)), a1, a2, a3, a4, _d(f))
+    return f
+
+
+def ref_membrane_dissipation(sample_ops, modulus, u, cur, nc):
+    R = ref_forces()
+    cms = [None if o is None else np.asfortranarray(o, dtype=np.float64) for o in sample_ops]
+    ns, nd = cms[1].shape
+    kc, cp = _parr([cur[k] for k in _KEYS5] + [cur["sigma"]])
+    uu = np.ascontiguousarray(u, dtype=np.float64)
+    sp = (_dp * 6)(*[None if o is None else o.ctypes.data_as(_dp) for o in cms])
+    f = np.zeros(3 * ns * nc)
+    R.ibref_membrane_dissipation(ns, nd, nc, sp, float(modulus), _d(uu), cp, _d(f))
+    return f
+
+
+def ref_membrane_tether(modulus, x_rest, x_cur):
+    R = ref_forces()
+    xr = np.ascontiguousarray(x_rest, dtype=np.float64)
+    xc = np.ascontiguousarray(x_cur, dtype=np.float64)
+    f = np.zeros(xr.size)
+    R.ibref_membrane_tether(float(modulus), xr.size // 3, _d(xr), _d(xc), _d(f))
+    return f
+
+
+def ref_curve_tension(law, shear, bulk, rest, cur):
+    R = ref_forces()
+    kr, rp = _parr([rest["tu"], rest["tuu"], rest["sigma"]])
+    kc, cp = _parr([cur["tu"], cur["tuu"]])
+    n = kr[2].size
+    f = np.zeros(2 * n)
+    R.ibref_curve_tension(int(law), float(shear), float(bulk), n, rp, cp, _d(f))
+    return f
