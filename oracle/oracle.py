@@ -25,6 +25,7 @@ HERE = os.path.dirname(os.path.abspath(__file__))
 LIB_PATH = os.path.join(HERE, "libibk_oracle.so")
 REF_PATH = os.path.join(HERE, "_ref", "libibref.so")
 REF_FORCES_PATH = os.path.join(HERE, "_ref", "libibref_forces.so")
+REF_SOLVER_PATH = os.path.join(HERE, "_ref", "libibref_solver.so")
 
 PERIODIC, SOLID = 0, 1
 TAG_MAC, TAG_CENTERED = 0, 1
@@ -35,6 +36,7 @@ _lock = threading.Lock()
 _lib = None
 _ref = None
 _ref_forces = None
+_ref_solver = None
 
 _dp = ctypes.POINTER(ctypes.c_double)
 _ip = ctypes.POINTER(ctypes.c_int)
@@ -564,3 +566,48 @@ def ref_curve_tension(law, shear, bulk, rest, cur):
     f = np.zeros(2 * n)
     R.ibref_curve_tension(int(law), float(shear), float(bulk), n, rp, cp, _d(f))
     return f
+
+
+# ---- the reference's own solver loop (ref_solver.cc), for pinning the diffusion solve
+_APPLY = ctypes.CFUNCTYPE(None, _dp, _dp, ctypes.c_void_p)
+
+
+def ref_solver():
+    """solvers::pcg and algo::chebyshev built on host shims, or None."""
+    global _ref_solver
+    if ref() is None or not os.path.exists(REF_SOLVER_PATH):
+        return None
+    with _lock:
+        if _ref_solver is None:
+            R = ctypes.CDLL(REF_SOLVER_PATH)
+            R.ibref_chebpcg.argtypes = [ctypes.c_int, _APPLY, ctypes.c_void_p, ctypes.c_double, ctypes.c_double,
+                                        _dp, ctypes.c_double, _dp]
+            R.ibref_chebpcg.restype = ctypes.c_longlong
+            R.ibref_chebyshev_weights.argtypes = [ctypes.c_double, ctypes.c_double, _dp]
+            _ref_solver = R
+    return _ref_solver
+
+
+def ref_chebyshev_weights(a, b):
+    out = np.zeros(4)
+    ref_solver().ibref_chebyshev_weights(float(a), float(b), _d(out))
+    return out
+
+
+def ref_chebpcg(fg: FluidGrid, lam, b, tolerance):
+    """x = (I~ - lam L)^-1 b by the reference's pcg and Chebyshev
+    preconditioner, the operator being the oracle's, on the oracle's
+    Gershgorin interval; returns (x, operator applications)."""
+    n = fg.size
+    lower, upper = gershgorin(fg, lam)
+
+    def apply(inp, out, ctx):
+        src = np.ctypeslib.as_array(inp, shape=(n,))
+        dst = np.ctypeslib.as_array(out, shape=(n,))
+        dst[:] = diffusion_apply(fg, 2, src.copy(), lam=lam)
+
+    cb = _APPLY(apply)
+    bb = np.ascontiguousarray(b, dtype=np.float64)
+    x = np.zeros(n)
+    calls = ref_solver().ibref_chebpcg(n, cb, None, float(lower), float(upper), _d(bb), float(tolerance), _d(x))
+    return x, int(calls)

@@ -1,0 +1,3 @@
+/* host shim: see linalg.h in this directory */
+#pragma once
+#include "linalg/linalg.h"
